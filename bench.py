@@ -1,0 +1,401 @@
+"""Benchmark: CCSDT iteration on 40 spatial orbitals (16 electrons, 64 virtual spin orbitals).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision split|fp64]
+
+A step is one CC iteration of ccq's solver loop (update sweep of every T1..T3
+spin block in the reference's order, energy, DIIS ring write, residuum, and
+the DIIS extrapolation every diis_space+1 iterations) on the seeded synthetic
+Hamiltonian (ERIs from an L=80 factorisation, sigma=0.025, seed 2; no molecular
+integrals travel with the repository).  The working set (T3 blocks 4 x 134 MB
+plus the DIIS ring) exceeds the 126 MB L2, so no flush is needed between steps.
+
+``value`` is device seconds per iteration (CUDA events on the library's
+stream), whole job: max over ranks of the time / (ranks x K).  Multi-GPU runs
+are independent replicas (one solve per GPU, no collective on the data path).
+``e2e`` is the same metric through the C ABI with the T vector in pinned host
+memory: set_t + iterate + get_t per step.  ``--impl reference`` times the CPU
+restatement of the reference algorithm (numpy + threaded BLAS) on this host.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'CCSDT s/iter + TFLOP/s on 1 B200, split vs FP64 GPU; |dE| vs FP64 oracle'
+WORKLOAD = 'CCSDT, 40 spatial orbitals, nel=16, nvir=64, L=80, sigma=0.025, seed=2, UHF spin blocks'
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=12)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    p.add_argument('--precision', default='auto', choices=['auto', 'split', 'fp64'])
+    p.add_argument('--slices', type=int, default=int(os.environ.get('CCQ_B200_SLICES', '4')))
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-converge', action='store_true')
+    return p.parse_args()
+
+
+def dist_init(n):
+    import torch
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, local):
+        self.local = local
+        self.proc = None
+        self.path = os.path.join(ROOT, 'gpurun_out', f'clocks_rank{local}.csv')
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.local), f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith('active'):
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no samples']}
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': max(smax), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def measure_peaks():
+    """cuBLAS DGEMM and int8 GEMM throughput on this GPU (denominators not in MEASURED_PEAKS.json)."""
+    import torch
+    out = {}
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device='cuda')
+    b = torch.randn(n, n, dtype=torch.float64, device='cuda')
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    out['fp64_tflops'] = 2 * n ** 3 / (best * 1e-3) / 1e12
+    del a, b
+    try:
+        a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device='cuda')
+        b = torch.randint(-64, 64, (n, n), dtype=torch.int8, device='cuda').t().contiguous().t()
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        out['int8_tops'] = 2 * n ** 3 / (best * 1e-3) / 1e12
+    except Exception as ex:  # noqa: BLE001
+        out['int8_tops'] = None
+        out['int8_error'] = str(ex)[:120]
+    torch.cuda.empty_cache()
+    return out
+
+
+def measured_peaks_file():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        return json.load(open(p)), 'measured'
+    return {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0, 'bf16_tflops_sustained': 1400.0}, 'fallback'
+
+
+def golden_c2():
+    p = os.path.join(ROOT, 'tests', 'golden', 'synthetic.json')
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get('c2_ccsdt')
+    return None
+
+
+def cpu_reference(system, steps, warmup, budget_s=150.0):
+    """Oracle (numpy restatement of the reference algorithm) on this host's cores."""
+    from oracle.blockcc import BlockCC
+    try:
+        from threadpoolctl import threadpool_info
+        cores = max([x.get('num_threads', 1) for x in threadpool_info()] or [os.cpu_count()])
+    except Exception:  # noqa: BLE001
+        cores = os.cpu_count()
+    txt = open(os.path.join(ROOT, 'ccq_b200', 'plans', 'CCSDT.plan')).read()
+    s = system
+    bc = BlockCC(txt, s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], s['dims'], 'CCSDT')
+    from oracle import solver as S
+    from ccq_b200 import integrals as I
+    lay = I.TLayout(s['dims'])
+    tvec = np.zeros(lay.t_size)
+    ring = S.Ring(5, lay.t_size)
+    times = []
+    t_start = time.time()
+    it = 0
+    while True:
+        it += 1
+        t0 = time.perf_counter()
+        bc.update(tvec)
+        e = bc.energy(tvec)
+        ring.write(it, tvec)
+        ring.residuum(it)
+        if it % 6 == 0:
+            tvec[:] = ring.diis()
+        dt = time.perf_counter() - t0
+        if it > warmup:
+            times.append(dt)
+        if len(times) >= steps or (time.time() - t_start > budget_s and times):
+            break
+    return {'s_per_iter': float(np.median(times)), 'iters_timed': len(times), 'cores': int(cores or 1),
+            'e_last': e}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from ccq_b200 import synth
+    s = synth.system(synth.C2)
+    w = max(0, min(args.warmup, 1))
+    r = cpu_reference(s, max(1, min(args.steps, 3)), w)
+    line = {
+        'metric': METRIC, 'impl': 'reference', 'value': r['s_per_iter'], 'unit': 's/iter',
+        'n_gpus': args.gpus, 'steps': r['iters_timed'], 'warmup': w, 'ms_per_step': r['s_per_iter'] * 1e3,
+        'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic (seeded generator, no molecular integrals)',
+        'config': {'workload': WORKLOAD, 'parallelism': 'cpu threads', 'l2': 'working set > L2'},
+        'cpu_baseline': {'value': r['s_per_iter'], 'unit': 's/iter', 'cores': r['cores'], 'kind': 'port',
+                         'sample': f"{r['iters_timed']} full CCSDT iteration(s) after {w} warm-up, numpy restatement "
+                                   'of the reference algorithm (ccq has no Fortran compiler on this image)'},
+        'e2e': {'value': r['s_per_iter'], 'unit': 's/iter', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def time_leg(ctx, it0, steps, world):
+    """Run `steps` iterations; returns (device ms list, energies)."""
+    import torch
+    ms, es = [], []
+    barrier(world)
+    torch.cuda.synchronize()
+    for k in range(steps):
+        e, res, did = ctx.iterate(it0 + k)
+        ms.append(ctx.timing()[1])
+        es.append(e)
+    torch.cuda.synchronize()
+    barrier(world)
+    return ms, es
+
+
+def main():
+    args = parse()
+    import torch
+    rank, world, local = dist_init(args.gpus)
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    from ccq_b200 import lib, synth
+    if args.warmup < 3:
+        args.warmup = 3
+    s = synth.system(synth.C2)
+    d = s['dims']
+    peaks_live = measure_peaks()
+    peaks_file, peaks_kind = measured_peaks_file()
+
+    def new_ctx():
+        c = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CCSDT', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                        s['v_bb'], rhf=False, shift=0.0, diis_space=5)
+        c.use_graph(True)
+        return c
+
+    ctx = new_ctx()
+    split_ok = True
+    try:
+        ctx.set_precision(lib.PREC_SPLIT, args.slices)
+        ctx.set_precision(lib.PREC_FP64, args.slices)
+    except lib.CCQB200Error:
+        split_ok = False
+    headline = args.precision if args.precision != 'auto' else ('split' if split_ok else 'fp64')
+    legs = ['fp64'] + (['split'] if split_ok and args.precision != 'fp64' else [])
+    clocks = Clocks(local)
+    results = {}
+    it = 1
+    for leg in legs:
+        ctx.set_precision(lib.PREC_SPLIT if leg == 'split' else lib.PREC_FP64, args.slices)
+        # warm-up continues the same solve (iterations keep counting, DIIS on schedule)
+        for _ in range(args.warmup):
+            ctx.iterate(it)
+            it += 1
+        if leg == headline:
+            clocks.start()
+        ms, es = time_leg(ctx, it, args.steps, world)
+        if leg == headline:
+            clk = clocks.stop()
+        it += args.steps
+        st = ctx.stats()
+        tot = allmax(sum(ms), world)
+        results[leg] = {'s_per_iter': tot / 1e3 / (world * args.steps), 'ms_total': tot,
+                        'tflops': st['flops'] * world * args.steps / (tot * 1e-3) / 1e12,
+                        'launches_per_iter': st['launches'], 'flops_per_iter': st['flops']}
+    head = results[headline]
+
+    # per-kernel roofline: eager sweep with events around every launch
+    ctx.set_precision(lib.PREC_SPLIT if headline == 'split' else lib.PREC_FP64, args.slices)
+    ctx.profile(True)
+    for _ in range(2):
+        ctx.iterate(it)
+        it += 1
+    prof = ctx.profile_get()
+    ctx.profile(False)
+    kname = 'gett_split' if headline == 'split' else 'gett_f64'
+    kp = prof[kname]
+    achieved = kp['flops'] / (kp['ms'] * 1e-3) / 1e12 if kp['ms'] > 0 else 0.0
+    if headline == 'fp64':
+        peak, peak_src = peaks_live['fp64_tflops'], 'cuBLAS DGEMM 8192^3 measured in this run'
+    else:
+        peak, peak_src = peaks_live.get('int8_tops') or 2 * peaks_file['bf16_tflops'], \
+            'cuBLASLt int8 GEMM 8192^3 measured in this run (FP64-algorithmic FLOP/s vs int8 op/s)'
+    roofline = {'bound': 'tensor', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                'frac': achieved / peak if peak else None, 'traffic': None, 'kernel': kname,
+                'peak_source': peak_src, 'profile': prof,
+                'note': 'achieved = algorithmic FP64 FLOPs of all GETT launches of 2 eager sweeps / their summed '
+                        'CUDA-event durations'}
+
+    # end-to-end through the C ABI with host buffers
+    pinned = torch.empty(ctx.t_size, dtype=torch.float64, pin_memory=True)
+    pinned.copy_(torch.from_numpy(ctx.get_t()))
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        ctx.set_t_ptr(pinned.data_ptr(), ctx.t_size)
+        ctx.iterate(it)
+        it += 1
+        ctx.get_t_ptr(pinned.data_ptr(), ctx.t_size)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_s = allmax(time.perf_counter() - t0, world) / (world * args.steps)
+    bytes_t = ctx.t_size * 8
+    ctx.close()
+
+    # convergence to tol with the headline path, |dE| vs the FP64 oracle fixture
+    conv = None
+    if not args.no_converge:
+        from ccq_b200 import config, driver
+        c2 = new_ctx()
+        cfg = config.Config(calc_type='CCSDT', tol=1e-8, diis_space=5, max_iter=100,
+                            gpu_precision=headline, gpu_slices=args.slices).calc_macros()
+        r = driver.solve_cc(c2, cfg, out=lambda x: None)
+        c2.close()
+        g = golden_c2()
+        conv = {'iterations': r.iterations, 'e_cor': r.e_cor, 'failed': r.failed,
+                'dE_vs_fp64_oracle': (abs(r.e_cor - g['e_cor']) if g else None),
+                'oracle': 'tests/golden/synthetic.json c2_ccsdt' if g else 'fixture missing',
+                'split_iterations': sum(1 for h in r.history if h['split'])}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference(s, 1, 0, budget_s=60.0)
+        cpu = {'value': r['s_per_iter'], 'unit': 's/iter', 'cores': r['cores'], 'kind': 'port',
+               'sample': 'first CCSDT iteration of the same workload (one full update sweep + energy + ring), numpy '
+                         'restatement of the reference algorithm with threaded BLAS'}
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': head['s_per_iter'], 'unit': 's/iter', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': head['s_per_iter'] * 1e3 * world,
+            'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f64' if headline == 'fp64' else f'f64 (int8 x{args.slices} slices, int32 acc)',
+            'data': 'synthetic (seeded generator, no molecular integrals)',
+            'config': {'workload': WORKLOAD, 'precision': headline, 'parallelism': f'replicas x{world}',
+                       'l2': 'working set (T3 4x134 MB + DIIS ring) > 126 MB L2, no flush'},
+            'tflops': head['tflops'], 'legs': results,
+            'speedup_split_vs_fp64': (results['fp64']['s_per_iter'] / results['split']['s_per_iter']
+                                      if 'split' in results else None),
+            'roofline': roofline,
+            'cpu_baseline': cpu,
+            'e2e': {'value': e2e_s, 'unit': 's/iter', 'h2d_bytes_per_step': bytes_t,
+                    'd2h_bytes_per_step': bytes_t + 16},
+            'gpu_launches': head['launches_per_iter'] * args.steps,
+            'clocks': clk, 'convergence': conv,
+            'peaks': {'live': peaks_live, 'file': peaks_file, 'file_kind': peaks_kind},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,168 @@
+"""ccq input-file parser (keys and calc_type macros of ``src/parser.f90``).
+
+  * ``parse``          <- ``get_config`` (``src/parser.f90:99-185``): a line
+    containing ``#`` or ``!`` anywhere is skipped; ``key=value`` or bare flag keys
+  * key aliases        <- ``get_sys_data`` (``:440-470``), ``get_run_opts``
+    (``:638-732``), defaults of ``set_default_options`` (``:779-844``)
+  * ``process``        <- ``process_sys_data`` (``:476-504``)
+  * ``calc_macros``    <- ``get_calc_macros`` (``:316-432``)
+
+New keys of this engine are prefixed ``gpu_``: ``gpu_precision`` (fp64 |
+split), ``gpu_slices`` (int8 slices per operand), ``gpu_fp64_finish`` (|dE|
+below which the split mode hands over to FP64), ``gpu_graph`` (replay each
+sweep as one CUDA graph).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+
+def _logical(val):
+    v = val.strip().lower().strip('.')
+    if v in ('true', 't', 'yes', '1'):
+        return True
+    if v in ('false', 'f', 'no', '0'):
+        return False
+    raise ValueError(f'CONFIGURATION ERROR: {val!r} must be logical')
+
+
+def _ftrunc_div(a, b):
+    return int(a / b) if b else 0
+
+
+@dataclass
+class Config:
+    froz_spin: int = 0
+    nel: int = -1
+    nvirt: int = -1
+    mult: int = 0
+    rhf: bool = False
+    shift: float = 0.0
+    max_iter: int = 60
+    diis_space: int = 5
+    tol: float = 1.0e-4
+    calc_type: str = ''
+    onebody: str = 'onebody.inp'
+    twobody: str = 'twobody.inp'
+    keep_bin: bool = True
+    num_threads: int = 1
+    restart: bool = False
+    label: str = ''
+    sym_file: str = ''
+    gpu_precision: str = 'fp64'
+    gpu_slices: int = 4
+    gpu_fp64_finish: float = 1.0e-6
+    gpu_graph: bool = True
+    # derived (process_sys_data)
+    froz: int = 0
+    occ_a: int = 0
+    occ_b: int = 0
+    orbs: int = 0
+    lvl_t: bool = False
+    lvl_q: bool = False
+    extra: dict = field(default_factory=dict)
+
+    def process(self):
+        self.froz = self.froz_spin // 2
+        self.occ_a = self.nel // 2
+        self.occ_b = self.occ_a - _ftrunc_div(self.mult - 1, 2)
+        self.orbs = (self.nel + self.nvirt) // 2
+        return self
+
+    def calc_macros(self):
+        ct = self.calc_type
+        if ct == 'CCSD':
+            self.lvl_t, self.lvl_q = False, False
+        elif ct == 'CCSDT':
+            self.lvl_t, self.lvl_q = True, False
+        elif ct == 'CCSDTQ':
+            self.lvl_t, self.lvl_q = True, True
+        else:
+            raise ValueError(f'calc_type {ct!r} is not served by this engine '
+                             '(CCSD, CCSDT, CCSDTQ are; the others stay on the CPU program)')
+        return self
+
+
+def parse_lines(lines):
+    cfg = Config()
+    for raw in lines:
+        line = raw.rstrip('\n')
+        if '#' in line or '!' in line:
+            continue
+        if line.strip() == '':
+            continue
+        if '=' in line:
+            k, v = line.split('=', 1)
+            key, val = k.strip(), v.strip()
+        else:
+            key, val = line.strip(), ''
+        _apply(cfg, key, val)
+    return cfg.process()
+
+
+def parse(path):
+    with open(path) as fh:
+        return parse_lines(fh.readlines())
+
+
+def _apply(cfg, key, val):
+    if key in ('core', 'nfroz', 'frozen', 'froz'):
+        cfg.froz_spin = int(val)
+    elif key in ('nel', 'electrons'):
+        cfg.nel = int(val)
+    elif key in ('nvir', 'nvirt', 'virtuals'):
+        cfg.nvirt = int(val)
+    elif key in ('multiplicity', 'mult'):
+        cfg.mult = int(val)
+    elif key == 'rhf':
+        cfg.rhf = _logical(val)
+    elif key == 'shift':
+        cfg.shift = float(val.replace('d', 'e').replace('D', 'E'))
+    elif key in ('max_iterations', 'max_iter'):
+        cfg.max_iter = int(val)
+    elif key in ('diis_space', 'diis'):
+        cfg.diis_space = int(val)
+    elif key in ('tolerance', 'tol', 'itol'):
+        try:
+            itol = int(val)
+            cfg.tol = 10.0 ** itol
+        except ValueError:
+            cfg.tol = float(val.replace('d', 'e').replace('D', 'E'))
+    elif key == 'calc_type':
+        cfg.calc_type = val
+    elif key in ('restart', 'rest'):
+        cfg.restart = True
+    elif key == 'label':
+        cfg.label = val
+    elif key in ('symfile', 'sym_file'):
+        cfg.sym_file = val
+    elif key == 'onebody':
+        cfg.onebody = val
+    elif key == 'twobody':
+        cfg.twobody = val
+    elif key == 'keep_bin':
+        cfg.keep_bin = _logical(val)
+    elif key == 'num_threads':
+        cfg.num_threads = int(val)
+    elif key == 'gpu_precision':
+        if val not in ('fp64', 'split'):
+            raise ValueError('gpu_precision must be fp64 or split')
+        cfg.gpu_precision = val
+    elif key == 'gpu_slices':
+        cfg.gpu_slices = int(val)
+    elif key == 'gpu_fp64_finish':
+        cfg.gpu_fp64_finish = float(val)
+    elif key == 'gpu_graph':
+        cfg.gpu_graph = _logical(val)
+    else:
+        cfg.extra[key] = val
+
+
+def format_config(cfg):
+    return (f'froz={cfg.froz} occ_a={cfg.occ_a} occ_b={cfg.occ_b} orbs={cfg.orbs} calc_type={cfg.calc_type} '
+            f'tol={cfg.tol:.1e} diis_space={cfg.diis_space} shift={cfg.shift}')
+
+
+def isclose(a, b):
+    return math.isclose(a, b, rel_tol=0, abs_tol=1e-15)

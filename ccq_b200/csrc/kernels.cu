@@ -1,0 +1,417 @@
+// Device kernels of libccq_b200; see kernels.cuh for the role of each.
+#include "kernels.cuh"
+
+namespace ccqb {
+
+// ---------------------------------------------------------------------------
+// GETT, FP64 on the DMMA tensor pipe
+// ---------------------------------------------------------------------------
+constexpr int BM = 64, BN = 64, BKT = 16, PADS = 4;
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    int sz = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// Loads one BKT x BM tile of a GETT operand into shared memory [k][m].
+// kmajor: consecutive threads walk k (operand stride-1 along its k modes),
+// else they walk m.  Rows beyond M or columns beyond kend are zero-filled.
+template <bool KMAJOR>
+__device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *base, const int *offm_reg,
+                                          const int *offk, int m0, int M, int k0, int kend, int tid) {
+    if (KMAJOR) {
+        int kk = tid & 15;
+        int mrow = tid >> 4;
+        int k = k0 + kk;
+        bool kin = k < kend;
+        int ok = kin ? __ldg(offk + k) : 0;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            int m = mrow + 8 * p;
+            bool in = kin && (m0 + m < M);
+            const double *src = in ? base + (long long)offm_reg[p] + ok : base;
+            cp_async8(&S[kk][m], src, in);
+        }
+    } else {
+        int m = tid & 63;
+        int krow = tid >> 6;
+        bool min_ = (m0 + m) < M;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            int kk = krow + 2 * p;
+            int k = k0 + kk;
+            bool in = min_ && k < kend;
+            const double *src = in ? base + (long long)offm_reg[0] + __ldg(offk + k) : base;
+            cp_async8(&S[kk][m], src, in);
+        }
+    }
+}
+
+template <bool AK, bool BKM>
+__global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
+    __shared__ __align__(16) double As[2][BKT][BM + PADS];
+    __shared__ __align__(16) double Bs[2][BKT][BN + PADS];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kbeg = blockIdx.z * g.kchunk;
+    const int kend = min(g.K, kbeg + g.kchunk);
+
+    int offa[8], offb[8];
+    if (AK) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            int m = m0 + (tid >> 4) + 8 * p;
+            offa[p] = m < g.M ? __ldg(g.offA_m + m) : 0;
+        }
+    } else {
+        int m = m0 + (tid & 63);
+        offa[0] = m < g.M ? __ldg(g.offA_m + m) : 0;
+    }
+    if (BKM) {
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            int n = n0 + (tid >> 4) + 8 * p;
+            offb[p] = n < g.N ? __ldg(g.offB_n + n) : 0;
+        }
+    } else {
+        int n = n0 + (tid & 63);
+        offb[0] = n < g.N ? __ldg(g.offB_n + n) : 0;
+    }
+
+    double acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+    const int ntiles = kend > kbeg ? (kend - kbeg + BKT - 1) / BKT : 0;
+    if (ntiles > 0) {
+        load_tile<AK>(As[0], g.A, offa, g.offA_k, m0, g.M, kbeg, kend, tid);
+        load_tile<BKM>(Bs[0], g.B, offb, g.offB_k, n0, g.N, kbeg, kend, tid);
+        cp_async_commit();
+    }
+    for (int t = 0; t < ntiles; ++t) {
+        const int st = t & 1;
+        if (t + 1 < ntiles) {
+            int k0 = kbeg + (t + 1) * BKT;
+            load_tile<AK>(As[st ^ 1], g.A, offa, g.offA_k, m0, g.M, k0, kend, tid);
+            load_tile<BKM>(Bs[st ^ 1], g.B, offb, g.offB_k, n0, g.N, k0, kend, tid);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BKT; kk += 4) {
+            double a[2][2], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                a[mi][0] = As[st][kk + tig][wm + mi * 16 + gid];
+                a[mi][1] = As[st][kk + tig][wm + mi * 16 + gid + 8];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[st][kk + tig][wn + ni * 8 + gid];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], a[mi][0], a[mi][1], b[ni]);
+        }
+        __syncthreads();
+    }
+
+    const bool atomic = gridDim.z > 1;
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            int m = m0 + wm + mi * 16 + gid + 8 * h;
+            if (m >= g.M) continue;
+            long long om = __ldg(g.offC_m + m);
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    int n = n0 + wn + ni * 8 + 2 * tig + j;
+                    if (n >= g.N) continue;
+                    double *c = g.C + om + __ldg(g.offC_n + n);
+                    double v = g.alpha * acc[mi][ni][2 * h + j];
+                    if (atomic)
+                        atomicAdd(c, v);
+                    else
+                        *c = g.beta ? *c + v : v;
+                }
+            }
+        }
+    }
+}
+
+void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
+    dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, (a.K + a.kchunk - 1) / a.kchunk);
+    if (grid.z == 0) grid.z = 1;
+    if (a_kmajor && b_kmajor)
+        gett_f64_kernel<true, true><<<grid, 128, 0, s>>>(a);
+    else if (a_kmajor)
+        gett_f64_kernel<true, false><<<grid, 128, 0, s>>>(a);
+    else if (b_kmajor)
+        gett_f64_kernel<false, true><<<grid, 128, 0, s>>>(a);
+    else
+        gett_f64_kernel<false, false><<<grid, 128, 0, s>>>(a);
+}
+
+__global__ void zero_view_kernel(double *C, const int *offm, const int *offn, int M, int N) {
+    long long total = (long long)M * N;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        int m = (int)(i / N), n = (int)(i % N);
+        C[(long long)offm[m] + offn[n]] = 0.0;
+    }
+}
+
+void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N, cudaStream_t s) {
+    long long total = (long long)M * N;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    zero_view_kernel<<<blocks, 256, 0, s>>>(C, offm, offn, M, N);
+}
+
+// ---------------------------------------------------------------------------
+// assemble: residual gather + Jacobi + antisymmetric fill
+// ---------------------------------------------------------------------------
+__global__ void assemble_kernel(AsmArgs a) {
+    for (long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x; lin < a.total;
+         lin += (long long)gridDim.x * blockDim.x) {
+        int x[MAXR];
+        long long r = lin;
+        for (int d = a.rank - 1; d >= 0; --d) {
+            x[d] = (int)(r % a.dims[d]);
+            r /= a.dims[d];
+        }
+        bool canon = true;
+        for (int d = 1; d < a.rank; ++d)
+            if (!a.runstart[d] && x[d] <= x[d - 1]) canon = false;
+        if (!canon) continue;
+        double R = 0.0;
+        for (int t = 0; t < a.nterms; ++t) {
+            const AsmTerm &tm = a.terms[t];
+            long long off = 0;
+            for (int d = 0; d < a.rank; ++d) off += (long long)tm.stride[d] * x[d];
+            R += tm.coef * tm.p[off];
+        }
+        long long toff = 0;
+        for (int d = 0; d < a.rank; ++d) toff += (long long)a.tstride[d] * x[d];
+        double tnew;
+        if (a.mode == 0) {
+            double D = a.shift;
+            for (int d = 0; d < a.level; ++d) D -= a.fdiag[a.spin[d]][x[d]];
+            for (int d = a.level; d < a.rank; ++d) D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[d]];
+            tnew = a.T[toff] - R / D;
+        } else {
+            tnew = R;
+        }
+        for (int p = 0; p < a.nperm; ++p) {
+            const signed char *P = a.perm + p * a.rank;
+            long long o = 0;
+            for (int d = 0; d < a.rank; ++d) o += (long long)a.tstride[d] * x[P[d]];
+            a.T[o] = a.psign[p] * tnew;
+        }
+    }
+}
+
+void launch_assemble(const AsmArgs &a, cudaStream_t s) {
+    long long blocks = (a.total + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    assemble_kernel<<<(int)blocks, 256, 0, s>>>(a);
+}
+
+__global__ void fill_kernel(double *p, double v, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+void launch_fill(double *p, double v, long long n, cudaStream_t s) {
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    fill_kernel<<<(int)blocks, 256, 0, s>>>(p, v, n);
+}
+
+// ---------------------------------------------------------------------------
+// DIIS on the HBM ring (src/diis.F90)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void sqdiff_kernel(const double *a, const double *b, long long n, double *out) {
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double d = (a ? a[i] : 0.0) - b[i];
+        acc += d * d;
+    }
+    acc = warp_sum(acc);
+    __shared__ double sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) atomicAdd(out, v);
+    }
+}
+
+void launch_sqdiff(const double *a, const double *b, long long n, double *out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(double), s);
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    sqdiff_kernel<<<(int)blocks, 256, 0, s>>>(a, b, n, out);
+}
+
+template <int DS>
+__global__ void gram_kernel(const double *ring, long long stride, long long n, double *gram) {
+    double acc[DS][DS];
+#pragma unroll
+    for (int i = 0; i < DS; ++i)
+#pragma unroll
+        for (int j = 0; j < DS; ++j) acc[i][j] = 0.0;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n; x += (long long)gridDim.x * blockDim.x) {
+        double v[DS + 1];
+#pragma unroll
+        for (int i = 0; i <= DS; ++i) v[i] = ring[i * stride + x];
+        double d[DS];
+#pragma unroll
+        for (int i = 0; i < DS; ++i) d[i] = v[i + 1] - v[i];
+#pragma unroll
+        for (int i = 0; i < DS; ++i)
+#pragma unroll
+            for (int j = i; j < DS; ++j) acc[i][j] += d[i] * d[j];
+    }
+    __shared__ double sh[32];
+#pragma unroll
+    for (int i = 0; i < DS; ++i)
+#pragma unroll
+        for (int j = i; j < DS; ++j) {
+            double v = warp_sum(acc[i][j]);
+            __syncthreads();
+            if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                double w = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+                w = warp_sum(w);
+                if (threadIdx.x == 0) atomicAdd(&gram[i * DS + j], w);
+            }
+        }
+}
+
+void launch_diis_gram(const double *ring, long long stride, int ds, long long n, double *gram, cudaStream_t s) {
+    cudaMemsetAsync(gram, 0, sizeof(double) * ds * ds, s);
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    if (blocks < 1) blocks = 1;
+    switch (ds) {
+#define CASE(D) \
+    case D: gram_kernel<D><<<(int)blocks, 256, 0, s>>>(ring, stride, n, gram); break;
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10) CASE(11) CASE(12)
+#undef CASE
+        default: break;
+    }
+}
+
+// Bordered DIIS system of construct_b_mat (diis.F90:159-242, the corner is -1
+// as in the reference) solved by LU with partial pivoting like dgesv.
+__global__ void diis_solve_kernel(const double *gram, int ds, double *coef, int *info) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = ds + 1;
+    double B[13][13];
+    double c[13];
+    for (int i = 0; i < ds; ++i)
+        for (int j = 0; j < ds; ++j) B[i][j] = (i <= j) ? gram[i * ds + j] : gram[j * ds + i];
+    for (int i = 0; i < n; ++i) {
+        B[i][ds] = -1.0;
+        B[ds][i] = -1.0;
+        c[i] = 0.0;
+    }
+    c[ds] = -1.0;
+    int inf = 0;
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        double best = fabs(B[k][k]);
+        for (int i = k + 1; i < n; ++i)
+            if (fabs(B[i][k]) > best) {
+                best = fabs(B[i][k]);
+                p = i;
+            }
+        if (best == 0.0) {
+            inf = k + 1;
+            break;
+        }
+        if (p != k) {
+            for (int j = 0; j < n; ++j) {
+                double t = B[k][j];
+                B[k][j] = B[p][j];
+                B[p][j] = t;
+            }
+            double t = c[k];
+            c[k] = c[p];
+            c[p] = t;
+        }
+        for (int i = k + 1; i < n; ++i) {
+            double f = B[i][k] / B[k][k];
+            for (int j = k; j < n; ++j) B[i][j] -= f * B[k][j];
+            c[i] -= f * c[k];
+        }
+    }
+    if (!inf) {
+        for (int i = n - 1; i >= 0; --i) {
+            double s = c[i];
+            for (int j = i + 1; j < n; ++j) s -= B[i][j] * c[j];
+            c[i] = s / B[i][i];
+        }
+        for (int i = 0; i < n; ++i) coef[i] = c[i];
+    }
+    *info = inf;
+}
+
+void launch_diis_solve(double *gram, int ds, double *coef, int *info, cudaStream_t s) {
+    diis_solve_kernel<<<1, 32, 0, s>>>(gram, ds, coef, info);
+}
+
+__global__ void diis_extrap_kernel(const double *ring, long long stride, int ds, long long n, const double *coef,
+                                   double *t) {
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n; x += (long long)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int i = 0; i < ds; ++i) acc += coef[i] * ring[i * stride + x];
+        t[x] = acc;
+    }
+}
+
+void launch_diis_extrap(const double *ring, long long stride, int ds, long long n, const double *coef, double *t,
+                        cudaStream_t s) {
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    diis_extrap_kernel<<<(int)blocks, 256, 0, s>>>(ring, stride, ds, n, coef, t);
+}
+
+}  // namespace ccqb

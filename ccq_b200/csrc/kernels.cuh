@@ -1,0 +1,69 @@
+// Device kernels of libccq_b200 (sm_100a).
+//
+//  gett_f64     : GEMM over strided/permuted tensor views (GETT) in FP64 on the
+//                 DMMA tensor pipe (mma.sync m16n8k4 f64).  Operand addresses
+//                 come from per-mode offset tables, so a permuted slice of a
+//                 resident tensor is read in place: this fuses the reference's
+//                 reorder_shift / reorder_stripe + egemm + sum_stripe triple
+//                 (src/cc/reorder_stripe.f90, src/dgemm.f90) into one kernel.
+//  assemble     : residual gather of a spin block from permuted views, Jacobi
+//                 step and antisymmetric fill (src/cc/t*_update.f90 tails).
+//  diis_*       : ring residuum, B matrix, bordered solve and extrapolation
+//                 (src/diis.F90).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ccqb {
+
+constexpr int MAXR = 8;        // max tensor rank (T4 blocks)
+constexpr int MAX_TERMS = 512; // max views gathered by one assemble
+
+struct GettArgs {
+    const double *A;
+    const double *B;
+    double *C;
+    const int *offA_m, *offA_k, *offB_n, *offB_k, *offC_m, *offC_n;
+    int M, N, K;
+    double alpha;
+    int beta;       // 0: overwrite, 1: accumulate
+    int kchunk;     // K range handled by one blockIdx.z (split-K, atomic epilogue)
+};
+
+struct AsmTerm {
+    const double *p;
+    double coef;
+    int stride[MAXR];   // stride of the source for each target axis
+};
+
+struct AsmArgs {
+    double *T;
+    int rank;                 // 2 * level
+    int level;
+    int dims[MAXR];
+    int tstride[MAXR];
+    int spin[MAXR];           // 0 alpha, 1 beta per axis
+    int runstart[MAXR];       // 1 if this axis starts a same-spin run within its half
+    const double *fdiag[2];   // undressed Fock diagonals (active range)
+    int nocc[2];
+    double shift;
+    int mode;                 // 0 jacobi, 1 copy
+    int nterms;
+    const AsmTerm *terms;
+    int nperm;                // orbit permutations of a canonical element
+    const signed char *perm;  // nperm x rank axis maps
+    const signed char *psign; // nperm signs
+    long long total;
+};
+
+void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s);
+void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N, cudaStream_t s);
+void launch_assemble(const AsmArgs &a, cudaStream_t s);
+void launch_fill(double *p, double v, long long n, cudaStream_t s);
+void launch_sqdiff(const double *a, const double *b, long long n, double *out, cudaStream_t s);
+void launch_diis_gram(const double *ring, long long stride, int ds, long long n, double *gram, cudaStream_t s);
+void launch_diis_solve(double *gram, int ds, double *coef, int *info, cudaStream_t s);
+void launch_diis_extrap(const double *ring, long long stride, int ds, long long n, const double *coef, double *t,
+                        cudaStream_t s);
+
+}  // namespace ccqb

@@ -1,0 +1,1022 @@
+// Host runtime of libccq_b200: plan instantiation, resident device state,
+// ccq's iteration step and the C ABI declared in include/ccq_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ccq_b200.h"
+#include "kernels.cuh"
+#include "plans_embedded.h"
+#include "split.cuh"
+
+using namespace ccqb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                     \
+    do {                                                                                          \
+        cudaError_t e_ = (x);                                                                     \
+        if (e_ != cudaSuccess)                                                                    \
+            throw Error(e_ == cudaErrorMemoryAllocation ? CCQ_B200_ENOMEM : CCQ_B200_ECUDA,       \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                         \
+    } while (0)
+
+int fail(const Error &e) {
+    g_last_error = e.what();
+    return e.code;
+}
+
+// ---------------------------------------------------------------------------
+// plan text
+// ---------------------------------------------------------------------------
+struct AxisSpec {
+    std::string label, size, start;
+};
+struct ViewSpec {
+    std::string buf;
+    std::vector<AxisSpec> axes;
+};
+
+ViewSpec parse_view(const std::string &tok) {
+    ViewSpec v;
+    size_t lb = tok.find('[');
+    if (lb == std::string::npos || tok.back() != ']') throw Error(CCQ_B200_EPLAN, "bad view " + tok);
+    v.buf = tok.substr(0, lb);
+    std::string body = tok.substr(lb + 1, tok.size() - lb - 2);
+    if (!body.empty()) {
+        std::stringstream ss(body);
+        std::string a;
+        while (std::getline(ss, a, ',')) {
+            AxisSpec ax;
+            ax.start = "0";
+            size_t at = a.find('@');
+            if (at != std::string::npos) {
+                ax.start = a.substr(at + 1);
+                a = a.substr(0, at);
+            }
+            size_t c = a.find(':');
+            if (c == std::string::npos) throw Error(CCQ_B200_EPLAN, "bad axis " + a);
+            ax.label = a.substr(0, c);
+            ax.size = a.substr(c + 1);
+            v.axes.push_back(ax);
+        }
+    }
+    return v;
+}
+
+enum OpKind { OP_GETT, OP_ASM, OP_COPY, OP_ZERO, OP_PHASE };
+
+struct Op {
+    OpKind kind;
+    // GETT
+    double alpha = 1.0;
+    int beta = 0;
+    ViewSpec c, a, b;
+    std::string tag;
+    // ASSEMBLE
+    std::string block, mode;
+    std::vector<std::pair<double, ViewSpec>> terms;
+    // COPY / ZERO / PHASE
+    std::string arg0, arg1;
+    // instantiated
+    GettArgs g{};
+    int akm = 1, bkm = 1;
+    bool zero_first = false;
+    bool split = false;        // eligible for split precision
+    long long mnk[3] = {0, 0, 0};
+    AsmArgs asmargs{};
+};
+
+struct BufSpec {
+    std::string name, kind;
+    std::vector<std::string> dims;
+};
+
+struct Plan {
+    std::string method;
+    std::vector<BufSpec> bufs;
+    std::vector<Op> ops;
+};
+
+Plan parse_plan(const char *text) {
+    Plan p;
+    std::stringstream in(text);
+    std::string line;
+    std::getline(in, line);
+    {
+        std::stringstream ls(line);
+        std::string w;
+        ls >> w >> p.method;
+        if (w != "PLAN") throw Error(CCQ_B200_EPLAN, "plan header");
+    }
+    while (std::getline(in, line)) {
+        std::stringstream ls(line);
+        std::string w;
+        ls >> w;
+        if (w == "BUF") {
+            BufSpec b;
+            int nd;
+            ls >> b.name >> b.kind >> nd;
+            for (int i = 0; i < nd; ++i) {
+                std::string d;
+                ls >> d;
+                b.dims.push_back(d);
+            }
+            p.bufs.push_back(b);
+        } else if (w == "OPS") {
+            continue;
+        } else if (w == "GETT") {
+            Op o;
+            o.kind = OP_GETT;
+            std::string c, a, b;
+            ls >> o.alpha >> o.beta >> c >> a >> b;
+            ls >> o.tag;
+            o.c = parse_view(c);
+            o.a = parse_view(a);
+            o.b = parse_view(b);
+            p.ops.push_back(o);
+        } else if (w == "ASSEMBLE") {
+            Op o;
+            o.kind = OP_ASM;
+            int nt;
+            ls >> o.block >> o.mode >> nt;
+            for (int i = 0; i < nt; ++i) {
+                std::getline(in, line);
+                std::stringstream ts(line);
+                std::string tw, vv;
+                double coef;
+                ts >> tw >> coef >> vv;
+                if (tw != "TERM") throw Error(CCQ_B200_EPLAN, "TERM expected");
+                o.terms.push_back({coef, parse_view(vv)});
+            }
+            p.ops.push_back(o);
+        } else if (w == "COPY" || w == "ZERO" || w == "PHASE") {
+            Op o;
+            o.kind = w == "COPY" ? OP_COPY : (w == "ZERO" ? OP_ZERO : OP_PHASE);
+            ls >> o.arg0 >> o.arg1;
+            p.ops.push_back(o);
+        } else if (w == "END") {
+            break;
+        } else if (!w.empty()) {
+            throw Error(CCQ_B200_EPLAN, "unknown plan line: " + line);
+        }
+    }
+    return p;
+}
+
+const char *find_plan(const std::string &calc_type, bool rhf) {
+    std::string key = calc_type + (rhf ? "_rhf" : "");
+    for (int i = 0; ccqb_plans[i].name; ++i)
+        if (key == ccqb_plans[i].name) return ccqb_plans[i].text;
+    return nullptr;
+}
+
+struct DevBuf {
+    double *ptr = nullptr;
+    std::vector<long long> shape, stride;
+    long long numel = 0;
+};
+
+}  // namespace
+
+struct ccq_b200_ctx {
+    std::string calc_type;
+    int rhf = 0;
+    double shift = 0.0;
+    int ds = 5;
+    long long oa, ob, va, vb, n, froz;
+    std::map<std::string, long long> size;
+    Plan plan;
+    std::map<std::string, DevBuf> bufs;
+    std::vector<void *> owned;
+    double *tvec = nullptr;
+    long long t_size = 0, vec_size = 0;
+    double *ring = nullptr;
+    double *scratch = nullptr;  // residuum / gram / coef
+    int *dinfo = nullptr;
+    double *fdiag_a = nullptr, *fdiag_b = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    double iter_ms = 0.0;
+    // per-op profiling (eager sweeps only): events around every launch
+    int profile = 0;
+    std::vector<cudaEvent_t> pev;
+    double prof_ms[4] = {0, 0, 0, 0};       // gett_f64, gett_split, assemble, other
+    double prof_flops[4] = {0, 0, 0, 0};
+    long long prof_launch[4] = {0, 0, 0, 0};
+    size_t energy_op = 0;
+    double flops = 0.0;
+    long long launches = 0;
+    double sweep_ms = 0.0;
+    int precision = CCQ_B200_PREC_FP64;
+    int nslices = 4;
+    int use_graph = 0;
+    cudaGraphExec_t gexec = nullptr;
+    int device = 0;
+    SplitWorkspace split{};
+
+    void *dalloc(size_t bytes) {
+        void *p = nullptr;
+        CK(cudaMalloc(&p, bytes ? bytes : 8));
+        owned.push_back(p);
+        return p;
+    }
+    ~ccq_b200_ctx() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        split_free(split);
+        for (void *p : owned) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (ev2) cudaEventDestroy(ev2);
+        for (auto e : pev) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+long long tok(const ccq_b200_ctx *c, const std::string &s) {
+    auto it = c->size.find(s);
+    if (it == c->size.end()) throw Error(CCQ_B200_EPLAN, "unknown size token " + s);
+    return it->second;
+}
+
+struct Resolved {
+    double *base;
+    std::map<std::string, long long> stride;   // per label
+    std::map<std::string, long long> extent;
+    std::vector<std::string> order;            // labels in axis order (first occurrence)
+};
+
+Resolved resolve(ccq_b200_ctx *c, const ViewSpec &v) {
+    auto it = c->bufs.find(v.buf);
+    if (it == c->bufs.end()) throw Error(CCQ_B200_EPLAN, "unknown buffer " + v.buf);
+    const DevBuf &b = it->second;
+    if (b.shape.size() != v.axes.size()) throw Error(CCQ_B200_EPLAN, "rank mismatch for " + v.buf);
+    Resolved r;
+    long long off = 0;
+    for (size_t d = 0; d < v.axes.size(); ++d) {
+        const AxisSpec &a = v.axes[d];
+        long long st = tok(c, a.start);
+        long long ex = tok(c, a.size);
+        if (st + ex > b.shape[d]) throw Error(CCQ_B200_EPLAN, "view exceeds buffer " + v.buf);
+        off += st * b.stride[d];
+        if (!r.stride.count(a.label)) {
+            r.order.push_back(a.label);
+            r.stride[a.label] = 0;
+            r.extent[a.label] = ex;
+        }
+        r.stride[a.label] += b.stride[d];
+    }
+    r.base = b.ptr + off;
+    return r;
+}
+
+bool has(const Resolved &r, const std::string &l) { return r.stride.count(l) > 0; }
+
+void build_table(const std::vector<std::string> &labels, const std::map<std::string, long long> &extent,
+                 const Resolved &x, const Resolved *y, std::vector<int> &tx, std::vector<int> &ty) {
+    long long total = 1;
+    for (auto &l : labels) total *= extent.at(l);
+    tx.assign(total, 0);
+    if (y) ty.assign(total, 0);
+    std::vector<long long> idx(labels.size(), 0);
+    for (long long i = 0; i < total; ++i) {
+        long long ox = 0, oy = 0;
+        for (size_t d = 0; d < labels.size(); ++d) {
+            ox += idx[d] * x.stride.at(labels[d]);
+            if (y) oy += idx[d] * y->stride.at(labels[d]);
+        }
+        if (ox > INT32_MAX || oy > INT32_MAX) throw Error(CCQ_B200_ERANGE, "view offset beyond int32");
+        tx[i] = (int)ox;
+        if (y) ty[i] = (int)oy;
+        for (int d = (int)labels.size() - 1; d >= 0; --d) {
+            if (++idx[d] < extent.at(labels[d])) break;
+            idx[d] = 0;
+        }
+    }
+}
+
+void instantiate(ccq_b200_ctx *c) {
+    // ---- buffers -----------------------------------------------------------
+    // amplitude blocks T1..T3 live in t_vec at get_t_sizes offsets
+    static const char *tv_order[] = {"T1A", "T1B", "T2A", "T2B", "T2C", "T3A", "T3B", "T3C", "T3D"};
+    std::map<std::string, long long> tv_off;
+    long long off = 0;
+    std::map<std::string, std::vector<std::string>> bdims;
+    for (auto &b : c->plan.bufs) bdims[b.name] = b.dims;
+    for (auto *nm : tv_order) {
+        auto it = bdims.find(nm);
+        if (it == bdims.end()) throw Error(CCQ_B200_EPLAN, std::string("plan lacks block ") + nm);
+        long long ne = 1;
+        for (auto &d : it->second) ne *= tok(c, d);
+        tv_off[nm] = off;
+        off += ne;
+    }
+    c->t_size = off;
+    c->vec_size = (c->calc_type == "CCSD") ? tv_off["T3A"] : c->t_size;
+    c->tvec = (double *)c->dalloc(sizeof(double) * c->t_size);
+    CK(cudaMemsetAsync(c->tvec, 0, sizeof(double) * c->t_size, c->stream));
+
+    // work buffers: one arena, each phase packs its Z/X buffers from offset 0
+    std::map<std::string, std::string> first_phase;
+    {
+        std::string phase = "init";
+        auto note = [&](const ViewSpec &v) {
+            if (!first_phase.count(v.buf)) first_phase[v.buf] = phase;
+            else if (first_phase[v.buf] != phase && (v.buf[0] == 'Z' || v.buf[0] == 'X'))
+                throw Error(CCQ_B200_EPLAN, "work buffer used across phases: " + v.buf);
+        };
+        for (auto &o : c->plan.ops) {
+            if (o.kind == OP_PHASE) phase = o.arg0 + "#" + std::to_string(&o - &c->plan.ops[0]);
+            if (o.kind == OP_GETT) {
+                note(o.c);
+                note(o.a);
+                note(o.b);
+            }
+            if (o.kind == OP_ASM)
+                for (auto &t : o.terms) note(t.second);
+        }
+    }
+    std::map<std::string, long long> phase_fill;
+    std::map<std::string, long long> work_off;
+    long long arena = 0;
+    for (auto &b : c->plan.bufs) {
+        if (b.kind != "work") continue;
+        long long ne = 1;
+        for (auto &d : b.dims) ne *= tok(c, d);
+        ne = (ne + 31) / 32 * 32;
+        std::string ph = first_phase.count(b.name) ? first_phase[b.name] : "unused";
+        work_off[b.name] = phase_fill[ph];
+        phase_fill[ph] += ne;
+        arena = std::max(arena, phase_fill[ph]);
+    }
+    double *arena_ptr = (double *)c->dalloc(sizeof(double) * std::max(arena, 1LL));
+    for (auto &b : c->plan.bufs) {
+        DevBuf d;
+        for (auto &x : b.dims) d.shape.push_back(tok(c, x));
+        d.stride.assign(d.shape.size(), 1);
+        for (int i = (int)d.shape.size() - 2; i >= 0; --i) d.stride[i] = d.stride[i + 1] * d.shape[i + 1];
+        d.numel = 1;
+        for (auto s : d.shape) d.numel *= s;
+        if (tv_off.count(b.name)) {
+            d.ptr = c->tvec + tv_off[b.name];
+        } else if (b.kind == "work") {
+            d.ptr = arena_ptr + work_off[b.name];
+        } else {
+            d.ptr = (double *)c->dalloc(sizeof(double) * std::max(d.numel, 1LL));
+            CK(cudaMemsetAsync(d.ptr, 0, sizeof(double) * std::max(d.numel, 1LL), c->stream));
+        }
+        c->bufs[b.name] = d;
+    }
+    launch_fill(c->bufs.at("ONES").ptr, 1.0, c->bufs.at("ONES").numel, c->stream);
+
+    // ---- operations ----------------------------------------------------------
+    std::vector<int> itab;
+    struct Pend {
+        size_t op;
+        size_t am, ak, bn, bk, cm, cn;
+    };
+    std::vector<Pend> pend;
+    std::vector<AsmTerm> hterms;
+    std::vector<signed char> hperm, hsign;
+    struct PendA {
+        size_t op, t0, p0;
+    };
+    std::vector<PendA> penda;
+    c->flops = 0.0;
+    for (size_t i = 0; i < c->plan.ops.size(); ++i) {
+        Op &o = c->plan.ops[i];
+        if (o.kind == OP_PHASE && o.arg0 == "energy") c->energy_op = i;
+        if (o.kind == OP_GETT) {
+            Resolved C = resolve(c, o.c), A = resolve(c, o.a), B = resolve(c, o.b);
+            std::vector<std::string> ml, nl, kl;
+            std::map<std::string, long long> ext;
+            for (auto &l : A.order) {
+                ext[l] = A.extent[l];
+                if (has(C, l) && !has(B, l)) ml.push_back(l);
+                else if (has(B, l) && !has(C, l)) kl.push_back(l);
+                else throw Error(CCQ_B200_EPLAN, "label " + l + " of A must be in exactly one of B, C");
+            }
+            for (auto &l : B.order) {
+                ext[l] = B.extent[l];
+                if (has(C, l) && !has(A, l)) nl.push_back(l);
+                else if (!has(A, l)) throw Error(CCQ_B200_EPLAN, "dangling label " + l);
+            }
+            for (auto &l : C.order)
+                if (!has(A, l) && !has(B, l)) throw Error(CCQ_B200_EPLAN, "output label not produced: " + l);
+            std::vector<int> am, ak, bn, bk, cm, cn;
+            build_table(ml, ext, A, &C, am, cm);
+            build_table(kl, ext, A, &B, ak, bk);
+            build_table(nl, ext, B, &C, bn, cn);
+            Pend p{i, itab.size(), 0, 0, 0, 0, 0};
+            itab.insert(itab.end(), am.begin(), am.end());
+            p.ak = itab.size();
+            itab.insert(itab.end(), ak.begin(), ak.end());
+            p.bn = itab.size();
+            itab.insert(itab.end(), bn.begin(), bn.end());
+            p.bk = itab.size();
+            itab.insert(itab.end(), bk.begin(), bk.end());
+            p.cm = itab.size();
+            itab.insert(itab.end(), cm.begin(), cm.end());
+            p.cn = itab.size();
+            itab.insert(itab.end(), cn.begin(), cn.end());
+            pend.push_back(p);
+            long long M = (long long)am.size(), N = (long long)bn.size(), K = (long long)ak.size();
+            if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) throw Error(CCQ_B200_ERANGE, "GETT too large");
+            o.mnk[0] = M;
+            o.mnk[1] = N;
+            o.mnk[2] = K;
+            c->flops += 2.0 * M * N * K;
+            auto kmajor = [](const Resolved &X, const std::vector<std::string> &mm, const std::vector<std::string> &kk) {
+                long long sk = kk.empty() ? (1LL << 40) : X.stride.at(kk.back());
+                long long sm = mm.empty() ? (1LL << 40) : X.stride.at(mm.back());
+                return sk <= sm ? 1 : 0;
+            };
+            o.akm = kmajor(A, ml, kl);
+            o.bkm = kmajor(B, nl, kl);
+            o.g.A = A.base;
+            o.g.B = B.base;
+            o.g.C = C.base;
+            o.g.M = (int)M;
+            o.g.N = (int)N;
+            o.g.K = (int)K;
+            o.g.alpha = o.alpha;
+            o.g.beta = o.beta;
+            long long tiles = ((M + 63) / 64) * ((N + 63) / 64);
+            int splits = 1;
+            if (tiles < 296 && K >= 128) {
+                long long want = (296 + tiles - 1) / tiles;
+                long long maxs = (K + 63) / 64;
+                splits = (int)std::min<long long>(std::min<long long>(want, maxs), 128);
+                if (splits < 1) splits = 1;
+            }
+            long long chunk = (K + splits - 1) / splits;
+            chunk = (chunk + 15) / 16 * 16;
+            if (chunk < 16) chunk = 16;
+            o.g.kchunk = (int)chunk;
+            o.zero_first = (K + chunk - 1) / chunk > 1 && o.beta == 0;
+            if (K == 0) o.g.kchunk = 16;
+            o.split = o.tag.size() > 2 && o.tag[0] == 'T' && (o.tag[1] == '3' || o.tag[1] == '4');
+        } else if (o.kind == OP_ASM) {
+            auto it = c->bufs.find(o.block);
+            if (it == c->bufs.end()) throw Error(CCQ_B200_EPLAN, "assemble target " + o.block);
+            const DevBuf &T = it->second;
+            AsmArgs &a = o.asmargs;
+            int level = o.block[1] - '0';
+            int nb = (int)(strchr("ABCDE", o.block[2]) - "ABCDE");
+            a.level = level;
+            a.rank = 2 * level;
+            if (a.rank > MAXR || (int)T.shape.size() != a.rank) throw Error(CCQ_B200_EPLAN, "block rank");
+            std::vector<int> spins(level);
+            for (int k = 0; k < level; ++k) spins[k] = k < level - nb ? 0 : 1;
+            a.total = 1;
+            for (int d = 0; d < a.rank; ++d) {
+                a.dims[d] = (int)T.shape[d];
+                a.tstride[d] = (int)T.stride[d];
+                a.spin[d] = spins[d % level];
+                a.runstart[d] = (d % level == 0) || spins[d % level] != spins[d % level - 1];
+                a.total *= T.shape[d];
+            }
+            a.T = T.ptr;
+            a.fdiag[0] = c->fdiag_a;
+            a.fdiag[1] = c->fdiag_b;
+            a.nocc[0] = (int)c->oa;
+            a.nocc[1] = (int)c->ob;
+            a.shift = c->shift;
+            a.mode = o.mode == "jacobi" ? 0 : 1;
+            std::vector<std::string> target;
+            for (int k = 0; k < level; ++k) target.push_back("i" + std::to_string(k));
+            for (int k = 0; k < level; ++k) target.push_back("a" + std::to_string(k));
+            PendA pa{i, hterms.size(), hperm.size()};
+            for (auto &t : o.terms) {
+                Resolved V = resolve(c, t.second);
+                AsmTerm at{};
+                at.p = V.base;
+                at.coef = t.first;
+                for (int d = 0; d < a.rank; ++d) {
+                    auto s = V.stride.find(target[d]);
+                    at.stride[d] = s == V.stride.end() ? 0 : (int)s->second;
+                }
+                hterms.push_back(at);
+            }
+            a.nterms = (int)o.terms.size();
+            if (a.nterms > MAX_TERMS) throw Error(CCQ_B200_EPLAN, "too many assemble terms");
+            // orbit permutations: within same-spin runs of each half
+            std::vector<std::vector<int>> runs;
+            for (int half = 0; half < 2; ++half) {
+                int d = half * level;
+                while (d < (half + 1) * level) {
+                    int e = d + 1;
+                    while (e < (half + 1) * level && spins[e % level] == spins[d % level]) ++e;
+                    std::vector<int> r;
+                    for (int q = d; q < e; ++q) r.push_back(q);
+                    runs.push_back(r);
+                    d = e;
+                }
+            }
+            std::vector<std::vector<std::pair<std::vector<int>, int>>> rp;
+            for (auto &r : runs) {
+                std::vector<int> p(r.size());
+                for (size_t q = 0; q < r.size(); ++q) p[q] = (int)q;
+                std::vector<std::pair<std::vector<int>, int>> lst;
+                do {
+                    int sg = 1;
+                    for (size_t x = 0; x < p.size(); ++x)
+                        for (size_t y = x + 1; y < p.size(); ++y)
+                            if (p[y] < p[x]) sg = -sg;
+                    lst.push_back({p, sg});
+                } while (std::next_permutation(p.begin(), p.end()));
+                rp.push_back(lst);
+            }
+            std::vector<size_t> cur(rp.size(), 0);
+            int np = 0;
+            while (true) {
+                std::vector<signed char> P(a.rank);
+                int sg = 1;
+                for (size_t r = 0; r < runs.size(); ++r) {
+                    auto &pr = rp[r][cur[r]];
+                    sg *= pr.second;
+                    for (size_t q = 0; q < runs[r].size(); ++q) P[runs[r][q]] = (signed char)runs[r][pr.first[q]];
+                }
+                hperm.insert(hperm.end(), P.begin(), P.end());
+                hsign.push_back((signed char)sg);
+                ++np;
+                size_t r = 0;
+                while (r < rp.size() && ++cur[r] == rp[r].size()) cur[r++] = 0;
+                if (r == rp.size()) break;
+            }
+            a.nperm = np;
+            penda.push_back(pa);
+        }
+    }
+    int *dtab = (int *)c->dalloc(sizeof(int) * std::max<size_t>(itab.size(), 1));
+    CK(cudaMemcpyAsync(dtab, itab.data(), sizeof(int) * itab.size(), cudaMemcpyHostToDevice, c->stream));
+    for (auto &p : pend) {
+        Op &o = c->plan.ops[p.op];
+        o.g.offA_m = dtab + p.am;
+        o.g.offA_k = dtab + p.ak;
+        o.g.offB_n = dtab + p.bn;
+        o.g.offB_k = dtab + p.bk;
+        o.g.offC_m = dtab + p.cm;
+        o.g.offC_n = dtab + p.cn;
+    }
+    AsmTerm *dterms = (AsmTerm *)c->dalloc(sizeof(AsmTerm) * std::max<size_t>(hterms.size(), 1));
+    CK(cudaMemcpyAsync(dterms, hterms.data(), sizeof(AsmTerm) * hterms.size(), cudaMemcpyHostToDevice, c->stream));
+    signed char *dperm = (signed char *)c->dalloc(std::max<size_t>(hperm.size(), 1));
+    signed char *dsign = (signed char *)c->dalloc(std::max<size_t>(hsign.size(), 1));
+    CK(cudaMemcpyAsync(dperm, hperm.data(), hperm.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dsign, hsign.data(), hsign.size(), cudaMemcpyHostToDevice, c->stream));
+    {
+        size_t signs_before = 0;
+        for (auto &p : penda) {
+            Op &o = c->plan.ops[p.op];
+            o.asmargs.terms = dterms + p.t0;
+            o.asmargs.perm = dperm + p.p0;
+            o.asmargs.psign = dsign + signs_before;
+            signs_before += o.asmargs.nperm;
+        }
+    }
+    // ring and scratch
+    c->ring = (double *)c->dalloc(sizeof(double) * (size_t)(c->ds + 1) * std::max(c->vec_size, 1LL));
+    c->scratch = (double *)c->dalloc(sizeof(double) * 512);
+    c->dinfo = (int *)c->dalloc(sizeof(int) * 4);
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+int op_class(const ccq_b200_ctx *c, const Op &o) {
+    if (o.kind == OP_GETT) return (c->precision == CCQ_B200_PREC_SPLIT && o.split) ? 1 : 0;
+    if (o.kind == OP_ASM) return 2;
+    return 3;
+}
+
+void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
+    bool prof = c->profile != 0;
+    if (prof && c->pev.size() < 2 * c->plan.ops.size()) {
+        for (auto e : c->pev) cudaEventDestroy(e);
+        c->pev.assign(2 * c->plan.ops.size(), nullptr);
+        for (auto &e : c->pev) CK(cudaEventCreate(&e));
+    }
+    for (size_t i = from; i < to; ++i) {
+        Op &o = c->plan.ops[i];
+        if (prof) CK(cudaEventRecord(c->pev[2 * i], c->stream));
+        switch (o.kind) {
+            case OP_GETT:
+                if (o.g.M == 0 || o.g.N == 0) break;
+                if (o.zero_first) {
+                    launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, c->stream);
+                    ++c->launches;
+                }
+                if (o.g.K == 0) {
+                    if (!o.beta) {
+                        launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, c->stream);
+                        ++c->launches;
+                    }
+                    break;
+                }
+                if (c->precision == CCQ_B200_PREC_SPLIT && o.split) {
+                    c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, c->stream);
+                } else {
+                    launch_gett_f64(o.g, o.akm, o.bkm, c->stream);
+                    ++c->launches;
+                }
+                break;
+            case OP_ASM:
+                launch_assemble(o.asmargs, c->stream);
+                ++c->launches;
+                break;
+            case OP_COPY: {
+                DevBuf &d = c->bufs.at(o.arg0);
+                DevBuf &s = c->bufs.at(o.arg1);
+                if (d.numel != s.numel) throw Error(CCQ_B200_EPLAN, "COPY size mismatch");
+                CK(cudaMemcpyAsync(d.ptr, s.ptr, sizeof(double) * d.numel, cudaMemcpyDeviceToDevice, c->stream));
+                break;
+            }
+            case OP_ZERO: {
+                DevBuf &d = c->bufs.at(o.arg0);
+                CK(cudaMemsetAsync(d.ptr, 0, sizeof(double) * std::max(d.numel, 1LL), c->stream));
+                break;
+            }
+            case OP_PHASE:
+                break;
+        }
+        if (prof) CK(cudaEventRecord(c->pev[2 * i + 1], c->stream));
+    }
+    CK(cudaGetLastError());
+    if (prof) {
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t i = from; i < to; ++i) {
+            Op &o = c->plan.ops[i];
+            if (o.kind == OP_PHASE) continue;
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->pev[2 * i], c->pev[2 * i + 1]));
+            int k = op_class(c, o);
+            c->prof_ms[k] += ms;
+            c->prof_launch[k] += 1;
+            if (o.kind == OP_GETT) c->prof_flops[k] += 2.0 * o.mnk[0] * o.mnk[1] * o.mnk[2];
+        }
+    }
+}
+
+void sweep(ccq_b200_ctx *c) {
+    if (c->use_graph && !c->profile) {
+        if (!c->gexec) {
+            cudaGraph_t g;
+            long long l0 = c->launches;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                run_ops(c, 0, c->plan.ops.size());
+            } catch (...) {
+                cudaStreamEndCapture(c->stream, &g);
+                throw;
+            }
+            CK(cudaStreamEndCapture(c->stream, &g));
+            CK(cudaGraphInstantiate(&c->gexec, g, 0));
+            CK(cudaGraphDestroy(g));
+            c->launches = l0 + (c->launches - l0);
+        }
+        CK(cudaGraphLaunch(c->gexec, c->stream));
+    } else {
+        run_ops(c, 0, c->plan.ops.size());
+    }
+}
+
+long long count_sweep_launches(ccq_b200_ctx *c) {
+    long long n = 0;
+    for (auto &o : c->plan.ops) {
+        if (o.kind == OP_GETT && o.g.M && o.g.N) {
+            if (o.zero_first || o.g.K == 0) ++n;
+            if (o.g.K) n += (c->precision == CCQ_B200_PREC_SPLIT && o.split) ? split_launch_count(o.g, c->nslices) : 1;
+        } else if (o.kind == OP_ASM) {
+            ++n;
+        }
+    }
+    return n;
+}
+
+// Fortran column-major (n,n,n,n) -> C-order [p][q][r][s] of v(p,q,r,s)
+void fortran4_to_c(const double *f, std::vector<double> &out, long long n) {
+    out.resize((size_t)(n * n * n * n));
+    for (long long s = 0; s < n; ++s)
+        for (long long r = 0; r < n; ++r)
+            for (long long q = 0; q < n; ++q)
+                for (long long p = 0; p < n; ++p) out[((p * n + q) * n + r) * n + s] = f[p + n * (q + n * (r + n * s))];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int ccq_b200_last_error(char *buf, int64_t len) {
+    if (!buf || len <= 0) return CCQ_B200_EINVAL;
+    snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+    return 0;
+}
+
+int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
+                  const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
+                  int64_t diis_space, ccq_b200_ctx **out) {
+    ccq_b200_ctx *c = nullptr;
+    try {
+        if (!dims || !calc_type || !f_a || !f_b || !v_aa || !v_ab || !v_bb || !out)
+            throw Error(CCQ_B200_EINVAL, "null argument");
+        *out = nullptr;
+        if (diis_space < 1 || diis_space > 12) throw Error(CCQ_B200_EINVAL, "diis_space must be in 1..12");
+        long long fr = dims->froz, oa = dims->occ_a - fr, ob = dims->occ_b - fr;
+        long long va = dims->orbs - dims->occ_a, vb = dims->orbs - dims->occ_b, n = dims->orbs - fr;
+        if (fr < 0 || oa < 1 || ob < 1 || va < 1 || vb < 1)
+            throw Error(CCQ_B200_EINVAL, "invalid dimensions (need at least one occupied and virtual per spin)");
+        std::string ct(calc_type);
+        if (ct != "CCSD" && ct != "CCSDT" && ct != "CCSDTQ")
+            throw Error(CCQ_B200_EINVAL, "calc_type must be CCSD, CCSDT or CCSDTQ");
+        if (rhf && oa != ob) throw Error(CCQ_B200_EINVAL, "rhf requires occ_a == occ_b");
+        const char *text = find_plan(ct, rhf != 0);
+        if (!text) throw Error(CCQ_B200_EPLAN, "no plan for " + ct);
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(CCQ_B200_ENODEV, "no CUDA device");
+        c = new ccq_b200_ctx();
+        CK(cudaGetDevice(&c->device));
+        c->calc_type = ct;
+        c->rhf = rhf != 0;
+        c->shift = shift;
+        c->ds = (int)diis_space;
+        c->oa = oa;
+        c->ob = ob;
+        c->va = va;
+        c->vb = vb;
+        c->n = n;
+        c->froz = fr;
+        c->size = {{"oa", oa}, {"ob", ob}, {"va", va}, {"vb", vb}, {"n", n}, {"1", 1}, {"0", 0}};
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&c->ev0));
+        CK(cudaEventCreate(&c->ev1));
+        CK(cudaEventCreate(&c->ev2));
+        c->plan = parse_plan(text);
+        // host-side integral preparation
+        long long orbs = dims->orbs;
+        std::vector<double> FA(n * n), FB(n * n);
+        for (long long p = 0; p < n; ++p)
+            for (long long q = 0; q < n; ++q) {
+                FA[p * n + q] = f_a[(p + fr) + orbs * (q + fr)];
+                FB[p * n + q] = f_b[(p + fr) + orbs * (q + fr)];
+            }
+        std::vector<double> VAA, VAB, VBB;
+        fortran4_to_c(v_aa, VAA, n);
+        fortran4_to_c(v_ab, VAB, n);
+        fortran4_to_c(v_bb, VBB, n);
+        std::vector<double> HA(FA), HB(FB);
+        auto V = [&](const std::vector<double> &x, long long p, long long q, long long r, long long s) {
+            return x[((p * n + q) * n + r) * n + s];
+        };
+        for (long long p = 0; p < n; ++p)
+            for (long long q = 0; q < n; ++q) {
+                double a = 0, b = 0;
+                for (long long i = 0; i < oa; ++i) a += V(VAA, p, i, q, i);
+                for (long long i = 0; i < ob; ++i) a += V(VAB, p, i, q, i);
+                for (long long i = 0; i < ob; ++i) b += V(VBB, p, i, q, i);
+                for (long long i = 0; i < oa; ++i) b += V(VAB, i, p, i, q);
+                HA[p * n + q] -= a;
+                HB[p * n + q] -= b;
+            }
+        std::vector<double> da(n), db(n);
+        for (long long p = 0; p < n; ++p) {
+            da[p] = FA[p * n + p];
+            db[p] = FB[p * n + p];
+        }
+        c->fdiag_a = (double *)c->dalloc(sizeof(double) * n);
+        c->fdiag_b = (double *)c->dalloc(sizeof(double) * n);
+        CK(cudaMemcpy(c->fdiag_a, da.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->fdiag_b, db.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        instantiate(c);
+        auto up = [&](const char *name, const std::vector<double> &h) {
+            DevBuf &d = c->bufs.at(name);
+            if ((size_t)d.numel != h.size()) throw Error(CCQ_B200_EPLAN, std::string("size of ") + name);
+            CK(cudaMemcpy(d.ptr, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+        };
+        up("FA0", FA);
+        up("FB0", FB);
+        up("HA0", HA);
+        up("HB0", HB);
+        up("VAA0", VAA);
+        up("VAB0", VAB);
+        up("VBB0", VBB);
+        CK(cudaDeviceSynchronize());
+        *out = c;
+        return 0;
+    } catch (const Error &e) {
+        delete c;
+        return fail(e);
+    } catch (const std::exception &e) {
+        delete c;
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_sizes(const ccq_b200_ctx *c, int64_t *t_size, int64_t *vec_size) {
+    if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
+    if (t_size) *t_size = c->t_size;
+    if (vec_size) *vec_size = c->vec_size;
+    return 0;
+}
+
+int ccq_b200_set_t(ccq_b200_ctx *c, const double *t, int64_t n) {
+    try {
+        if (!c || !t || n != c->t_size) throw Error(CCQ_B200_EINVAL, "set_t: size must equal t_size");
+        CK(cudaMemcpyAsync(c->tvec, t, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_get_t(const ccq_b200_ctx *c, double *t, int64_t n) {
+    try {
+        if (!c || !t || n != c->t_size) throw Error(CCQ_B200_EINVAL, "get_t: size must equal t_size");
+        CK(cudaMemcpyAsync(t, c->tvec, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_update(ccq_b200_ctx *c) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        CK(cudaSetDevice(c->device));
+        run_ops(c, 0, c->energy_op);
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_energy(ccq_b200_ctx *c, double *e) {
+    try {
+        if (!c || !e) throw Error(CCQ_B200_EINVAL, "null argument");
+        CK(cudaSetDevice(c->device));
+        run_ops(c, c->energy_op, c->plan.ops.size());
+        CK(cudaMemcpyAsync(e, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e2) {
+        return fail(e2);
+    } catch (const std::exception &e2) {
+        return fail(Error(CCQ_B200_EINVAL, e2.what()));
+    }
+}
+
+int ccq_b200_iterate(ccq_b200_ctx *c, int64_t iter, double *e_cor, double *res, int64_t *did_diis) {
+    try {
+        if (!c || iter < 1) throw Error(CCQ_B200_EINVAL, "iterate: bad argument");
+        CK(cudaSetDevice(c->device));
+        c->launches = 0;
+        CK(cudaEventRecord(c->ev0, c->stream));
+        sweep(c);
+        CK(cudaEventRecord(c->ev1, c->stream));
+        c->launches = count_sweep_launches(c);
+        int ds = c->ds;
+        long long vs = c->vec_size;
+        auto slot = [&](long long it) {
+            long long s = it % (ds + 1);
+            return s == 0 ? ds + 1 : s;
+        };
+        double *cur = c->ring + (slot(iter) - 1) * vs;
+        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
+        const double *prev = iter == 1 ? nullptr : c->ring + (slot(iter - 1) - 1) * vs;
+        launch_sqdiff(prev, cur, vs, c->scratch, c->stream);
+        c->launches += 1;
+        int diis = (iter % (ds + 1)) == 0;
+        if (diis) {
+            launch_diis_gram(c->ring, vs, ds, vs, c->scratch + 8, c->stream);
+            launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
+            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
+            c->launches += 3;
+        }
+        CK(cudaEventRecord(c->ev2, c->stream));
+        double hs[2];
+        int info = 0;
+        CK(cudaMemcpyAsync(&hs[0], c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&hs[1], c->scratch, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (diis) CK(cudaMemcpyAsync(&info, c->dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->sweep_ms = ms;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev2));
+        c->iter_ms = ms;
+        if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
+        if (e_cor) *e_cor = hs[0];
+        if (res) *res = std::sqrt(std::sqrt(hs[1]));
+        if (did_diis) *did_diis = diis;
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        if (mode != CCQ_B200_PREC_FP64 && mode != CCQ_B200_PREC_SPLIT) throw Error(CCQ_B200_EINVAL, "precision mode");
+        if (mode == CCQ_B200_PREC_SPLIT && (nslices < 2 || nslices > MAX_SLICES))
+            throw Error(CCQ_B200_EINVAL, "nslices out of range");
+        if (mode == CCQ_B200_PREC_SPLIT) split_reserve(c->split, c->plan.ops.size() ? [&] {
+            long long ma = 0, mb = 0, mc = 0;
+            for (auto &o : c->plan.ops)
+                if (o.kind == OP_GETT && o.split) {
+                    ma = std::max(ma, o.mnk[0] * ((o.mnk[2] + 127) / 128 * 128));
+                    mb = std::max(mb, o.mnk[1] * ((o.mnk[2] + 127) / 128 * 128));
+                    mc = std::max(mc, o.mnk[0] + o.mnk[1]);
+                }
+            return SplitSizes{ma, mb, mc};
+        }() : SplitSizes{0, 0, 0}, (int)nslices);
+        if (c->gexec) {
+            cudaGraphExecDestroy(c->gexec);
+            c->gexec = nullptr;
+        }
+        c->precision = (int)mode;
+        c->nslices = (int)nslices;
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_use_graph(ccq_b200_ctx *c, int64_t enable) {
+    if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
+    c->use_graph = enable != 0;
+    return 0;
+}
+
+int ccq_b200_stats(const ccq_b200_ctx *c, int64_t *launches, double *flops, double *sweep_ms) {
+    if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
+    if (launches) *launches = c->launches;
+    if (flops) *flops = c->flops;
+    if (sweep_ms) *sweep_ms = c->sweep_ms;
+    return 0;
+}
+
+int ccq_b200_timing(const ccq_b200_ctx *c, double *sweep_ms, double *iter_ms) {
+    if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
+    if (sweep_ms) *sweep_ms = c->sweep_ms;
+    if (iter_ms) *iter_ms = c->iter_ms;
+    return 0;
+}
+
+int ccq_b200_profile(ccq_b200_ctx *c, int64_t enable) {
+    if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
+    c->profile = enable != 0;
+    for (int k = 0; k < 4; ++k) {
+        c->prof_ms[k] = 0;
+        c->prof_flops[k] = 0;
+        c->prof_launch[k] = 0;
+    }
+    return 0;
+}
+
+int ccq_b200_profile_get(const ccq_b200_ctx *c, int64_t kind, double *ms, double *flops, int64_t *launches) {
+    if (!c || kind < 0 || kind > 3) return fail(Error(CCQ_B200_EINVAL, "profile_get: bad argument"));
+    if (ms) *ms = c->prof_ms[kind];
+    if (flops) *flops = c->prof_flops[kind];
+    if (launches) *launches = c->prof_launch[kind];
+    return 0;
+}
+
+int ccq_b200_free(ccq_b200_ctx *c) {
+    delete c;
+    return 0;
+}
+
+}  // extern "C"

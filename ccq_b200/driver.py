@@ -1,0 +1,132 @@
+"""ccq-compatible driver on the resident GPU solver.
+
+Keeps the reference's outer program and replaces only the amplitude update
+underneath it:
+  * ``run``            <- ``run_calcs``/``init_system`` (``src/calc_driver.f90:11-141``)
+  * ``solve_cc``       <- ``solve_cc`` + ``jacobi_iter`` (``src/solve_cc.f90:12-269``):
+    update, energy, ring write, residuum and DIIS every ``diis_space+1``
+    iterations (inside ``Context.iterate``), the iteration table, the
+    ``cc.comm`` stop file, NaN and max-iteration exits, and convergence when
+    the last three |dE| are below tol (``:293-316``)
+  * printing           <- ``print_iter_head``/``print_iteration``/``print_summary``
+    (``src/printing.F90:260-349``)
+
+Usage: ``python -m ccq_b200.driver input.inp``.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import config as cfgmod
+from . import integrals as I
+from . import lib
+
+
+class Result:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def print_iter_head(out):
+    out(f"\n  {'It.':>4}{'E (Corr)':>15}{'dE':>15}{'Residuum':>15}{'Wall Time':>16}")
+    out('  ' + '-' * 65)
+
+
+def print_iteration(out, it, ecor, de, res, secs):
+    nmin = int(secs) // 60
+    nsec = secs - nmin * 60.0
+    out(f'  {it:4d}{ecor:15.10f}{de:15.10f}{res:15.10f}{nmin:5d} min{nsec:5.1f} s')
+
+
+def solve_cc(ctx, cfg, out=print, precision=None):
+    """jacobi_iter on the device.  Returns a Result with energies and timings."""
+    prec = precision or cfg.gpu_precision
+    split = prec == 'split'
+    ctx.set_precision(lib.PREC_SPLIT if split else lib.PREC_FP64, cfg.gpu_slices)
+    ctx.use_graph(cfg.gpu_graph)
+    conv = [1.0, 1.0, 1.0]
+    en_cor = 0.0
+    failed = False
+    hist = []
+    prev = time.time()
+    print_iter_head(out)
+    it = 0
+    fp64_iters = 0
+    for it in range(1, cfg.max_iter + 1):
+        e_new, res, did = ctx.iterate(it)
+        st = ctx.stats()
+        diff = en_cor - e_new
+        conv = [conv[1], conv[2], diff]
+        en_cor = e_new
+        if did:
+            out('      DIIS cycle')
+        now = time.time()
+        print_iteration(out, it, e_new, diff, res, now - prev)
+        hist.append(dict(e=e_new, de=diff, res=res, ms=st['sweep_ms'], split=split, launches=st['launches']))
+        prev = now
+        if not split:
+            fp64_iters += 1
+        if os.path.exists('cc.comm'):
+            os.remove('cc.comm')
+            out('Signaled to end')
+            break
+        if split and abs(diff) < cfg.gpu_fp64_finish:
+            # hand over to FP64: the remaining iterations converge the exact equations
+            split = False
+            ctx.set_precision(lib.PREC_FP64, cfg.gpu_slices)
+            out('      FP64 finish')
+        if not split and fp64_iters >= 3 and all(abs(c) < cfg.tol for c in conv):
+            break
+        if math.isnan(e_new):
+            out('FAILED TO CONVERGE')
+            failed = True
+            break
+        if it == cfg.max_iter:
+            out(f'FAILED TO CONVERGE IN {cfg.max_iter} ITERATIONS. KEEPING LAST T VECTOR.')
+            failed = True
+    return Result(e_cor=en_cor, iterations=it, failed=failed, history=hist)
+
+
+def load_system(cfg, base_dir='.'):
+    def path(p):
+        return p if os.path.isabs(p) else os.path.join(base_dir, p)
+    e1 = I.read_onebody(path(cfg.onebody), cfg.orbs)
+    e2, enuc = I.read_twobody(path(cfg.twobody), cfg.orbs)
+    fa, fb = I.fock(e1, e2, cfg.occ_a, cfg.occ_b)
+    vaa, vab, vbb = I.spin_blocks(e2, cfg.froz)
+    eref = I.hf_energy(e1, e2, cfg.occ_a, cfg.occ_b) + enuc
+    return dict(f_a=fa, f_b=fb, v_aa=vaa, v_ab=vab, v_bb=vbb, e_ref=eref)
+
+
+def run(input_path, out=print, base_dir='.'):
+    cfg = cfgmod.parse(input_path).calc_macros()
+    sysd = load_system(cfg, base_dir)
+    out('Calculation parameters: ' + cfgmod.format_config(cfg))
+    out(f"  Reference energy {sysd['e_ref']:.12f}")
+    out('Coupled cluster')
+    out('---------------')
+    ctx = lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, cfg.calc_type, sysd['f_a'], sysd['f_b'],
+                      sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
+                      diis_space=cfg.diis_space)
+    try:
+        r = solve_cc(ctx, cfg, out)
+    finally:
+        ctx.close()
+    out('\nCalculation Summary (Eh)')
+    out('------------------------')
+    out(f"{'Reference':>20}{sysd['e_ref']:18.12f}")
+    out(f"{'Correlation':>20}{r.e_cor:18.12f}")
+    out(f"{cfg.calc_type:>20}{sysd['e_ref'] + r.e_cor:18.12f}")
+    r.e_ref = sysd['e_ref']
+    r.e_total = sysd['e_ref'] + r.e_cor
+    return r
+
+
+if __name__ == '__main__':
+    res = run(sys.argv[1])
+    sys.exit(1 if res.failed else 0)

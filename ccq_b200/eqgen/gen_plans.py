@@ -1,0 +1,28 @@
+"""Regenerate the committed contraction plans (``ccq_b200/plans/*.plan``).
+
+    python -m ccq_b200.eqgen.gen_plans [CCSD CCSDT CCSDTQ]
+
+CCSDTQ takes several minutes (the level-4 antisymmetriser search).
+"""
+import os
+import sys
+
+from .plan import build_plan
+
+HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def main(methods):
+    out = os.path.join(HERE, 'plans')
+    os.makedirs(out, exist_ok=True)
+    for m in methods:
+        for rhf in (False, True):
+            p = build_plan(m, rhf)
+            name = m + ('_rhf' if rhf else '')
+            with open(os.path.join(out, name + '.plan'), 'w') as fh:
+                fh.write(p.text())
+            print(name, len(p.ops), 'ops', f'{p.flops:.3e} FLOP at 40 orbitals')
+
+
+if __name__ == '__main__':
+    main(sys.argv[1:] or ['CCSD', 'CCSDT', 'CCSDTQ'])

@@ -1,0 +1,497 @@
+"""Plan compiler: spin-orbital residuals -> spin-blocked contraction plan.
+
+The reference's generated update routines (``src/cc/t*_update.f90``) are,
+per spin block, sequences of ``reorder_shift``/``reorder_stripe`` (permute a
+slice), ``egemm`` (``dgemm('t','n')``), ``sum_stripe`` (permuted accumulate)
+and a closing Jacobi step.  This compiler produces the same kind of sequence
+as data: every diagram becomes one or more GETT operations (a GEMM whose
+operands and result are strided, permuted views of resident tensors, so no
+permute copies are made), every antisymmetriser becomes a list of permuted
+views read by the block's closing ASSEMBLE (residual gather + Jacobi + fill).
+
+Spin integration: each spin-orbital label gets a spin; external spins are
+fixed by the target block, dummy spins are summed; every factor is mapped to
+its stored spin block (v_aa, v_ab, v_bb, T2A, T2B, ...) with the index
+permutation and sign of the canonical (alpha-first) ordering.
+
+The plan is symbolic in the dimension tokens ``oa ob va vb n`` and is
+serialised as text; ``libccq_b200`` instantiates it for concrete sizes.
+"""
+from __future__ import annotations
+
+import itertools
+from dataclasses import dataclass, field
+from fractions import Fraction
+
+from . import wick
+
+SIZE = {('o', 0): 'oa', ('o', 1): 'ob', ('v', 0): 'va', ('v', 1): 'vb'}
+START = {('o', 0): '0', ('o', 1): '0', ('v', 0): 'oa', ('v', 1): 'ob'}
+
+
+def _sp(label):
+    return 'o' if label[0] in 'io' else 'v'
+
+
+@dataclass
+class Axis:
+    label: str
+    size: str
+    start: str = '0'
+
+    def text(self):
+        s = f'{self.label}:{self.size}'
+        if self.start != '0':
+            s += f'@{self.start}'
+        return s
+
+
+@dataclass
+class View:
+    buf: str
+    axes: list
+
+    def text(self):
+        return f"{self.buf}[{','.join(a.text() for a in self.axes)}]"
+
+    def labels(self):
+        return [a.label for a in self.axes]
+
+
+@dataclass
+class Gett:
+    c: View
+    a: View
+    b: View
+    alpha: float
+    beta: int
+    tag: str = ''
+
+    def text(self):
+        return f'GETT {self.alpha!r} {self.beta} {self.c.text()} {self.a.text()} {self.b.text()} {self.tag}'.rstrip()
+
+
+@dataclass
+class Assemble:
+    block: str
+    mode: str                 # 'jacobi' or 'copy'
+    terms: list = field(default_factory=list)   # (coef, View with target labels)
+
+    def text(self):
+        out = [f'ASSEMBLE {self.block} {self.mode} {len(self.terms)}']
+        for c, v in self.terms:
+            out.append(f'TERM {float(c)!r} {v.text()}')
+        return '\n'.join(out)
+
+
+@dataclass
+class Simple:
+    kind: str
+    args: tuple
+
+    def text(self):
+        return ' '.join([self.kind] + [str(a) for a in self.args])
+
+
+BLOCK_DIMS = {
+    'T1A': ('oa', 'va'), 'T1B': ('ob', 'vb'),
+    'T2A': ('oa', 'oa', 'va', 'va'), 'T2B': ('oa', 'ob', 'va', 'vb'), 'T2C': ('ob', 'ob', 'vb', 'vb'),
+    'T3A': ('oa', 'oa', 'oa', 'va', 'va', 'va'), 'T3B': ('oa', 'oa', 'ob', 'va', 'va', 'vb'),
+    'T3C': ('oa', 'ob', 'ob', 'va', 'vb', 'vb'), 'T3D': ('ob', 'ob', 'ob', 'vb', 'vb', 'vb'),
+    'T4A': ('oa',) * 4 + ('va',) * 4, 'T4B': ('oa', 'oa', 'oa', 'ob', 'va', 'va', 'va', 'vb'),
+    'T4C': ('oa', 'oa', 'ob', 'ob', 'va', 'va', 'vb', 'vb'), 'T4D': ('oa', 'ob', 'ob', 'ob', 'va', 'vb', 'vb', 'vb'),
+    'T4E': ('ob',) * 4 + ('vb',) * 4,
+}
+
+
+def block_spins(name):
+    n = int(name[1])
+    nb = 'ABCDE'.index(name[2])
+    return [0] * (n - nb) + [1] * nb
+
+
+def _psign(p):
+    s = 1
+    p = list(p)
+    for i in range(len(p)):
+        for j in range(i + 1, len(p)):
+            if p[j] < p[i]:
+                s = -s
+    return s
+
+
+def _stable_spin_sort(labels, spin):
+    order = sorted(range(len(labels)), key=lambda k: spin[labels[k]])
+    return [labels[k] for k in order], _psign(order)
+
+
+def map_factor(name, labels, spin, undressed=False):
+    """Stored view of one spin-orbital factor for a spin assignment, or None.
+
+    Returns (sign, View) with axes labelled by the term's labels.
+    """
+    def ax(l):
+        key = (_sp(l), spin[l])
+        return Axis(l, SIZE[key], START[key])
+
+    if name == 'f':
+        p, q = labels
+        if spin[p] != spin[q]:
+            return None
+        buf = ('FA' if spin[p] == 0 else 'FB') + ('0' if undressed else '')
+        return 1, View(buf, [ax(p), ax(q)])
+    if name == 'v':
+        p, q, r, s = labels
+        sp = (spin[p], spin[q], spin[r], spin[s])
+        z = '0' if undressed else ''
+        if sp == (0, 0, 0, 0):
+            return 1, View('VAA' + z, [ax(p), ax(q), ax(r), ax(s)])
+        if sp == (1, 1, 1, 1):
+            return 1, View('VBB' + z, [ax(p), ax(q), ax(r), ax(s)])
+        if sp == (0, 1, 0, 1):
+            return 1, View('VAB' + z, [ax(p), ax(q), ax(r), ax(s)])
+        if sp == (1, 0, 1, 0):
+            return 1, View('VAB' + z, [ax(q), ax(p), ax(s), ax(r)])
+        if sp == (0, 1, 1, 0):
+            return -1, View('VAB' + z, [ax(p), ax(q), ax(s), ax(r)])
+        if sp == (1, 0, 0, 1):
+            return -1, View('VAB' + z, [ax(q), ax(p), ax(r), ax(s)])
+        return None
+    # amplitudes: (vir..., occ...)
+    n = len(labels) // 2
+    vl = list(labels[:n])
+    ol = list(labels[n:])
+    if sorted(spin[l] for l in vl) != sorted(spin[l] for l in ol):
+        return None
+    vs, sv = _stable_spin_sort(vl, spin)
+    os_, so = _stable_spin_sort(ol, spin)
+    nb = sum(spin[l] for l in vl)
+    block = f'T{n}' + 'ABCDE'[nb]
+    axes = [Axis(l, SIZE[('o', spin[l])]) for l in os_] + [Axis(l, SIZE[('v', spin[l])]) for l in vs]
+    return sv * so, View(block, axes)
+
+
+SIZES_C2 = {'oa': 8, 'ob': 8, 'va': 32, 'vb': 32, 'n': 40, '1': 1}
+
+
+def _numel(view, sizes):
+    out = 1
+    for a in view.axes:
+        out *= sizes[a.size]
+    return out
+
+
+def _label_size(views, sizes):
+    d = {}
+    for v in views:
+        for a in v.axes:
+            d[a.label] = sizes[a.size]
+    return d
+
+
+class PlanBuilder:
+    def __init__(self, method, rhf=False, est_sizes=None):
+        self.method = method
+        self.rhf = rhf
+        self.tranks = wick.METHOD_TRANKS[method]
+        self.nmax = max(self.tranks)
+        self.sizes = est_sizes or SIZES_C2
+        self.buffers = {}
+        self.ops = []
+        self.nz = 0
+        self.nx = 0
+        self.flops = 0
+
+    # -- buffers --------------------------------------------------------------
+    def buf(self, name, kind, dims):
+        self.buffers[name] = (kind, tuple(dims))
+        return name
+
+    def new_z(self, dims):
+        name = f'Z{self.nz}'
+        self.nz += 1
+        return self.buf(name, 'work', dims)
+
+    def new_x(self, dims):
+        name = f'X{self.nx}'
+        self.nx += 1
+        return self.buf(name, 'work', dims)
+
+    # -- spin-summed contraction chains --------------------------------------
+    def _order(self, base):
+        """Order of cluster factors minimising the spin-orbital GEMM cost."""
+        so = {'o': 2 * self.sizes['oa'], 'v': 2 * self.sizes['va']}
+        best = None
+        for order in itertools.permutations(range(1, len(base))):
+            cur = set(base[0][1])
+            cost = 0
+            for k in order:
+                tl = set(base[k][1])
+                sh = cur & tl
+                c = 1
+                for l in cur | tl:
+                    c *= so[_sp(l)]
+                cost += c
+                cur = (cur | tl) - sh
+            if best is None or cost < best[0]:
+                best = (cost, order)
+        return best[1]
+
+    def emit_chain(self, base, espin, dst, scale, tag, beta, undressed=False):
+        """Emit GETTs for ``scale * base`` (external spins ``espin``) into ``dst``.
+
+        Intermediates are spin-summed: X_s for a spin assignment of its free
+        labels is the sum over the spins of the labels contracted at step s,
+        so no spin term is evaluated twice.  Contributions that differ only
+        by renaming summed labels are merged.  Returns the updated beta flag.
+        """
+        order = self._order(base)
+        facs = [base[0]] + [base[k] for k in order]
+        free = [list(facs[0][1])]
+        shared = [[]]
+        for s in range(1, len(facs)):
+            prev = free[s - 1]
+            tl = list(facs[s][1])
+            sh = [l for l in prev if l in tl]
+            shared.append(sh)
+            free.append([l for l in prev if l not in sh] + [l for l in tl if l not in sh])
+        last = len(facs) - 1
+        memo = {}
+
+        def get(s, spins):
+            key = (s, tuple(sorted(spins.items())))
+            if key in memo:
+                return memo[key]
+            if s == 0:
+                r = map_factor(facs[0][0], facs[0][1], spins, undressed)
+                out = [] if r is None else [(r[0], r[1])]
+                memo[key] = out
+                return out
+            contribs = self._contribs(s, spins, facs, free, shared, get, undressed)
+            if not contribs:
+                memo[key] = []
+                return []
+            axes = [Axis(l, SIZE[(_sp(l), spins[l])]) for l in free[s]]
+            name = self.new_x([a.size for a in axes])
+            xv = View(name, axes)
+            b = 0
+            for alpha, xa, tb in contribs:
+                self._gett(xv, xa, tb, alpha, b, tag)
+                b = 1
+            memo[key] = [(1, xv)]
+            return memo[key]
+
+        spins = {l: espin[l] for l in free[last]}
+        contribs = self._contribs(last, spins, facs, free, shared, get, undressed)
+        for alpha, xa, tb in contribs:
+            self._gett(dst, xa, tb, alpha * float(scale), beta, tag)
+            beta = 1
+        return beta
+
+    def _contribs(self, s, spins, facs, free, shared, get, undressed):
+        sh = shared[s]
+        prevfree = free[s - 1]
+        merged = {}
+        orderk = []
+        for ds in itertools.product((0, 1), repeat=len(sh)):
+            sp = dict(spins)
+            sp.update(zip(sh, ds))
+            xs = get(s - 1, {l: sp[l] for l in prevfree})
+            if not xs:
+                continue
+            r = map_factor(facs[s][0], facs[s][1], sp, undressed)
+            if r is None:
+                continue
+            st, tv = r
+            for sx, xv in xs:
+                ren = {}
+                for a in xv.axes + tv.axes:
+                    if a.label in sh and a.label not in ren:
+                        ren[a.label] = f'k{len(ren)}'
+                key = (xv.buf, tuple((ren.get(a.label, a.label), a.size, a.start) for a in xv.axes),
+                       tv.buf, tuple((ren.get(a.label, a.label), a.size, a.start) for a in tv.axes))
+                if key not in merged:
+                    merged[key] = [0, xv, tv]
+                    orderk.append(key)
+                merged[key][0] += st * sx
+        return [(merged[k][0], merged[k][1], merged[k][2]) for k in orderk if merged[k][0] != 0]
+
+    def _gett(self, c, a, b, alpha, beta, tag):
+        lsz = _label_size([a, b, c], self.sizes)
+        f = 2
+        for l in set(a.labels()) | set(b.labels()):
+            f *= lsz[l]
+        self.flops += f
+        self.ops.append(Gett(c, a, b, float(alpha), beta, tag))
+
+    # -- residual of one block -------------------------------------------------
+    def emit_block(self, block):
+        level = int(block[1])
+        spins_t = block_spins(block)
+        ext_o = [f'i{k}' for k in range(level)]
+        ext_v = [f'a{k}' for k in range(level)]
+        tspin = {l: s for l, s in zip(ext_o, spins_t)}
+        tspin.update({l: s for l, s in zip(ext_v, spins_t)})
+        terms = wick.residual_terms(level, self.tranks)
+        groups = wick.orbit_groups(level, terms)
+        asm = Assemble(block, 'jacobi')
+        direct = {}
+        direct_order = []
+        zshare = {}
+        self.ops.append(Simple('PHASE', (block,)))
+        for gi, (base, members) in enumerate(groups):
+            bypat = {}
+            for tau, c in members:
+                pat = tuple(tspin[tau[l]] for l in ext_o + ext_v)
+                bypat.setdefault(pat, []).append((tau, c))
+            for pat, mem in bypat.items():
+                espin = dict(zip(ext_o + ext_v, pat))
+                if len(base) == 1:
+                    name, ls = base[0]
+                    r = map_factor(name, ls, espin)
+                    if r is None:
+                        continue
+                    sign, v = r
+                    for tau, c in mem:
+                        axes = [Axis(tau[a.label], a.size, a.start) for a in v.axes]
+                        key = View(v.buf, axes).text()
+                        if key not in direct:
+                            direct[key] = [Fraction(0), View(v.buf, axes)]
+                            direct_order.append(key)
+                        direct[key][0] += c * sign
+                    continue
+                zaxes = [Axis(l, SIZE[(_sp(l), espin[l])]) for l in ext_o + ext_v]
+                mem_sorted = sorted(mem, key=lambda tc: tuple(tc[0][l] for l in ext_o + ext_v))
+                c0 = mem_sorted[0][1]
+                norm = (pat, tuple((tuple(tc[0][l] for l in ext_o + ext_v), tc[1] / c0) for tc in mem_sorted))
+                if norm in zshare:
+                    z, cref, state = zshare[norm]
+                    scale = c0 / cref
+                else:
+                    z = self.new_z([a.size for a in zaxes])
+                    state = [0]
+                    cref = c0
+                    scale = Fraction(1)
+                    zshare[norm] = (z, cref, state)
+                    for tau, c in mem_sorted:
+                        axes = [Axis(tau[a.label], a.size) for a in zaxes]
+                        asm.terms.append((c, View(z, axes)))
+                state[0] = self.emit_chain(base, espin, View(z, zaxes), scale, f'{block}.g{gi}', state[0])
+        for key in direct_order:
+            c, v = direct[key]
+            if c != 0:
+                asm.terms.append((c, v))
+        # drop Z buffers that never received a contribution
+        self.ops.append(asm)
+
+    def emit_dress(self):
+        """exp(-T1) H exp(T1): copy undressed blocks, four quarter transforms each."""
+        self.ops.append(Simple('PHASE', ('dress',)))
+        for d, s in (('VAA', 'VAA0'), ('VAB', 'VAB0'), ('VBB', 'VBB0'), ('HA', 'HA0'), ('HB', 'HB0')):
+            self.ops.append(Simple('COPY', (d, s)))
+        full = lambda l: Axis(l, 'n')
+        spins_of = {'VAA': (0, 0, 0, 0), 'VAB': (0, 1, 0, 1), 'VBB': (1, 1, 1, 1), 'HA': (0, 0), 'HB': (1, 1)}
+        for buf, sps in spins_of.items():
+            rank = len(sps)
+            creators = [0, 1] if rank == 4 else [0]
+            annih = [2, 3] if rank == 4 else [1]
+            for slot in range(rank):
+                sp = sps[slot]
+                t1 = 'T1A' if sp == 0 else 'T1B'
+                o, v = ('oa', 'va') if sp == 0 else ('ob', 'vb')
+                rest = [f'x{k}' for k in range(rank)]
+                if slot in creators:
+                    # X[p in v] -= sum_i t1[i,p] X[p = i]
+                    caxes = [full(l) for l in rest]
+                    caxes[slot] = Axis('p', v, o)
+                    baxes = [full(l) for l in rest]
+                    baxes[slot] = Axis('i', o)
+                    a = View(t1, [Axis('i', o), Axis('p', v)])
+                    self.ops.append(Gett(View(buf, caxes), a, View(buf, baxes), -1.0, 1, 'dress'))
+                else:
+                    # X[r in o] += sum_a X[r = a] t1[r,a]
+                    caxes = [full(l) for l in rest]
+                    caxes[slot] = Axis('r', o)
+                    baxes = [full(l) for l in rest]
+                    baxes[slot] = Axis('e', v, o)
+                    a = View(t1, [Axis('r', o), Axis('e', v)])
+                    self.ops.append(Gett(View(buf, caxes), a, View(buf, baxes), 1.0, 1, 'dress'))
+        # f = h + sum_i v[p,i,q,i]
+        self.ops.append(Simple('COPY', ('FA', 'HA')))
+        self.ops.append(Simple('COPY', ('FB', 'HB')))
+        P, Q = Axis('p', 'n'), Axis('q', 'n')
+        ia, ib = Axis('i', 'oa'), Axis('i', 'ob')
+        self.ops.append(Gett(View('FA', [P, Q]), View('VAA', [P, ia, Q, ia]), View('ONES', [ia]), 1.0, 1, 'dress'))
+        self.ops.append(Gett(View('FA', [P, Q]), View('VAB', [P, ib, Q, ib]), View('ONES', [ib]), 1.0, 1, 'dress'))
+        self.ops.append(Gett(View('FB', [P, Q]), View('VBB', [P, ib, Q, ib]), View('ONES', [ib]), 1.0, 1, 'dress'))
+        self.ops.append(Gett(View('FB', [P, Q]), View('VAB', [ia, P, ia, Q]), View('ONES', [ia]), 1.0, 1, 'dress'))
+
+    def emit_energy(self):
+        """E_cor with undressed f, v (``src/energy.f90:138-270``) into scalar E."""
+        self.ops.append(Simple('PHASE', ('energy',)))
+        self.ops.append(Simple('ZERO', ('E',)))
+        for coef, tensors in wick.energy_terms():
+            self.emit_chain(tensors, {}, View('E', []), coef, 'energy', 1, undressed=True)
+
+    def emit_rhf_copy(self, block):
+        src = {'T2C': 'T2A', 'T1B': 'T1A', 'T3D': 'T3A', 'T4E': 'T4A'}
+        self.ops.append(Simple('PHASE', (block,)))
+        level = int(block[1])
+        lab = [f'i{k}' for k in range(level)] + [f'a{k}' for k in range(level)]
+        dims = BLOCK_DIMS[block]
+        if block in src:
+            s = src[block]
+            v = View(s, [Axis(l, d) for l, d in zip(lab, BLOCK_DIMS[s])])
+        elif block == 'T3C':
+            # T3C[i,j,k,a,b,c] = T3B[j,k,i,b,c,a]   (src/cc/tran3Bto3C.f90)
+            order = ['i1', 'i2', 'i0', 'a1', 'a2', 'a0']
+            v = View('T3B', [Axis(l, d) for l, d in zip(order, BLOCK_DIMS['T3B'])])
+        elif block == 'T4D':
+            order = ['i1', 'i2', 'i3', 'i0', 'a1', 'a2', 'a3', 'a0']
+            v = View('T4B', [Axis(l, d) for l, d in zip(order, BLOCK_DIMS['T4B'])])
+        else:
+            raise KeyError(block)
+        self.ops.append(Assemble(block, 'copy', [(Fraction(1), v)]))
+
+    def build(self):
+        n = 'n'
+        for b in ('FA0', 'FB0', 'HA0', 'HB0', 'FA', 'FB', 'HA', 'HB'):
+            self.buf(b, 'int', (n, n))
+        for b in ('VAA0', 'VAB0', 'VBB0', 'VAA', 'VAB', 'VBB'):
+            self.buf(b, 'int', (n, n, n, n))
+        self.buf('ONES', 'ones', (n,))
+        self.buf('E', 'scalar', ())
+        for b, d in BLOCK_DIMS.items():
+            if int(b[1]) <= max(3, self.nmax):
+                self.buf(b, 'amp', d)
+        order = ['T2A', 'T2C', 'T2B', 'T1A', 'T1B']
+        if self.nmax >= 3:
+            order += ['T3A', 'T3D', 'T3B', 'T3C']
+        if self.nmax >= 4:
+            order += ['T4A', 'T4B', 'T4C', 'T4D', 'T4E']
+        self.emit_dress()
+        for b in order:
+            if b == 'T1B' and not self.rhf:
+                self.emit_dress()
+            if b == 'T3A':
+                self.emit_dress()
+            if self.rhf and b in ('T2C', 'T1B', 'T3D', 'T3C', 'T4D', 'T4E'):
+                self.emit_rhf_copy(b)
+            else:
+                self.emit_block(b)
+        self.emit_energy()
+        return self
+
+    def text(self):
+        lines = [f'PLAN {self.method} rhf={int(self.rhf)}']
+        for name, (kind, dims) in self.buffers.items():
+            lines.append(f'BUF {name} {kind} {len(dims)} ' + ' '.join(dims))
+        lines.append(f'OPS {len(self.ops)}')
+        for op in self.ops:
+            lines.append(op.text())
+        lines.append('END')
+        return '\n'.join(lines) + '\n'
+
+
+def build_plan(method, rhf=False):
+    return PlanBuilder(method, rhf).build()

@@ -1,0 +1,206 @@
+"""ctypes binding of ``libccq_b200.so`` (the C ABI of ``include/ccq_b200.h``).
+
+This is the same boundary a Fortran build of ccq binds with ISO_C_BINDING.
+There is no CPU fallback: if the library is missing or no GPU is present the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libccq_b200.so')
+
+PREC_FP64 = 0
+PREC_SPLIT = 1
+
+_lib = None
+
+I64 = C.c_int64
+DP = C.POINTER(C.c_double)
+
+
+class CCQB200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f'ccq_b200 error {code}: {msg}')
+        self.code = code
+
+
+class Dims(C.Structure):
+    _fields_ = [('froz', I64), ('occ_a', I64), ('occ_b', I64), ('orbs', I64)]
+
+
+SIGNATURES = {
+    'ccq_b200_egemm': (C.c_int, [I64, I64, I64, DP, DP, DP]),
+    'ccq_b200_egemm1': (C.c_int, [I64, I64, DP, DP, DP]),
+    'ccq_b200_egemm2': (C.c_int, [I64, I64, DP, DP, DP]),
+    'ccq_b200_init': (C.c_int, [C.POINTER(Dims), C.c_char_p, DP, DP, DP, DP, DP, I64, C.c_double, I64,
+                                C.POINTER(C.c_void_p)]),
+    'ccq_b200_sizes': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(I64)]),
+    'ccq_b200_set_t': (C.c_int, [C.c_void_p, DP, I64]),
+    'ccq_b200_get_t': (C.c_int, [C.c_void_p, DP, I64]),
+    'ccq_b200_update': (C.c_int, [C.c_void_p]),
+    'ccq_b200_energy': (C.c_int, [C.c_void_p, DP]),
+    'ccq_b200_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
+    'ccq_b200_set_precision': (C.c_int, [C.c_void_p, I64, I64]),
+    'ccq_b200_use_graph': (C.c_int, [C.c_void_p, I64]),
+    'ccq_b200_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), DP, DP]),
+    'ccq_b200_timing': (C.c_int, [C.c_void_p, DP, DP]),
+    'ccq_b200_profile': (C.c_int, [C.c_void_p, I64]),
+    'ccq_b200_profile_get': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
+    'ccq_b200_free': (C.c_int, [C.c_void_p]),
+    'ccq_b200_last_error': (C.c_int, [C.c_char_p, I64]),
+}
+
+
+def load(path=LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CCQB200Error(-6, f'{path} not built (python -m ccq_b200.build)')
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _err(code):
+    if code != 0:
+        buf = C.create_string_buffer(1024)
+        _lib.ccq_b200_last_error(buf, 1024)
+        raise CCQB200Error(code, buf.value.decode(errors='replace'))
+
+
+def _p(a):
+    return a.ctypes.data_as(DP)
+
+
+def egemm(k1, k2, k3, A, B):
+    """C(k2,k1) = B(k3,k2)^T A(k3,k1) on Fortran-ordered host arrays."""
+    lib = load()
+    A = np.asfortranarray(A, dtype=np.float64).reshape((k3, k1), order='F')
+    B = np.asfortranarray(B, dtype=np.float64).reshape((k3, k2), order='F')
+    Cm = np.zeros((k2, k1), order='F')
+    _err(lib.ccq_b200_egemm(k1, k2, k3, _p(A), _p(B), _p(Cm)))
+    return Cm
+
+
+def egemm1(k1, k3, A, B):
+    lib = load()
+    A = np.asfortranarray(A, dtype=np.float64).reshape((k3, k1), order='F')
+    B = np.ascontiguousarray(B, dtype=np.float64).reshape(k3)
+    Cv = np.zeros(k1)
+    _err(lib.ccq_b200_egemm1(k1, k3, _p(A), _p(B), _p(Cv)))
+    return Cv
+
+
+def egemm2(k2, k3, A, B):
+    lib = load()
+    A = np.ascontiguousarray(A, dtype=np.float64).reshape(k3)
+    B = np.asfortranarray(B, dtype=np.float64).reshape((k3, k2), order='F')
+    Cv = np.zeros(k2)
+    _err(lib.ccq_b200_egemm2(k2, k3, _p(A), _p(B), _p(Cv)))
+    return Cv
+
+
+class Context:
+    """A resident CC solve on the current CUDA device."""
+
+    def __init__(self, froz, occ_a, occ_b, orbs, calc_type, f_a, f_b, v_aa, v_ab, v_bb,
+                 rhf=False, shift=0.0, diis_space=5):
+        lib = load()
+        self._lib = lib
+        self.ptr = C.c_void_p()
+        d = Dims(froz, occ_a, occ_b, orbs)
+        # Fortran (column-major) layout, as sys%ints arrays are in ccq
+        self._keep = [np.asfortranarray(x, dtype=np.float64) for x in (f_a, f_b, v_aa, v_ab, v_bb)]
+        fa, fb, vaa, vab, vbb = self._keep
+        _err(lib.ccq_b200_init(C.byref(d), calc_type.encode(), _p(fa), _p(fb), _p(vaa), _p(vab), _p(vbb),
+                               int(bool(rhf)), float(shift), int(diis_space), C.byref(self.ptr)))
+        self._keep = None
+        ts, vs = I64(), I64()
+        _err(lib.ccq_b200_sizes(self.ptr, C.byref(ts), C.byref(vs)))
+        self.t_size, self.vec_size = ts.value, vs.value
+
+    def set_t(self, t):
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        _err(self._lib.ccq_b200_set_t(self.ptr, _p(t), t.size))
+
+    def get_t(self):
+        t = np.empty(self.t_size)
+        _err(self._lib.ccq_b200_get_t(self.ptr, _p(t), t.size))
+        return t
+
+    def update(self):
+        _err(self._lib.ccq_b200_update(self.ptr))
+
+    def energy(self):
+        e = C.c_double()
+        _err(self._lib.ccq_b200_energy(self.ptr, C.byref(e)))
+        return e.value
+
+    def iterate(self, it):
+        e, r, d = C.c_double(), C.c_double(), I64()
+        _err(self._lib.ccq_b200_iterate(self.ptr, it, C.byref(e), C.byref(r), C.byref(d)))
+        return e.value, r.value, bool(d.value)
+
+    def set_precision(self, mode, nslices=4):
+        _err(self._lib.ccq_b200_set_precision(self.ptr, mode, nslices))
+
+    def use_graph(self, enable=True):
+        _err(self._lib.ccq_b200_use_graph(self.ptr, int(bool(enable))))
+
+    def stats(self):
+        n, f, ms = I64(), C.c_double(), C.c_double()
+        _err(self._lib.ccq_b200_stats(self.ptr, C.byref(n), C.byref(f), C.byref(ms)))
+        return {'launches': n.value, 'flops': f.value, 'sweep_ms': ms.value}
+
+    def timing(self):
+        a, b = C.c_double(), C.c_double()
+        _err(self._lib.ccq_b200_timing(self.ptr, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def profile(self, enable=True):
+        _err(self._lib.ccq_b200_profile(self.ptr, int(bool(enable))))
+
+    def profile_get(self):
+        out = {}
+        for k, name in enumerate(('gett_f64', 'gett_split', 'assemble', 'other')):
+            ms, fl, n = C.c_double(), C.c_double(), I64()
+            _err(self._lib.ccq_b200_profile_get(self.ptr, k, C.byref(ms), C.byref(fl), C.byref(n)))
+            out[name] = {'ms': ms.value, 'flops': fl.value, 'launches': n.value}
+        return out
+
+    def set_t_ptr(self, ptr, n):
+        """set_t from a raw host pointer (pinned buffers)."""
+        _err(self._lib.ccq_b200_set_t(self.ptr, C.cast(ptr, DP), n))
+
+    def get_t_ptr(self, ptr, n):
+        _err(self._lib.ccq_b200_get_t(self.ptr, C.cast(ptr, DP), n))
+
+    def close(self):
+        if self.ptr:
+            self._lib.ccq_b200_free(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def header_symbols(header=None):
+    """Function names declared in include/ccq_b200.h."""
+    import re
+    header = header or os.path.join(HERE, '..', 'include', 'ccq_b200.h')
+    text = open(header).read()
+    text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+    return sorted(set(re.findall(r'^\s*(?:int|void)\s+(\w+)\s*\(', text, flags=re.M)))

@@ -1,0 +1,146 @@
+/*
+ * ccq_b200 — C ABI of the B200 coupled-cluster amplitude-update engine.
+ *
+ * Drop-in boundary for ccq (piecuch-group/ccq).  Every entry point is
+ * extern "C", takes plain pointers, 64-bit integers (ccq is built with
+ * -fdefault-integer-8 / ILP64 BLAS) and FP64 data in the reference's
+ * Fortran (column-major) layout, and returns 0 on success or a negative
+ * CCQ_B200_E* code; ccq_b200_last_error() gives the message.  A Fortran
+ * caller binds them with ISO_C_BINDING interfaces and calls stop_all() on a
+ * non-zero status, which keeps ccq's exit-code behaviour (errors.f90:11-27).
+ *
+ * Two levels:
+ *  1. The dgemm.f90 call surface (egemm / egemm1 / egemm2) on host arrays.
+ *  2. A resident solver context: integrals and T1..T4 stay in HBM across
+ *     iterations; the host driver keeps ccq's loop (solve_cc.f90:175-269)
+ *     and calls update + energy through the procedure-pointer slots
+ *     update_ptr / calculate_energy_ptr (proc_pointers.f90:7-31).
+ */
+#ifndef CCQ_B200_H
+#define CCQ_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCQ_B200_OK 0
+#define CCQ_B200_EINVAL (-1)     /* bad argument / size                  */
+#define CCQ_B200_ECUDA (-2)      /* CUDA runtime error                   */
+#define CCQ_B200_ENOMEM (-3)     /* device allocation failed             */
+#define CCQ_B200_EPLAN (-4)      /* plan text could not be parsed        */
+#define CCQ_B200_ESINGULAR (-5)  /* DIIS system singular (diis.F90:64)   */
+#define CCQ_B200_ENODEV (-6)     /* no CUDA device                       */
+#define CCQ_B200_ERANGE (-7)     /* size beyond a fixed maximum          */
+
+typedef struct ccq_b200_ctx ccq_b200_ctx;
+
+/* Problem sizes (sys_t, system.f90:60-98).  froz/occ_a/occ_b/orbs are the
+ * reference's spatial-orbital counts: occupied alpha = occ_a - froz, etc. */
+typedef struct {
+    int64_t froz;
+    int64_t occ_a;
+    int64_t occ_b;
+    int64_t orbs;
+} ccq_b200_dims;
+
+/* Precision of the bulk contractions (GETT operations on T3/T4 blocks). */
+#define CCQ_B200_PREC_FP64 0     /* FP64 DMMA tensor cores                */
+#define CCQ_B200_PREC_SPLIT 1    /* Ozaki int8 slices, tcgen05, INT32 acc */
+
+/* ---- level 1: dgemm.f90 call surface (host arrays) ---------------------- */
+
+/* Replaces egemm (src/dgemm.f90:1-29): C(k2,k1) = B(k3,k2)^T A(k3,k1),
+ * i.e. dgemm('t','n',k2,k1,k3,1,B,k3,A,k3,0,C,k2).  Column-major host
+ * arrays; copies in and out of device memory on every call. */
+int ccq_b200_egemm(int64_t k1, int64_t k2, int64_t k3,
+                   const double *A, const double *B, double *C);
+/* Replaces egemm1 (src/dgemm.f90:31-57): C(k1) = A(k3,k1)^T B(k3). */
+int ccq_b200_egemm1(int64_t k1, int64_t k3, const double *A, const double *B, double *C);
+/* Replaces egemm2 (src/dgemm.f90:59-73): C(k2) = B(k3,k2)^T A(k3). */
+int ccq_b200_egemm2(int64_t k2, int64_t k3, const double *A, const double *B, double *C);
+
+/* Fortran link-level drop-ins with gfortran's names and by-reference
+ * arguments (ILP64 integers): link libccq_b200 in place of dgemm.o. */
+void egemm_(const int64_t *k1, const int64_t *k2, const int64_t *k3,
+            const double *A, const double *B, double *C);
+void egemm1_(const int64_t *k1, const int64_t *k3, const double *A, const double *B, double *C);
+void egemm2_(const int64_t *k2, const int64_t *k3, const double *A, const double *B, double *C);
+
+/* ---- level 2: resident solver ------------------------------------------- */
+
+/* Builds a context for calc_type "CCSD", "CCSDT" or "CCSDTQ"
+ * (parser.f90:316-432).  f_a, f_b: Fock matrices (orbs x orbs, Fortran
+ * order, sys%ints%f_a / f_b); v_aa, v_ab, v_bb: antisymmetrised two-body
+ * blocks over the active range ((orbs-froz)^4, Fortran order,
+ * sys%ints%v_aa/v_ab/v_bb, integrals.f90:264-276).  rhf != 0 selects the
+ * closed-shell copies of update_cc.F90:125-317.  diis_space as in
+ * run%diis_space.  The arrays are copied; the caller keeps ownership. */
+int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type,
+                  const double *f_a, const double *f_b,
+                  const double *v_aa, const double *v_ab, const double *v_bb,
+                  int64_t rhf, double shift, int64_t diis_space,
+                  ccq_b200_ctx **out);
+
+/* Length of t_vec (get_t_sizes, cc_utils.f90:479-559) and of the DIIS
+ * vector (solve_cc.f90:66-77). */
+int ccq_b200_sizes(const ccq_b200_ctx *ctx, int64_t *t_size, int64_t *vec_size);
+
+/* Copy the whole T vector (cc%t_vec layout) to / from the device. */
+int ccq_b200_set_t(ccq_b200_ctx *ctx, const double *t_vec, int64_t n);
+int ccq_b200_get_t(const ccq_b200_ctx *ctx, double *t_vec, int64_t n);
+
+/* One sweep of update_clusters_t4 (update_cc.F90:12-323): the update_ptr
+ * slot.  Blocks are updated in place in the reference's order. */
+int ccq_b200_update(ccq_b200_ctx *ctx);
+
+/* calculate_unsorted_energy (energy.f90:138-270): calculate_energy_ptr. */
+int ccq_b200_energy(ccq_b200_ctx *ctx, double *e_cor);
+
+/* One jacobi_iter step (solve_cc.f90:215-245): update, energy, ring write,
+ * residuum, and DIIS when iter % (diis_space+1) == 0.  *did_diis is set to
+ * 1 when an extrapolation was applied. */
+int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
+                     double *residuum, int64_t *did_diis);
+
+/* Precision of the bulk contractions; nslices = int8 slices per operand
+ * (2..7) for CCQ_B200_PREC_SPLIT. */
+int ccq_b200_set_precision(ccq_b200_ctx *ctx, int64_t mode, int64_t nslices);
+
+/* Capture one update+energy sweep in a CUDA graph and replay it (1) or run
+ * the kernels one by one (0). */
+int ccq_b200_use_graph(ccq_b200_ctx *ctx, int64_t enable);
+
+/* Counters: kernels launched by the last iterate, algorithmic FP64 FLOPs of
+ * one update+energy sweep, and the device time of the last sweep in ms. */
+int ccq_b200_stats(const ccq_b200_ctx *ctx, int64_t *launches, double *flops, double *sweep_ms);
+
+/* Device time of the last iterate: the update+energy sweep and the whole
+ * step including ring write, residuum and DIIS (CUDA events, ms). */
+int ccq_b200_timing(const ccq_b200_ctx *ctx, double *sweep_ms, double *iter_ms);
+
+/* Per-kernel profiling of eager sweeps (CUDA events around every launch;
+ * disables graph replay while on).  kind: 0 FP64 GETT, 1 split GETT,
+ * 2 assemble (gather + Jacobi + fill), 3 other.  Enabling resets the sums. */
+int ccq_b200_profile(ccq_b200_ctx *ctx, int64_t enable);
+int ccq_b200_profile_get(const ccq_b200_ctx *ctx, int64_t kind, double *ms, double *flops, int64_t *launches);
+
+int ccq_b200_free(ccq_b200_ctx *ctx);
+
+/* Last error message of this thread (NUL-terminated, truncated to len). */
+int ccq_b200_last_error(char *buf, int64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif

@@ -1,0 +1,73 @@
+"""Small-system CC oracle: dense spin-orbital residuals + ccq's driver.
+
+Composes ``oracle.spinorb`` (residuals from the symbolic equations, no spin
+integration) with ``oracle.solver`` (ccq's in-place block sweep, Jacobi step,
+DIIS and convergence rule).  Only ``tests/`` use this module.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from ccq_b200 import integrals as I
+from oracle import solver as S
+from oracle.spinorb import SpinOrbitalSystem
+
+METHOD = {'CCSD': (2,), 'CCSDT': (2, 3), 'CCSDTQ': (2, 3, 4)}
+
+
+class DenseCC:
+    def __init__(self, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, method, shift=0.0, rhf=False):
+        self.dims = dims
+        self.method = method
+        self.tranks = METHOD[method]
+        self.nmax = max(self.tranks)
+        self.shift = shift
+        self.rhf = rhf
+        fr = dims.froz
+        self.fa = f_a[fr:, fr:]
+        self.fb = f_b[fr:, fr:]
+        self.so = SpinOrbitalSystem(self.fa, self.fb, v_aa, v_ab, v_bb, dims.oa, dims.ob)
+        self.layout = I.TLayout(dims)
+        self.t4 = {b: np.zeros(s) for b, s in self.layout.t4_shape.items()} if self.nmax >= 4 else {}
+        self.blocks = [b for b in S.BLOCK_ORDER if int(b[1]) <= self.nmax]
+
+    def _blocks(self, tvec):
+        out = {b: self.layout.view(tvec, b) for b in I.T_VEC_ORDER if int(b[1]) <= self.nmax}
+        out.update(self.t4)
+        return out
+
+    def update(self, tvec):
+        fda = np.diag(self.fa)
+        fdb = np.diag(self.fb)
+        for name in self.blocks:
+            blocks = self._blocks(tvec)
+            if self.rhf and name in S.RHF_COPY:
+                src = S.RHF_COPY[name]
+                if src == 'tran3bto3c':
+                    new = S.tran3bto3c(blocks['T3B'])
+                elif src == 'tran4bto4d':
+                    new = S.tran4bto4d(blocks['T4B'])
+                else:
+                    new = blocks[src].copy()
+            else:
+                ts = self.so.from_blocks(blocks, self.nmax)
+                level = int(name[1])
+                R = self.so.residual(ts, level, self.tranks)
+                Rb = self.so.to_blocks({level: R}, [name])[name]
+                D = S.denominator(name, blocks[name].shape, fda, fdb, self.dims, self.shift)
+                new = S.jacobi_block(name, blocks[name], Rb, D)
+            if name in self.t4:
+                self.t4[name] = new
+            else:
+                self.layout.view(tvec, name)[...] = new
+
+    def energy(self, tvec):
+        blocks = self._blocks(tvec)
+        ts = self.so.from_blocks({k: v for k, v in blocks.items() if int(k[1]) <= 2}, 2)
+        return self.so.energy(ts)
+
+    def solve(self, diis_space=5, max_iter=60, tol=1e-8, log=None):
+        tvec = np.zeros(self.layout.t_size)
+        vs = self.layout.vec_size(self.method)
+        e, it, failed, hist = S.jacobi_iter(self.update, self.energy, tvec, vs, diis_space, max_iter, tol, log)
+        return e, it, failed, hist, tvec
