@@ -17,7 +17,7 @@
 namespace ccqb {
 
 constexpr int MAXR = 8;        // max tensor rank (T4 blocks)
-constexpr int MAX_TERMS = 512; // max views gathered by one assemble
+constexpr int MAX_TERMS = 65536; // max views gathered by one assemble
 
 struct GettArgs {
     const double *A;

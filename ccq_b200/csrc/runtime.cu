@@ -419,8 +419,12 @@ void instantiate(ccq_b200_ctx *c) {
                 if (has(C, l) && !has(A, l)) nl.push_back(l);
                 else if (!has(A, l)) throw Error(CCQ_B200_EPLAN, "dangling label " + l);
             }
-            for (auto &l : C.order)
+            for (auto &l : C.order) {
                 if (!has(A, l) && !has(B, l)) throw Error(CCQ_B200_EPLAN, "output label not produced: " + l);
+                if (C.extent[l] != ext[l]) throw Error(CCQ_B200_EPLAN, "extent mismatch for label " + l);
+            }
+            for (auto &l : kl)
+                if (B.extent[l] != A.extent[l]) throw Error(CCQ_B200_EPLAN, "extent mismatch for label " + l);
             std::vector<int> am, ak, bn, bk, cm, cn;
             build_table(ml, ext, A, &C, am, cm);
             build_table(kl, ext, A, &B, ak, bk);
@@ -439,7 +443,8 @@ void instantiate(ccq_b200_ctx *c) {
             itab.insert(itab.end(), cn.begin(), cn.end());
             pend.push_back(p);
             long long M = (long long)am.size(), N = (long long)bn.size(), K = (long long)ak.size();
-            if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) throw Error(CCQ_B200_ERANGE, "GETT too large");
+            if (M > INT32_MAX || N > INT32_MAX || K > INT32_MAX || (N + 63) / 64 > 65535)
+                throw Error(CCQ_B200_ERANGE, "GETT too large");
             o.mnk[0] = M;
             o.mnk[1] = N;
             o.mnk[2] = K;
@@ -510,9 +515,12 @@ void instantiate(ccq_b200_ctx *c) {
                 AsmTerm at{};
                 at.p = V.base;
                 at.coef = t.first;
+                if (V.order.size() != (size_t)a.rank) throw Error(CCQ_B200_EPLAN, "assemble term rank");
                 for (int d = 0; d < a.rank; ++d) {
                     auto s = V.stride.find(target[d]);
-                    at.stride[d] = s == V.stride.end() ? 0 : (int)s->second;
+                    if (s == V.stride.end() || V.extent[target[d]] != a.dims[d])
+                        throw Error(CCQ_B200_EPLAN, "assemble term does not cover " + target[d] + " of " + o.block);
+                    at.stride[d] = (int)s->second;
                 }
                 hterms.push_back(at);
             }
