@@ -10,6 +10,7 @@
 
 #include "../../include/ccq_b200.h"
 #include "kernels.cuh"
+#include "split.cuh"
 
 namespace {
 
@@ -86,6 +87,7 @@ int egemm_impl(long long k1, long long k2, long long k3, const double *A, const 
     g.K = (int)k3;
     g.alpha = 1.0;
     g.beta = 0;
+    g.c_nfast = 1;
     long long tiles = ((k1 + 63) / 64) * ((k2 + 63) / 64);
     int splits = 1;
     if (tiles < 296 && k3 >= 128) splits = (int)std::min<long long>(std::min<long long>((296 + tiles - 1) / tiles, (k3 + 63) / 64), 128);
@@ -99,9 +101,85 @@ int egemm_impl(long long k1, long long k2, long long k3, const double *A, const 
     return 0;
 }
 
+ccqb::SplitWorkspace g_split;
+
+// Split-precision egemm (same layout as egemm_impl), nslices int8 slices.
+int egemm_split_impl(long long k1, long long k2, long long k3, const double *A, const double *B, double *C, int S) {
+    if (k1 <= 0 || k2 <= 0 || k3 <= 0 || !A || !B || !C || S < 2 || S > 4) return CCQ_B200_EINVAL;
+    if (k1 > INT32_MAX || k2 > INT32_MAX || k3 > INT32_MAX || k1 * k3 > INT32_MAX || k2 * k3 > INT32_MAX ||
+        k1 * k2 > INT32_MAX)
+        return CCQ_B200_ERANGE;
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CCQ_B200_ENODEV;
+    if (g_st.device != dev) {
+        g_st = Staging();
+        g_st.device = dev;
+        if (cudaStreamCreateWithFlags(&g_st.s, cudaStreamNonBlocking) != cudaSuccess) return CCQ_B200_ECUDA;
+    }
+    size_t na = (size_t)(k1 * k3), nb = (size_t)(k2 * k3), nc = (size_t)(k1 * k2);
+    size_t nt = (size_t)(2 * k1 + 2 * k2 + 2 * k3);
+    int rc = 0;
+    if ((rc = grow((void **)&g_st.a, &g_st.ca, sizeof(double) * na))) return rc;
+    if ((rc = grow((void **)&g_st.b, &g_st.cb, sizeof(double) * nb))) return rc;
+    if ((rc = grow((void **)&g_st.c, &g_st.cc, sizeof(double) * nc))) return rc;
+    if ((rc = grow((void **)&g_st.tab, &g_st.ct, sizeof(int) * nt))) return rc;
+    std::vector<int> t(nt);
+    int *am = t.data(), *ak = am + k1, *bn = ak + k3, *bk = bn + k2, *cm = bk + k3, *cn = cm + k1;
+    for (long long i = 0; i < k1; ++i) {
+        am[i] = (int)(i * k3);
+        cm[i] = (int)(i * k2);
+    }
+    for (long long i = 0; i < k2; ++i) {
+        bn[i] = (int)(i * k3);
+        cn[i] = (int)i;
+    }
+    for (long long i = 0; i < k3; ++i) ak[i] = bk[i] = (int)i;
+    cudaStream_t s = g_st.s;
+    cudaMemcpyAsync(g_st.a, A, sizeof(double) * na, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(g_st.b, B, sizeof(double) * nb, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(g_st.tab, t.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s);
+    int *d = g_st.tab;
+    ccqb::GettArgs g{};
+    g.A = g_st.a;
+    g.B = g_st.b;
+    g.C = g_st.c;
+    g.offA_m = d;
+    g.offA_k = d + k1;
+    g.offB_n = d + k1 + k3;
+    g.offB_k = d + k1 + k3 + k2;
+    g.offC_m = d + k1 + 2 * k3 + k2;
+    g.offC_n = d + 2 * k1 + 2 * k3 + k2;
+    g.M = (int)k1;
+    g.N = (int)k2;
+    g.K = (int)k3;
+    g.alpha = 1.0;
+    g.beta = 0;
+    g.c_nfast = 1;
+    g.kchunk = (int)k3;
+    try {
+        long long kp = (k3 + 63) / 64 * 64;
+        ccqb::split_reserve(g_split, ccqb::SplitSizes{k1 * kp, k2 * kp, std::max(k1, k2)}, S);
+        ccqb::split_gett(g_split, g, 1, 1, S, s);
+    } catch (const std::exception &) {
+        return CCQ_B200_ECUDA;
+    }
+    cudaMemcpyAsync(C, g_st.c, sizeof(double) * nc, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return CCQ_B200_ECUDA;
+    if (cudaGetLastError() != cudaSuccess) return CCQ_B200_ECUDA;
+    if (ccqb::split_error(g_split)) return CCQ_B200_ECUDA;
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+int ccq_b200_egemm_split(int64_t k1, int64_t k2, int64_t k3, const double *A, const double *B, double *C,
+                         int64_t nslices) {
+    return egemm_split_impl(k1, k2, k3, A, B, C, (int)nslices);
+}
+
 
 int ccq_b200_egemm(int64_t k1, int64_t k2, int64_t k3, const double *A, const double *B, double *C) {
     return egemm_impl(k1, k2, k3, A, B, C);

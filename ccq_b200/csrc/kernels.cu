@@ -60,8 +60,10 @@ __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *
 
 template <bool AK, bool BKM>
 __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
-    __shared__ __align__(16) double As[2][BKT][BM + PADS];
-    __shared__ __align__(16) double Bs[2][BKT][BN + PADS];
+    constexpr int TILE = BKT * (BM + PADS);
+    __shared__ __align__(16) double smem[4 * TILE];
+    double (*As)[BKT][BM + PADS] = reinterpret_cast<double (*)[BKT][BM + PADS]>(smem);
+    double (*Bs)[BKT][BN + PADS] = reinterpret_cast<double (*)[BKT][BN + PADS]>(smem + 2 * TILE);
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
@@ -136,29 +138,35 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
         __syncthreads();
     }
 
+    // epilogue: stage the tile in shared memory, then write along the output's
+    // contiguous mode (g.c_nfast) so that stores and the beta read coalesce
+    static_assert(BM * (BN + 1) <= 4 * TILE, "C tile must fit in the operand buffers");
+    double (*Cs)[BN + 1] = reinterpret_cast<double (*)[BN + 1]>(smem);
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    Cs[wm + mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = g.alpha * acc[mi][ni][2 * h + j];
+    __syncthreads();
     const bool atomic = gridDim.z > 1;
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            int m = m0 + wm + mi * 16 + gid + 8 * h;
-            if (m >= g.M) continue;
-            long long om = __ldg(g.offC_m + m);
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) {
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    int n = n0 + wn + ni * 8 + 2 * tig + j;
-                    if (n >= g.N) continue;
-                    double *c = g.C + om + __ldg(g.offC_n + n);
-                    double v = g.alpha * acc[mi][ni][2 * h + j];
-                    if (atomic)
-                        atomicAdd(c, v);
-                    else
-                        *c = g.beta ? *c + v : v;
-                }
-            }
-        }
+    const int fast = tid & 63, slow0 = tid >> 6;
+#pragma unroll 4
+    for (int p = 0; p < 32; ++p) {
+        int slow = slow0 + 2 * p;
+        int ml = g.c_nfast ? slow : fast;
+        int nl = g.c_nfast ? fast : slow;
+        int m = m0 + ml, n = n0 + nl;
+        if (m >= g.M || n >= g.N) continue;
+        double *c = g.C + (long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + n);
+        double v = Cs[ml][nl];
+        if (atomic)
+            atomicAdd(c, v);
+        else
+            *c = g.beta ? *c + v : v;
     }
 }
 
@@ -211,9 +219,28 @@ __global__ void assemble_kernel(AsmArgs a) {
         double R = 0.0;
         for (int t = 0; t < a.nterms; ++t) {
             const AsmTerm &tm = a.terms[t];
+            int y[MAXR];
+            for (int j = 0; j < tm.rank; ++j) y[j] = x[tm.src[j]];
+            double sg = 1.0;
+            bool zero = false;
+            for (int g = 0; g < tm.ng; ++g) {
+                const signed char *gp = tm.gpos[g];
+                int L = tm.glen[g];
+                // insertion sort of the group's indices, one sign flip per swap
+                for (int i = 1; i < L; ++i)
+                    for (int j = i; j > 0 && y[gp[j - 1]] > y[gp[j]]; --j) {
+                        int tmp = y[gp[j]];
+                        y[gp[j]] = y[gp[j - 1]];
+                        y[gp[j - 1]] = tmp;
+                        sg = -sg;
+                    }
+                for (int i = 1; i < L; ++i)
+                    if (y[gp[i]] == y[gp[i - 1]]) zero = true;
+            }
+            if (zero) continue;
             long long off = 0;
-            for (int d = 0; d < a.rank; ++d) off += (long long)tm.stride[d] * x[d];
-            R += tm.coef * tm.p[off];
+            for (int j = 0; j < tm.rank; ++j) off += (long long)tm.zstride[j] * y[j];
+            R += sg * tm.coef * tm.p[off];
         }
         long long toff = 0;
         for (int d = 0; d < a.rank; ++d) toff += (long long)a.tstride[d] * x[d];

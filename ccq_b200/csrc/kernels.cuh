@@ -28,12 +28,23 @@ struct GettArgs {
     double alpha;
     int beta;       // 0: overwrite, 1: accumulate
     int kchunk;     // K range handled by one blockIdx.z (split-K, atomic epilogue)
+    int c_nfast;    // 1: output contiguous along n (write-out walks n), 0: along m
 };
 
+constexpr int MAXG = 4;  // antisymmetric axis groups per source view
+
+// One permuted view read by the assemble step.  Axis j of the source holds
+// target axis src[j]; groups list source axes stored only for increasing
+// indices (the source is antisymmetric in them), read sorted with sign.
 struct AsmTerm {
     const double *p;
     double coef;
-    int stride[MAXR];   // stride of the source for each target axis
+    int zstride[MAXR];
+    signed char src[MAXR];
+    signed char gpos[MAXG][MAXR];
+    signed char glen[MAXG];
+    signed char ng;
+    signed char rank;
 };
 
 struct AsmArgs {

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -89,6 +90,7 @@ struct Op {
     int beta = 0;
     ViewSpec c, a, b;
     std::string tag;
+    std::vector<std::vector<std::string>> restrict_groups;   // R= annotation
     // ASSEMBLE
     std::string block, mode;
     std::vector<std::pair<double, ViewSpec>> terms;
@@ -106,7 +108,17 @@ struct Op {
 struct BufSpec {
     std::string name, kind;
     std::vector<std::string> dims;
+    std::vector<std::vector<int>> groups;   // antisymmetric axis groups (G= annotation)
 };
+
+std::vector<std::string> split_str(const std::string &s, char sep) {
+    std::vector<std::string> out;
+    std::stringstream ss(s);
+    std::string x;
+    while (std::getline(ss, x, sep))
+        if (!x.empty()) out.push_back(x);
+    return out;
+}
 
 struct Plan {
     std::string method;
@@ -138,6 +150,15 @@ Plan parse_plan(const char *text) {
                 ls >> d;
                 b.dims.push_back(d);
             }
+            std::string ann;
+            if (ls >> ann) {
+                if (ann.rfind("G=", 0) != 0) throw Error(CCQ_B200_EPLAN, "bad buffer annotation " + ann);
+                for (auto &g : split_str(ann.substr(2), ';')) {
+                    std::vector<int> axes;
+                    for (auto &a : split_str(g, ',')) axes.push_back(std::stoi(a));
+                    b.groups.push_back(axes);
+                }
+            }
             p.bufs.push_back(b);
         } else if (w == "OPS") {
             continue;
@@ -146,7 +167,14 @@ Plan parse_plan(const char *text) {
             o.kind = OP_GETT;
             std::string c, a, b;
             ls >> o.alpha >> o.beta >> c >> a >> b;
-            ls >> o.tag;
+            std::string w2;
+            while (ls >> w2) {
+                if (w2.rfind("R=", 0) == 0) {
+                    for (auto &g : split_str(w2.substr(2), ';')) o.restrict_groups.push_back(split_str(g, ','));
+                } else {
+                    o.tag = w2;
+                }
+            }
             o.c = parse_view(c);
             o.a = parse_view(a);
             o.b = parse_view(b);
@@ -191,6 +219,7 @@ struct DevBuf {
     double *ptr = nullptr;
     std::vector<long long> shape, stride;
     long long numel = 0;
+    std::vector<std::vector<int>> groups;
 };
 
 }  // namespace
@@ -290,24 +319,48 @@ Resolved resolve(ccq_b200_ctx *c, const ViewSpec &v) {
 
 bool has(const Resolved &r, const std::string &l) { return r.stride.count(l) > 0; }
 
+// Offset tables of one index mode (labels, last fastest) for views x and y.
+// Restricted groups (label lists) are enumerated for increasing values only.
 void build_table(const std::vector<std::string> &labels, const std::map<std::string, long long> &extent,
-                 const Resolved &x, const Resolved *y, std::vector<int> &tx, std::vector<int> &ty) {
+                 const Resolved &x, const Resolved *y, const std::vector<std::vector<std::string>> &groups,
+                 std::vector<int> &tx, std::vector<int> &ty) {
+    tx.clear();
+    ty.clear();
+    std::vector<std::vector<int>> gidx;   // positions in `labels` of each group's members, in group order
+    for (auto &g : groups) {
+        std::vector<int> pos;
+        for (auto &l : g) {
+            auto it = std::find(labels.begin(), labels.end(), l);
+            if (it != labels.end()) pos.push_back((int)(it - labels.begin()));
+        }
+        if (pos.size() == g.size()) gidx.push_back(pos);
+    }
+    std::vector<long long> idx(labels.size(), 0);
+    bool more = true;
     long long total = 1;
     for (auto &l : labels) total *= extent.at(l);
-    tx.assign(total, 0);
-    if (y) ty.assign(total, 0);
-    std::vector<long long> idx(labels.size(), 0);
-    for (long long i = 0; i < total; ++i) {
-        long long ox = 0, oy = 0;
-        for (size_t d = 0; d < labels.size(); ++d) {
-            ox += idx[d] * x.stride.at(labels[d]);
-            if (y) oy += idx[d] * y->stride.at(labels[d]);
+    if (total == 0) return;
+    while (more) {
+        bool ok = true;
+        for (auto &g : gidx)
+            for (size_t q = 1; q < g.size(); ++q)
+                if (idx[g[q]] <= idx[g[q - 1]]) ok = false;
+        if (ok) {
+            long long ox = 0, oy = 0;
+            for (size_t d = 0; d < labels.size(); ++d) {
+                ox += idx[d] * x.stride.at(labels[d]);
+                if (y) oy += idx[d] * y->stride.at(labels[d]);
+            }
+            if (ox > INT32_MAX || oy > INT32_MAX) throw Error(CCQ_B200_ERANGE, "view offset beyond int32");
+            tx.push_back((int)ox);
+            if (y) ty.push_back((int)oy);
         }
-        if (ox > INT32_MAX || oy > INT32_MAX) throw Error(CCQ_B200_ERANGE, "view offset beyond int32");
-        tx[i] = (int)ox;
-        if (y) ty[i] = (int)oy;
+        more = false;
         for (int d = (int)labels.size() - 1; d >= 0; --d) {
-            if (++idx[d] < extent.at(labels[d])) break;
+            if (++idx[d] < extent.at(labels[d])) {
+                more = true;
+                break;
+            }
             idx[d] = 0;
         }
     }
@@ -354,6 +407,28 @@ void instantiate(ccq_b200_ctx *c) {
                 for (auto &t : o.terms) note(t.second);
         }
     }
+    {
+        // work buffers live in a shared arena: each must be overwritten before it is read
+        std::map<std::string, int> written;
+        auto work = [](const std::string &b) { return !b.empty() && (b[0] == 'Z' || b[0] == 'X'); };
+        for (auto &o : c->plan.ops) {
+            if (o.kind == OP_PHASE) written.clear();
+            if (o.kind == OP_GETT) {
+                for (auto *v : {&o.a, &o.b})
+                    if (work(v->buf) && !written.count(v->buf))
+                        throw Error(CCQ_B200_EPLAN, v->buf + " read before written");
+                if (work(o.c.buf)) {
+                    if (o.beta && !written.count(o.c.buf))
+                        throw Error(CCQ_B200_EPLAN, o.c.buf + " accumulated before written");
+                    written[o.c.buf] = 1;
+                }
+            }
+            if (o.kind == OP_ASM)
+                for (auto &t : o.terms)
+                    if (work(t.second.buf) && !written.count(t.second.buf))
+                        throw Error(CCQ_B200_EPLAN, t.second.buf + " read by assemble before written");
+        }
+    }
     std::map<std::string, long long> phase_fill;
     std::map<std::string, long long> work_off;
     long long arena = 0;
@@ -375,6 +450,7 @@ void instantiate(ccq_b200_ctx *c) {
         for (int i = (int)d.shape.size() - 2; i >= 0; --i) d.stride[i] = d.stride[i + 1] * d.shape[i + 1];
         d.numel = 1;
         for (auto s : d.shape) d.numel *= s;
+        d.groups = b.groups;
         if (tv_off.count(b.name)) {
             d.ptr = c->tvec + tv_off[b.name];
         } else if (b.kind == "work") {
@@ -425,10 +501,29 @@ void instantiate(ccq_b200_ctx *c) {
             }
             for (auto &l : kl)
                 if (B.extent[l] != A.extent[l]) throw Error(CCQ_B200_EPLAN, "extent mismatch for label " + l);
+            // restriction groups: each must lie entirely in one index mode
+            double kscale = 1.0;
+            for (auto &g : o.restrict_groups) {
+                auto in = [&](const std::vector<std::string> &lst) {
+                    for (auto &l : g)
+                        if (std::find(lst.begin(), lst.end(), l) == lst.end()) return false;
+                    return true;
+                };
+                if (in(kl)) {
+                    for (size_t q = 2; q <= g.size(); ++q) kscale *= (double)q;
+                } else if (!in(ml) && !in(nl)) {
+                    throw Error(CCQ_B200_EPLAN, "restriction group spans index modes");
+                }
+                for (auto &l : g)
+                    if (ext[l] != ext[g[0]]) throw Error(CCQ_B200_EPLAN, "restriction group with unequal extents");
+            }
             std::vector<int> am, ak, bn, bk, cm, cn;
-            build_table(ml, ext, A, &C, am, cm);
-            build_table(kl, ext, A, &B, ak, bk);
-            build_table(nl, ext, B, &C, bn, cn);
+            build_table(ml, ext, A, &C, o.restrict_groups, am, cm);
+            build_table(kl, ext, A, &B, o.restrict_groups, ak, bk);
+            build_table(nl, ext, B, &C, o.restrict_groups, bn, cn);
+            if (ml.empty()) { am.assign(1, 0); cm.assign(1, 0); }
+            if (nl.empty()) { bn.assign(1, 0); cn.assign(1, 0); }
+            if (kl.empty()) { ak.assign(1, 0); bk.assign(1, 0); }
             Pend p{i, itab.size(), 0, 0, 0, 0, 0};
             itab.insert(itab.end(), am.begin(), am.end());
             p.ak = itab.size();
@@ -456,13 +551,18 @@ void instantiate(ccq_b200_ctx *c) {
             };
             o.akm = kmajor(A, ml, kl);
             o.bkm = kmajor(B, nl, kl);
+            {
+                long long sn = nl.empty() ? (1LL << 40) : C.stride.at(nl.back());
+                long long sm = ml.empty() ? (1LL << 40) : C.stride.at(ml.back());
+                o.g.c_nfast = sn <= sm ? 1 : 0;
+            }
             o.g.A = A.base;
             o.g.B = B.base;
             o.g.C = C.base;
             o.g.M = (int)M;
             o.g.N = (int)N;
             o.g.K = (int)K;
-            o.g.alpha = o.alpha;
+            o.g.alpha = o.alpha * kscale;
             o.g.beta = o.beta;
             long long tiles = ((M + 63) / 64) * ((N + 63) / 64);
             int splits = 1;
@@ -512,15 +612,26 @@ void instantiate(ccq_b200_ctx *c) {
             PendA pa{i, hterms.size(), hperm.size()};
             for (auto &t : o.terms) {
                 Resolved V = resolve(c, t.second);
+                const DevBuf &src = c->bufs.at(t.second.buf);
                 AsmTerm at{};
                 at.p = V.base;
                 at.coef = t.first;
-                if (V.order.size() != (size_t)a.rank) throw Error(CCQ_B200_EPLAN, "assemble term rank");
-                for (int d = 0; d < a.rank; ++d) {
-                    auto s = V.stride.find(target[d]);
-                    if (s == V.stride.end() || V.extent[target[d]] != a.dims[d])
-                        throw Error(CCQ_B200_EPLAN, "assemble term does not cover " + target[d] + " of " + o.block);
-                    at.stride[d] = (int)s->second;
+                if (V.order.size() != (size_t)a.rank || t.second.axes.size() != (size_t)a.rank)
+                    throw Error(CCQ_B200_EPLAN, "assemble term rank");
+                at.rank = (signed char)a.rank;
+                for (int j = 0; j < a.rank; ++j) {
+                    const std::string &lab = t.second.axes[j].label;
+                    auto it = std::find(target.begin(), target.end(), lab);
+                    if (it == target.end() || V.extent[lab] != a.dims[it - target.begin()])
+                        throw Error(CCQ_B200_EPLAN, "assemble term does not cover " + lab + " of " + o.block);
+                    at.src[j] = (signed char)(it - target.begin());
+                    at.zstride[j] = (int)src.stride[j];
+                }
+                if (src.groups.size() > (size_t)MAXG) throw Error(CCQ_B200_EPLAN, "too many antisymmetric groups");
+                at.ng = (signed char)src.groups.size();
+                for (size_t g = 0; g < src.groups.size(); ++g) {
+                    at.glen[g] = (signed char)src.groups[g].size();
+                    for (size_t q = 0; q < src.groups[g].size(); ++q) at.gpos[g][q] = (signed char)src.groups[g][q];
                 }
                 hterms.push_back(at);
             }
@@ -609,7 +720,7 @@ void instantiate(ccq_b200_ctx *c) {
 }
 
 int op_class(const ccq_b200_ctx *c, const Op &o) {
-    if (o.kind == OP_GETT) return (c->precision == CCQ_B200_PREC_SPLIT && o.split) ? 1 : 0;
+    if (o.kind == OP_GETT) return (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g)) ? 1 : 0;
     if (o.kind == OP_ASM) return 2;
     return 3;
 }
@@ -638,7 +749,7 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
                     }
                     break;
                 }
-                if (c->precision == CCQ_B200_PREC_SPLIT && o.split) {
+                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g)) {
                     c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, c->stream);
                 } else {
                     launch_gett_f64(o.g, o.akm, o.bkm, c->stream);
@@ -669,6 +780,8 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
     CK(cudaGetLastError());
     if (prof) {
         CK(cudaStreamSynchronize(c->stream));
+        const char *dump = getenv("CCQ_B200_PROFILE_DUMP");
+        FILE *df = dump ? fopen(dump, "a") : nullptr;
         for (size_t i = from; i < to; ++i) {
             Op &o = c->plan.ops[i];
             if (o.kind == OP_PHASE) continue;
@@ -678,7 +791,17 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
             c->prof_ms[k] += ms;
             c->prof_launch[k] += 1;
             if (o.kind == OP_GETT) c->prof_flops[k] += 2.0 * o.mnk[0] * o.mnk[1] * o.mnk[2];
+            if (df) {
+                if (o.kind == OP_GETT)
+                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f\n", i, k, o.tag.c_str(), o.mnk[0], o.mnk[1],
+                            o.mnk[2], o.akm, o.bkm, o.beta, ms);
+                else if (o.kind == OP_ASM)
+                    fprintf(df, "%zu ASM %d %s %d %.6f\n", i, k, o.block.c_str(), o.asmargs.nterms, ms);
+                else
+                    fprintf(df, "%zu OTHER %d %s %.6f\n", i, k, o.arg0.c_str(), ms);
+            }
         }
+        if (df) fclose(df);
     }
 }
 
@@ -710,7 +833,9 @@ long long count_sweep_launches(ccq_b200_ctx *c) {
     for (auto &o : c->plan.ops) {
         if (o.kind == OP_GETT && o.g.M && o.g.N) {
             if (o.zero_first || o.g.K == 0) ++n;
-            if (o.g.K) n += (c->precision == CCQ_B200_PREC_SPLIT && o.split) ? split_launch_count(o.g, c->nslices) : 1;
+            if (o.g.K)
+                n += (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g))
+                         ? split_launch_count(o.g, c->nslices) : 1;
         } else if (o.kind == OP_ASM) {
             ++n;
         }
@@ -872,6 +997,26 @@ int ccq_b200_get_t(const ccq_b200_ctx *c, double *t, int64_t n) {
     }
 }
 
+int ccq_b200_block(ccq_b200_ctx *c, const char *name, double *host, int64_t n, int64_t to_device) {
+    try {
+        if (!c || !name || !host) throw Error(CCQ_B200_EINVAL, "block: null argument");
+        std::string nm(name);
+        if (nm.size() != 3 || nm[0] != 'T') throw Error(CCQ_B200_EINVAL, "block: amplitude block name expected");
+        auto it = c->bufs.find(nm);
+        if (it == c->bufs.end()) throw Error(CCQ_B200_EINVAL, "block: unknown block " + nm);
+        if (n != it->second.numel) throw Error(CCQ_B200_EINVAL, "block: size mismatch");
+        CK(cudaMemcpyAsync(to_device ? (void *)it->second.ptr : (void *)host,
+                           to_device ? (const void *)host : (const void *)it->second.ptr, sizeof(double) * n,
+                           to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
 int ccq_b200_update(ccq_b200_ctx *c) {
     try {
         if (!c) throw Error(CCQ_B200_EINVAL, "null context");
@@ -941,6 +1086,8 @@ int ccq_b200_iterate(ccq_b200_ctx *c, int64_t iter, double *e_cor, double *res, 
         CK(cudaEventElapsedTime(&ms, c->ev0, c->ev2));
         c->iter_ms = ms;
         if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
+        if (c->precision == CCQ_B200_PREC_SPLIT && split_error(c->split))
+            throw Error(CCQ_B200_ECUDA, "split GETT pipeline wait expired");
         if (e_cor) *e_cor = hs[0];
         if (res) *res = std::sqrt(std::sqrt(hs[1]));
         if (did_diis) *did_diis = diis;
@@ -962,9 +1109,9 @@ int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {
             long long ma = 0, mb = 0, mc = 0;
             for (auto &o : c->plan.ops)
                 if (o.kind == OP_GETT && o.split) {
-                    ma = std::max(ma, o.mnk[0] * ((o.mnk[2] + 127) / 128 * 128));
-                    mb = std::max(mb, o.mnk[1] * ((o.mnk[2] + 127) / 128 * 128));
-                    mc = std::max(mc, o.mnk[0] + o.mnk[1]);
+                    ma = std::max(ma, o.mnk[0] * ((o.mnk[2] + 63) / 64 * 64));
+                    mb = std::max(mb, o.mnk[1] * ((o.mnk[2] + 63) / 64 * 64));
+                    mc = std::max(mc, std::max(o.mnk[0], o.mnk[1]));
                 }
             return SplitSizes{ma, mb, mc};
         }() : SplitSizes{0, 0, 0}, (int)nslices);

@@ -1,9 +1,399 @@
-// Split-precision GETT (placeholder until the tcgen05 kernel lands).
+// Split-precision GETT on the tcgen05 tensor pipe (Ozaki scheme with int8 slices).
+//
+// A row r of an FP64 operand (read in place through its GETT offset tables) is
+// scaled by 2^-e_r so that |x| < 1, then cut into S int8 slices
+//     x 2^-e_r = s_1 2^-6 + s_2 2^-13 + ... + s_S 2^(-6-7(S-1)),  |s_t| <= 64.
+// Products of slices are exact in INT32.  The kernel accumulates, for every
+// level L = i + j (i, j slice indices, L <= S + 1), D_L = sum_k A_i B_j^T in
+// its own TMEM accumulator; the epilogue recombines
+//     C = alpha 2^(e_m + e_n - 12) sum_L D_L 2^(-7 (L - 2))
+// in FP64 and scatters through the GETT's output offset table.  Dropped
+// higher levels bound the error by ~S 2^(-7S-5) K max|A_m| max|B_n|.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
 #include <stdexcept>
+#include <string>
+
 #include "split.cuh"
+
 namespace ccqb {
-void split_reserve(SplitWorkspace &, SplitSizes, int) { throw std::runtime_error("split precision not built"); }
-void split_free(SplitWorkspace &) {}
-int split_gett(SplitWorkspace &, const GettArgs &, int, int, int, cudaStream_t) { throw std::runtime_error("split precision not built"); }
-int split_launch_count(const GettArgs &, int) { return 0; }
+
+namespace {
+
+constexpr int TM = 128;        // rows of the output tile (TMEM lanes)
+constexpr int BKB = 64;        // K bytes per pipeline stage (SWIZZLE_64B atom width)
+constexpr long long kWaitLimit = 1LL << 26;
+
+// ---------------------------------------------------------------------------
+// slicing
+// ---------------------------------------------------------------------------
+// One warp per row: exponent from the row maximum, then S int8 slices written
+// K-major into out[t][row][kp] (kp = padded K, zeros beyond K).
+__global__ void slice_rows_kernel(const double *base, const int *offr, const int *offk, int R, int K, int Kp, int S,
+                                  signed char *out, long long slice_stride, int *expo) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < R; r += nwarps) {
+        const double *row = base + offr[r];
+        double mx = 0.0;
+        for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(row[offk[k]]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        int e = 0;
+        if (mx > 0.0) frexp(mx, &e);   // mx = f 2^e, f in [0.5, 1)
+        if (lane == 0) expo[r] = e;
+        double scale = ldexp(1.0, -e);
+        signed char *dst = out + (long long)r * Kp;
+        for (int k = lane; k < Kp; k += 32) {
+            double x = k < K ? row[offk[k]] * scale : 0.0;
+            double t = x * 64.0;
+            for (int q = 0; q < S; ++q) {
+                double s = rint(t);
+                dst[q * slice_stride + k] = (signed char)s;
+                t = (t - s) * 128.0;
+            }
+        }
+    }
 }
+
+// ---------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes));
+}
+// Bounded wait on a phase parity; returns false when the limit is hit.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    unsigned a = smem_u32(bar);
+    for (long long it = 0; it < kWaitLimit; ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity));
+        if (ok) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ uint64_t smem_desc_sw64(const void *p) {
+    // K-major, SWIZZLE_64B: 8-row atoms of 64 B, stride between atoms 512 B.
+    uint64_t addr = smem_u32(p);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;           // start address [0,14)
+    d |= (uint64_t)1 << 16;                  // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;         // stride byte offset [32,46)
+    d |= (uint64_t)1 << 46;                  // descriptor version (sm100)
+    d |= (uint64_t)4 << 61;                  // layout: SWIZZLE_64B
+    return d;
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <int NT>
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+struct SplitArgs {
+    double *C;
+    const int *offC_m, *offC_n;
+    const int *ea, *eb;
+    int M, N, K, Kp;
+    double alpha;
+    int beta;
+    int *err;
+};
+
+// One CTA per 128 x NT output tile; warp 0 lane 0 issues TMA, warp 1 lane 0
+// issues MMAs, all four warps read TMEM in the epilogue.
+template <int S, int NT, int STAGES>
+__global__ void __launch_bounds__(128, 1)
+    split_gett_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, SplitArgs p) {
+    constexpr int A_BYTES = TM * BKB;           // one slice tile of A
+    constexpr int B_BYTES = NT * BKB;
+    constexpr int STAGE = S * (A_BYTES + B_BYTES);
+    constexpr int NLEV = S;                     // levels 2..S+1
+    constexpr int TCOLS = (NLEV * NT <= 32) ? 32 : (NLEV * NT <= 64) ? 64 : (NLEV * NT <= 128) ? 128
+                          : (NLEV * NT <= 256) ? 256 : 512;
+    static_assert(NLEV * NT <= 512, "TMEM capacity");
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + STAGES * STAGE);
+    uint64_t *empty = full + STAGES;
+    uint64_t *done = empty + STAGES;
+    uint32_t *tmem_slot = (uint32_t *)(done + 1);
+    __shared__ int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * TM, n0 = blockIdx.y * NT;
+    const int ktiles = p.Kp / BKB;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        for (int kt = 0; kt < ktiles; ++kt) {
+            int s = kt % STAGES;
+            if (kt >= STAGES && !mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1)) {
+                abort_flag = 1;
+                break;
+            }
+            unsigned char *st = smem + s * STAGE;
+            mbar_expect_tx(&full[s], STAGE);
+            tma_load_3d(st, &ta, &full[s], kt * BKB, m0, 0);
+            tma_load_3d(st + S * A_BYTES, &tb, &full[s], kt * BKB, n0, 0);
+        }
+        // drain: every issued copy has landed before the CTA can exit
+        for (int kt = (ktiles > STAGES ? ktiles - STAGES : 0); kt < ktiles; ++kt)
+            if (!mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1)) abort_flag = 1;
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: instruction descriptor S32 <- S8 x S8, K-major A and B
+        const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                               ((uint32_t)(TM >> 4) << 24);
+        bool ok = true;
+        for (int kt = 0; kt < ktiles && ok; ++kt) {
+            int s = kt % STAGES;
+            if (!mbar_wait(&full[s], (kt / STAGES) & 1)) {
+                abort_flag = 1;
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n");
+            unsigned char *st = smem + s * STAGE;
+#pragma unroll
+            for (int kk = 0; kk < BKB / 32; ++kk) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) {
+                    uint64_t da = smem_desc_sw64(st + i * A_BYTES) + (uint64_t)(kk * 32 >> 4);
+#pragma unroll
+                    for (int j = 0; j < S - i; ++j) {
+                        uint64_t db = smem_desc_sw64(st + S * A_BYTES + j * B_BYTES) + (uint64_t)(kk * 32 >> 4);
+                        int lev = i + j;   // level L - 2
+                        // the first product of each level (i = 0) at the first K step initialises it
+                        uint32_t acc = (kt > 0 || kk > 0 || i > 0) ? 1u : 0u;
+                        umma_i8(tmem + (uint32_t)(lev * NT), da, db, idesc, acc);
+                    }
+                }
+            }
+            umma_commit(&empty[s]);
+        }
+        umma_commit(done);
+    }
+    __syncwarp();
+    // epilogue: every thread owns one TMEM lane (output row)
+    bool good = mbar_wait(done, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    __syncthreads();
+    if (!good || abort_flag) {
+        if (threadIdx.x == 0) atomicExch(p.err, 1);
+    } else {
+        const int row = warp * 32 + lane;
+        const int m = m0 + row;
+        const long long om = m < p.M ? (long long)p.offC_m[m] : 0;
+        const int em = m < p.M ? p.ea[m] : 0;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 32) {
+            double val[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) val[q] = 0.0;
+#pragma unroll 1
+            for (int lev = NLEV - 1; lev >= 0; --lev) {
+                int v[32];
+                tmem_ld32<NT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(lev * NT + c0), v);
+                double w = ldexp(1.0, -7 * lev);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) val[q] += (double)v[q] * w;
+            }
+            if (m < p.M) {
+#pragma unroll 4
+                for (int q = 0; q < 32; ++q) {
+                    int n = n0 + c0 + q;
+                    if (n >= p.N) break;
+                    double x = p.alpha * ldexp(val[q], em + p.eb[n] - 12);
+                    double *c = p.C + om + p.offC_n[n];
+                    *c = p.beta ? *c + x : x;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn get_encode() {
+    static EncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeFn)p;
+    });
+    if (!fn) throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
+    return fn;
+}
+
+// 3-D map over int8 slices [S][rows][Kp]; box (64 B, tile rows, S).
+CUtensorMap make_map(signed char *base, long long rows, long long Kp, int S, int box_rows) {
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)S};
+    cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)(Kp * rows)};
+    cuuint32_t box[3] = {(cuuint32_t)BKB, (cuuint32_t)box_rows, (cuuint32_t)S};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, es,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+template <int S, int NT, int STAGES>
+void launch_split(const CUtensorMap &ta, const CUtensorMap &tb, const SplitArgs &a, cudaStream_t s) {
+    constexpr int STAGE = S * (TM * BKB + NT * BKB);
+    size_t smem = (size_t)STAGES * STAGE + 1024 + 256;
+    dim3 grid((a.M + TM - 1) / TM, (a.N + NT - 1) / NT);
+    split_gett_kernel<S, NT, STAGES><<<grid, 128, smem, s>>>(ta, tb, a);
+}
+
+int tile_n(int S) { return S <= 4 ? 128 : 64; }
+
+template <int S, int NT, int STAGES>
+void set_smem_attr() {
+    constexpr int STAGE = S * (TM * BKB + NT * BKB);
+    size_t smem = (size_t)STAGES * STAGE + 1024 + 256;
+    if (cudaFuncSetAttribute(split_gett_kernel<S, NT, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        throw std::runtime_error("cannot enable large shared memory for the split kernel");
+}
+
+}  // namespace
+
+void split_reserve(SplitWorkspace &w, SplitSizes sz, int nslices) {
+    auto need = [&](long long a, long long b, long long mn) {
+        return a * nslices > w.cap_a || b * nslices > w.cap_b || mn > w.cap_mn || nslices > w.slices;
+    };
+    if (!need(sz.a_elems, sz.b_elems, sz.mn) && w.err) return;
+    split_free(w);
+    long long ca = std::max(sz.a_elems, 1LL) * nslices, cb = std::max(sz.b_elems, 1LL) * nslices;
+    if (cudaMalloc(&w.a, ca) != cudaSuccess || cudaMalloc(&w.b, cb) != cudaSuccess ||
+        cudaMalloc(&w.ea, sizeof(int) * std::max(sz.mn, 1LL)) != cudaSuccess ||
+        cudaMalloc(&w.eb, sizeof(int) * std::max(sz.mn, 1LL)) != cudaSuccess ||
+        cudaMalloc(&w.err, sizeof(int)) != cudaSuccess) {
+        split_free(w);
+        throw std::runtime_error("split workspace allocation failed");
+    }
+    cudaMemset(w.err, 0, sizeof(int));
+    set_smem_attr<2, 128, 4>();
+    set_smem_attr<3, 128, 4>();
+    set_smem_attr<4, 128, 3>();
+    w.cap_a = ca;
+    w.cap_b = cb;
+    w.cap_mn = sz.mn;
+    w.slices = nslices;
+}
+
+void split_free(SplitWorkspace &w) {
+    if (w.a) cudaFree(w.a);
+    if (w.b) cudaFree(w.b);
+    if (w.ea) cudaFree(w.ea);
+    if (w.eb) cudaFree(w.eb);
+    if (w.err) cudaFree(w.err);
+    w = SplitWorkspace{};
+}
+
+bool split_eligible(const GettArgs &g) {
+    // enough 128 x 128 tiles to fill the GPU and enough K to amortise slicing
+    long long tiles = ((g.M + 127LL) / 128) * ((g.N + 127LL) / 128);
+    return g.M >= 64 && g.N >= 64 && g.K >= 64 && tiles >= 64;
+}
+
+int split_launch_count(const GettArgs &, int) { return 3; }
+
+int split_error(const SplitWorkspace &w) {
+    int h = 0;
+    if (w.err) cudaMemcpy(&h, w.err, sizeof(int), cudaMemcpyDeviceToHost);
+    return h;
+}
+
+int split_gett(SplitWorkspace &w, const GettArgs &g, int, int, int S, cudaStream_t s) {
+    if (S < 2 || S > 4) throw std::runtime_error("split GETT supports 2..4 slices");
+    long long Kp = ((long long)g.K + BKB - 1) / BKB * BKB;
+    long long Mr = g.M, Nr = g.N;
+    if (Mr * Kp * S > w.cap_a || Nr * Kp * S > w.cap_b || Mr > w.cap_mn || Nr > w.cap_mn)
+        throw std::runtime_error("split workspace too small");
+    int blocks_a = (int)std::min<long long>((Mr * 32 + 255) / 256, 148 * 16);
+    int blocks_b = (int)std::min<long long>((Nr * 32 + 255) / 256, 148 * 16);
+    slice_rows_kernel<<<blocks_a, 256, 0, s>>>(g.A, g.offA_m, g.offA_k, g.M, g.K, (int)Kp, S, w.a, Mr * Kp, w.ea);
+    slice_rows_kernel<<<blocks_b, 256, 0, s>>>(g.B, g.offB_n, g.offB_k, g.N, g.K, (int)Kp, S, w.b, Nr * Kp, w.eb);
+    CUtensorMap ta = make_map(w.a, Mr, Kp, S, TM);
+    CUtensorMap tb = make_map(w.b, Nr, Kp, S, tile_n(S));
+    SplitArgs a{g.C, g.offC_m, g.offC_n, w.ea, w.eb, g.M, g.N, g.K, (int)Kp, g.alpha, g.beta, w.err};
+    switch (S) {
+        case 2: launch_split<2, 128, 4>(ta, tb, a, s); break;
+        case 3: launch_split<3, 128, 4>(ta, tb, a, s); break;
+        case 4: launch_split<4, 128, 3>(ta, tb, a, s); break;
+    }
+    return 3;
+}
+
+}  // namespace ccqb

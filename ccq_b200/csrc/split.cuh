@@ -20,6 +20,7 @@ struct SplitWorkspace {
     signed char *b = nullptr;   // slices of B, K-major, [slice][N][Kpad]
     int *ea = nullptr;          // per-row exponents of A
     int *eb = nullptr;          // per-row exponents of B
+    int *err = nullptr;         // set by a kernel whose bounded wait expired
     long long cap_a = 0, cap_b = 0, cap_mn = 0;
     int slices = 0;
 };
@@ -29,5 +30,9 @@ void split_free(SplitWorkspace &w);
 // Runs one GETT in split precision; returns the number of kernels launched.
 int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor, int nslices, cudaStream_t s);
 int split_launch_count(const GettArgs &g, int nslices);
+// Large enough for the tensor-core split path (else FP64 DMMA).
+bool split_eligible(const GettArgs &g);
+// Nonzero when a split kernel gave up waiting (pipeline stall).
+int split_error(const SplitWorkspace &w);
 
 }  // namespace ccqb

@@ -7,7 +7,7 @@ CCSDTQ takes several minutes (the level-4 antisymmetriser search).
 import os
 import sys
 
-from .plan import build_plan
+from .plan import build_plan, plan_flops
 
 HERE = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -17,11 +17,11 @@ def main(methods):
     os.makedirs(out, exist_ok=True)
     for m in methods:
         for rhf in (False, True):
-            p = build_plan(m, rhf)
+            p = build_plan(m, rhf, workers=os.cpu_count())
             name = m + ('_rhf' if rhf else '')
             with open(os.path.join(out, name + '.plan'), 'w') as fh:
                 fh.write(p.text())
-            print(name, len(p.ops), 'ops', f'{p.flops:.3e} FLOP at 40 orbitals')
+            print(name, len(p.ops), 'ops', f'{plan_flops(p):.3e} FLOP per sweep at 40 orbitals', flush=True)
 
 
 if __name__ == '__main__':

@@ -66,9 +66,13 @@ class Gett:
     alpha: float
     beta: int
     tag: str = ''
+    restrict: list = field(default_factory=list)   # label groups enumerated in increasing order
 
     def text(self):
-        return f'GETT {self.alpha!r} {self.beta} {self.c.text()} {self.a.text()} {self.b.text()} {self.tag}'.rstrip()
+        r = ''
+        if self.restrict:
+            r = ' R=' + ';'.join(','.join(g) for g in self.restrict)
+        return f'GETT {self.alpha!r} {self.beta} {self.c.text()} {self.a.text()} {self.b.text()} {self.tag}{r}'.rstrip()
 
 
 @dataclass
@@ -171,6 +175,52 @@ def map_factor(name, labels, spin, undressed=False):
     return sv * so, View(block, axes)
 
 
+def antisym_groups(view):
+    """Label groups in which a stored view is antisymmetric (ordered by axis).
+
+    T blocks: labels on one same-spin run of the occupied or virtual half.
+    VAA/VBB (dressed or not): the bra pair (axes 0,1) and the ket pair (2,3)
+    when both axes cover the same orbital range.  Intermediates: none.
+    """
+    labs = view.labels()
+    if len(set(labs)) != len(labs):
+        return []
+    b = view.buf
+    out = []
+    if b.startswith('T') and len(b) == 3:
+        n = int(b[1])
+        spins = block_spins(b)
+        for half in (0, n):
+            start = 0
+            for k in range(1, n + 1):
+                if k == n or spins[k] != spins[start]:
+                    if k - start >= 2:
+                        out.append(tuple(labs[half + q] for q in range(start, k)))
+                    start = k
+    elif b in ('VAA', 'VBB', 'VAA0', 'VBB0'):
+        for p, q in ((0, 1), (2, 3)):
+            ap, aq = view.axes[p], view.axes[q]
+            if ap.size == aq.size and ap.start == aq.start:
+                out.append((labs[p], labs[q]))
+    return out
+
+
+def _refine(partitions, labels):
+    """Common refinement of label groupings: labels stay together only if grouped in all."""
+    key = {l: () for l in labels}
+    for groups in partitions:
+        gid = {}
+        for k, g in enumerate(groups):
+            for l in g:
+                gid[l] = k
+        for l in labels:
+            key[l] = key[l] + (gid.get(l, ('solo', l)),)
+    buckets = {}
+    for l in labels:
+        buckets.setdefault(key[l], []).append(l)
+    return [tuple(v) for v in buckets.values() if len(v) >= 2]
+
+
 SIZES_C2 = {'oa': 8, 'ob': 8, 'va': 32, 'vb': 32, 'n': 40, '1': 1}
 
 
@@ -190,7 +240,8 @@ def _label_size(views, sizes):
 
 
 class PlanBuilder:
-    def __init__(self, method, rhf=False, est_sizes=None):
+    def __init__(self, method, rhf=False, est_sizes=None, workers=None):
+        self.workers = workers
         self.method = method
         self.rhf = rhf
         self.tranks = wick.METHOD_TRANKS[method]
@@ -201,6 +252,7 @@ class PlanBuilder:
         self.nz = 0
         self.nx = 0
         self.flops = 0
+        self.zgroups = {}
 
     # -- buffers --------------------------------------------------------------
     def buf(self, name, kind, dims):
@@ -282,7 +334,15 @@ class PlanBuilder:
             return memo[key]
 
         spins = {l: espin[l] for l in free[last]}
+        nops, nx = len(self.ops), self.nx
         contribs = self._contribs(last, spins, facs, free, shared, get, undressed)
+        if not contribs:
+            # intermediates built for a product whose final contraction vanishes are dead
+            del self.ops[nops:]
+            for k in range(nx, self.nx):
+                self.buffers.pop(f'X{k}', None)
+            self.nx = nx
+            return beta
         for alpha, xa, tb in contribs:
             self._gett(dst, xa, tb, alpha * float(scale), beta, tag)
             beta = 1
@@ -296,11 +356,11 @@ class PlanBuilder:
         for ds in itertools.product((0, 1), repeat=len(sh)):
             sp = dict(spins)
             sp.update(zip(sh, ds))
-            xs = get(s - 1, {l: sp[l] for l in prevfree})
-            if not xs:
-                continue
             r = map_factor(facs[s][0], facs[s][1], sp, undressed)
             if r is None:
+                continue
+            xs = get(s - 1, {l: sp[l] for l in prevfree})
+            if not xs:
                 continue
             st, tv = r
             for sx, xv in xs:
@@ -333,8 +393,9 @@ class PlanBuilder:
         tspin = {l: s for l, s in zip(ext_o, spins_t)}
         tspin.update({l: s for l, s in zip(ext_v, spins_t)})
         terms = wick.residual_terms(level, self.tranks)
-        groups = wick.orbit_groups(level, terms)
+        groups = wick.orbit_groups(level, terms, workers=self.workers)
         asm = Assemble(block, 'jacobi')
+        block_start = len(self.ops)
         direct = {}
         direct_order = []
         zshare = {}
@@ -367,22 +428,107 @@ class PlanBuilder:
                 if norm in zshare:
                     z, cref, state = zshare[norm]
                     scale = c0 / cref
+                    state[0] = self.emit_chain(base, espin, View(z, zaxes), scale, f'{block}.g{gi}', state[0])
                 else:
+                    nz, nx, nops = self.nz, self.nx, len(self.ops)
                     z = self.new_z([a.size for a in zaxes])
                     state = [0]
-                    cref = c0
-                    scale = Fraction(1)
-                    zshare[norm] = (z, cref, state)
+                    state[0] = self.emit_chain(base, espin, View(z, zaxes), Fraction(1), f'{block}.g{gi}', 0)
+                    if state[0] == 0:
+                        # every spin term of this group vanishes: no buffer, no assemble terms
+                        assert len(self.ops) == nops
+                        del self.buffers[z]
+                        self.nz = nz
+                        continue
+                    zshare[norm] = (z, c0, state)
                     for tau, c in mem_sorted:
                         axes = [Axis(tau[a.label], a.size) for a in zaxes]
                         asm.terms.append((c, View(z, axes)))
-                state[0] = self.emit_chain(base, espin, View(z, zaxes), scale, f'{block}.g{gi}', state[0])
         for key in direct_order:
             c, v = direct[key]
             if c != 0:
                 asm.terms.append((c, v))
-        # drop Z buffers that never received a contribution
+        self._restrict_block(block_start, asm)
         self.ops.append(asm)
+
+    def _op_groups(self, op, zl):
+        grp = []
+        for side in (op.a, op.b):
+            for g in antisym_groups(side):
+                gg = tuple(l for l in g if l in zl)
+                if len(gg) >= 2:
+                    grp.append(gg)
+        return grp
+
+    def _restrict_block(self, start, asm):
+        """Antisymmetry restrictions for the GETTs of one block (ops[start:]).
+
+        Contracted labels forming an antisymmetric group of both operands are
+        summed over increasing tuples (the runtime scales alpha by the group's
+        factorial).  A Z buffer is declared antisymmetric in the label groups
+        that every contribution inherits from one operand; its GETTs then only
+        produce increasing tuples and the assemble step reads Z sorted with sign.
+        An expensive contribution that would lose its own restriction by sharing
+        a Z with less symmetric ones gets a Z buffer of its own.
+        """
+        ops = self.ops[start:]
+        byz = {}
+        for op in ops:
+            if isinstance(op, Gett) and op.c.buf.startswith('Z'):
+                byz.setdefault(op.c.buf, []).append(op)
+
+        def pairs(groups):
+            return frozenset((a, b) for g in groups for a in g for b in g if a < b)
+
+        for z in list(byz):
+            gs = byz[z]
+            zl = gs[0].c.labels()
+            sigs = [pairs(self._op_groups(op, zl)) for op in gs]
+            common = frozenset.intersection(*sigs)
+            moved = {}
+            for op, sg in zip(gs, sigs):
+                m, n, k, _ = gett_count(op, self.sizes)
+                if sg > common and 2 * m * n * k > 1e9:
+                    moved.setdefault(sg, []).append(op)
+            if not moved:
+                continue
+            zterms = [(c, v) for c, v in asm.terms if v.buf == z]
+            keep = [op for op in gs if not any(op in lst for lst in moved.values())]
+            for sg, lst in moved.items():
+                nz = self.new_z(list(self.buffers[z][1]))
+                for op in lst:
+                    op.c = View(nz, op.c.axes)
+                    op.beta = 1
+                lst[0].beta = 0
+                byz[nz] = lst
+                for c, v in zterms:
+                    asm.terms.append((c, View(nz, v.axes)))
+            byz[z] = keep
+            if keep:
+                keep[0].beta = 0
+            else:
+                asm.terms[:] = [(c, v) for c, v in asm.terms if v.buf != z]
+                del self.buffers[z]
+                del byz[z]
+        for z, gs in byz.items():
+            zl = gs[0].c.labels()
+            groups = _refine([self._op_groups(op, zl) for op in gs], zl)
+            if groups:
+                groups = [tuple(sorted(g, key=zl.index)) for g in groups]
+                self.zgroups[z] = [tuple(zl.index(l) for l in g) for g in groups]
+                for op in gs:
+                    op.restrict = op.restrict + [list(g) for g in groups]
+        for op in ops:
+            if not isinstance(op, Gett):
+                continue
+            ka = antisym_groups(op.a)
+            kb = antisym_groups(op.b)
+            kl = set(op.a.labels()) & set(op.b.labels())
+            for ga in ka:
+                for gb in kb:
+                    common = [l for l in ga if l in gb and l in kl]
+                    if len(common) >= 2:
+                        op.restrict = op.restrict + [common]
 
     def emit_dress(self):
         """exp(-T1) H exp(T1): copy undressed blocks, four quarter transforms each."""
@@ -485,7 +631,10 @@ class PlanBuilder:
     def text(self):
         lines = [f'PLAN {self.method} rhf={int(self.rhf)}']
         for name, (kind, dims) in self.buffers.items():
-            lines.append(f'BUF {name} {kind} {len(dims)} ' + ' '.join(dims))
+            g = ''
+            if name in self.zgroups:
+                g = ' G=' + ';'.join(','.join(str(a) for a in grp) for grp in self.zgroups[name])
+            lines.append(f'BUF {name} {kind} {len(dims)} ' + ' '.join(dims) + g)
         lines.append(f'OPS {len(self.ops)}')
         for op in self.ops:
             lines.append(op.text())
@@ -493,5 +642,46 @@ class PlanBuilder:
         return '\n'.join(lines) + '\n'
 
 
-def build_plan(method, rhf=False):
-    return PlanBuilder(method, rhf).build()
+def build_plan(method, rhf=False, workers=None):
+    return PlanBuilder(method, rhf, workers=workers).build()
+
+
+def _choose(n, k):
+    from math import comb
+    return comb(n, k)
+
+
+def gett_count(op, sizes=SIZES_C2):
+    """(M, N, K, alpha scale) of a GETT after its antisymmetry restrictions."""
+    lsz = _label_size([op.a, op.b, op.c], sizes)
+    uniq = lambda ls: list(dict.fromkeys(ls))
+    al, bl, cl = uniq(op.a.labels()), uniq(op.b.labels()), uniq(op.c.labels())
+    ml = [l for l in al if l in cl]
+    nl = [l for l in bl if l in cl]
+    kl = [l for l in al if l in bl]
+    out = []
+    scale = 1
+    for labs in (ml, nl, kl):
+        rest = set(labs)
+        cnt = 1
+        for g in op.restrict:
+            if set(g) <= set(labs):
+                n = lsz[g[0]]
+                cnt *= _choose(n, len(g))
+                rest -= set(g)
+                if labs is kl:
+                    from math import factorial
+                    scale *= factorial(len(g))
+        for l in rest:
+            cnt *= lsz[l]
+        out.append(cnt)
+    return out[0], out[1], out[2], scale
+
+
+def plan_flops(builder, sizes=SIZES_C2):
+    tot = 0
+    for op in builder.ops:
+        if isinstance(op, Gett):
+            m, n, k, _ = gett_count(op, sizes)
+            tot += 2 * m * n * k
+    return tot

@@ -319,7 +319,23 @@ def ext_labels(level):
     return tuple(f'a{k}' for k in range(level)) + tuple(f'i{k}' for k in range(level))
 
 
-def orbit_groups(level, terms):
+def _orbit_key(args):
+    level, tensors = args
+    occ = [f'i{k}' for k in range(level)]
+    vir = [f'a{k}' for k in range(level)]
+    best = None
+    for po in permutations(occ):
+        for pv in permutations(vir):
+            m = dict(zip(occ, po))
+            m.update(zip(vir, pv))
+            key, s = canonical(_relabel(tensors, m))
+            rk = _key_rank(key)
+            if best is None or rk < best[0]:
+                best = (rk, key, s, m)
+    return best[1], best[2], best[3]
+
+
+def orbit_groups(level, terms, workers=None):
     """Group terms related by permutations of external labels.
 
     Returns a list of ``(base_tensors, [(perm_map, coef), ...])``: the term
@@ -327,25 +343,19 @@ def orbit_groups(level, terms):
     to ``perm_map[x]``.  Evaluating ``base`` once per distinct spin pattern and
     adding the permuted copies is the antisymmetriser of the reference's
     generated code (its ``sum_stripe`` calls with permutation strings).
+    ``workers`` > 1 spreads the search over processes (level 4 has 576
+    external permutations per term).
     """
-    occ = [f'i{k}' for k in range(level)]
-    vir = [f'a{k}' for k in range(level)]
-    perms = []
-    for po in permutations(occ):
-        for pv in permutations(vir):
-            m = dict(zip(occ, po))
-            m.update(zip(vir, pv))
-            perms.append(m)
+    args = [(level, tensors) for _, tensors in terms]
+    if workers and workers > 1 and len(terms) > 50:
+        import multiprocessing as mp
+        with mp.get_context('spawn').Pool(workers) as pool:
+            keys = pool.map(_orbit_key, args, chunksize=8)
+    else:
+        keys = [_orbit_key(a) for a in args]
     groups = {}
     order = []
-    for coef, tensors in terms:
-        best = None
-        for m in perms:
-            key, s = canonical(_relabel(tensors, m))
-            rk = _key_rank(key)
-            if best is None or rk < best[0]:
-                best = (rk, key, s, m)
-        _, key, s, m = best
+    for (coef, tensors), (key, s, m) in zip(terms, keys):
         # tensors relabelled by m equals s * B  =>  tensors = s * (B relabelled by m^-1)
         inv = {v: k for k, v in m.items()}
         if key not in groups:

@@ -35,6 +35,7 @@ class Dims(C.Structure):
 
 SIGNATURES = {
     'ccq_b200_egemm': (C.c_int, [I64, I64, I64, DP, DP, DP]),
+    'ccq_b200_egemm_split': (C.c_int, [I64, I64, I64, DP, DP, DP, I64]),
     'ccq_b200_egemm1': (C.c_int, [I64, I64, DP, DP, DP]),
     'ccq_b200_egemm2': (C.c_int, [I64, I64, DP, DP, DP]),
     'ccq_b200_init': (C.c_int, [C.POINTER(Dims), C.c_char_p, DP, DP, DP, DP, DP, I64, C.c_double, I64,
@@ -42,6 +43,7 @@ SIGNATURES = {
     'ccq_b200_sizes': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(I64)]),
     'ccq_b200_set_t': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_get_t': (C.c_int, [C.c_void_p, DP, I64]),
+    'ccq_b200_block': (C.c_int, [C.c_void_p, C.c_char_p, DP, I64, I64]),
     'ccq_b200_update': (C.c_int, [C.c_void_p]),
     'ccq_b200_energy': (C.c_int, [C.c_void_p, DP]),
     'ccq_b200_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
@@ -92,6 +94,16 @@ def egemm(k1, k2, k3, A, B):
     return Cm
 
 
+def egemm_split(k1, k2, k3, A, B, nslices=4):
+    """egemm with int8 Ozaki slices on the tcgen05 tensor pipe."""
+    lib = load()
+    A = np.asfortranarray(A, dtype=np.float64).reshape((k3, k1), order='F')
+    B = np.asfortranarray(B, dtype=np.float64).reshape((k3, k2), order='F')
+    Cm = np.zeros((k2, k1), order='F')
+    _err(lib.ccq_b200_egemm_split(k1, k2, k3, _p(A), _p(B), _p(Cm), nslices))
+    return Cm
+
+
 def egemm1(k1, k3, A, B):
     lib = load()
     A = np.asfortranarray(A, dtype=np.float64).reshape((k3, k1), order='F')
@@ -137,6 +149,15 @@ class Context:
         t = np.empty(self.t_size)
         _err(self._lib.ccq_b200_get_t(self.ptr, _p(t), t.size))
         return t
+
+    def get_block(self, name, shape):
+        out = np.empty(shape)
+        _err(self._lib.ccq_b200_block(self.ptr, name.encode(), _p(out), out.size, 0))
+        return out
+
+    def set_block(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        _err(self._lib.ccq_b200_block(self.ptr, name.encode(), _p(a), a.size, 1))
 
     def update(self):
         _err(self._lib.ccq_b200_update(self.ptr))

@@ -1,0 +1,56 @@
+"""Single-kernel probes for profiling (one GETT launch of a fixed shape).
+
+    python -m ccq_b200.probe egemm K1 K2 K3 [repeats]
+
+Runs ccq_b200_egemm (the FP64 GETT kernel) on random column-major operands;
+the vvvv ladder of the CCSDT T3 update at 40 orbitals is (1024, 16384, 1024).
+"""
+import sys
+import time
+
+import numpy as np
+
+
+def main(argv):
+    from ccq_b200 import lib
+    kind = argv[0]
+    if kind == 'egemm':
+        k1, k2, k3 = (int(x) for x in argv[1:4])
+        rep = int(argv[4]) if len(argv) > 4 else 1
+        rng = np.random.default_rng(0)
+        A = np.asfortranarray(rng.normal(size=(k3, k1)))
+        B = np.asfortranarray(rng.normal(size=(k3, k2)))
+        for _ in range(rep):
+            t0 = time.perf_counter()
+            C = lib.egemm(k1, k2, k3, A, B)
+            dt = time.perf_counter() - t0
+        ref = B[:, :64].T @ A[:, :64]
+        err = float(np.abs(C[:64, :64] - ref).max())
+        print(f'egemm {k1}x{k2}x{k3}: wall {dt * 1e3:.2f} ms (incl. copies), max err {err:.2e}')
+        assert err < 1e-9
+    elif kind == 'sweep':
+        # per-operation device times of one CCSDT sweep on the 40-orbital workload
+        import os
+        from ccq_b200 import synth
+        prec = argv[1] if len(argv) > 1 else 'fp64'
+        out = argv[2] if len(argv) > 2 else 'ops_profile.txt'
+        s = synth.system(synth.C2)
+        d = s['dims']
+        ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CCSDT', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                          s['v_bb'])
+        ctx.set_precision(lib.PREC_SPLIT if prec == 'split' else lib.PREC_FP64, 4)
+        for it in range(1, 4):
+            ctx.iterate(it)
+        if os.path.exists(out):
+            os.remove(out)
+        os.environ['CCQ_B200_PROFILE_DUMP'] = out
+        ctx.profile(True)
+        ctx.iterate(4)
+        print(ctx.profile_get())
+        ctx.close()
+    else:
+        raise SystemExit(f'unknown probe {kind}')
+
+
+if __name__ == '__main__':
+    main(sys.argv[1:])

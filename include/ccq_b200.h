@@ -65,6 +65,13 @@ int ccq_b200_egemm1(int64_t k1, int64_t k3, const double *A, const double *B, do
 /* Replaces egemm2 (src/dgemm.f90:59-73): C(k2) = B(k3,k2)^T A(k3). */
 int ccq_b200_egemm2(int64_t k2, int64_t k3, const double *A, const double *B, double *C);
 
+/* egemm in split precision: FP64 operands cut into nslices (2..4) int8
+ * slices with a power-of-two scale per row, slice products on the tcgen05
+ * tensor pipe with INT32 accumulation, recombined in FP64.  Absolute error
+ * about nslices * 2^(-7 nslices - 5) * k3 * max|A col| * max|B col|. */
+int ccq_b200_egemm_split(int64_t k1, int64_t k2, int64_t k3,
+                         const double *A, const double *B, double *C, int64_t nslices);
+
 /* Fortran link-level drop-ins with gfortran's names and by-reference
  * arguments (ILP64 integers): link libccq_b200 in place of dgemm.o. */
 void egemm_(const int64_t *k1, const int64_t *k2, const int64_t *k3,
@@ -94,6 +101,12 @@ int ccq_b200_sizes(const ccq_b200_ctx *ctx, int64_t *t_size, int64_t *vec_size);
 /* Copy the whole T vector (cc%t_vec layout) to / from the device. */
 int ccq_b200_set_t(ccq_b200_ctx *ctx, const double *t_vec, int64_t n);
 int ccq_b200_get_t(const ccq_b200_ctx *ctx, double *t_vec, int64_t n);
+
+/* Copy one amplitude block ("T1A".."T3D" inside t_vec, or the T4 blocks
+ * "T4A".."T4E" that the reference keeps in its T4 scratch files,
+ * cc_utils.f90:89-168) to the device (to_device=1) or back (0).  n must equal
+ * the block's element count; layout as the reference's Fortran array. */
+int ccq_b200_block(ccq_b200_ctx *ctx, const char *name, double *host, int64_t n, int64_t to_device);
 
 /* One sweep of update_clusters_t4 (update_cc.F90:12-323): the update_ptr
  * slot.  Blocks are updated in place in the reference's order. */

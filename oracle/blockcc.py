@@ -40,14 +40,15 @@ def parse_plan(text):
     while lines[k].startswith('BUF'):
         p = lines[k].split()
         nd = int(p[3])
-        plan['buffers'][p[1]] = (p[2], p[4:4 + nd])
+        plan['buffers'][p[1]] = (p[2], p[4:4 + nd])   # a trailing G= (antisymmetric axes) is a GPU hint
         k += 1
     assert lines[k].startswith('OPS')
     k += 1
     while lines[k] != 'END':
         p = lines[k].split()
         if p[0] == 'GETT':
-            tag = p[6] if len(p) > 6 else ''
+            # a trailing R= token restricts index tuples on the GPU; the full sum is identical
+            tag = p[6] if len(p) > 6 and not p[6].startswith('R=') else ''
             plan['ops'].append(('GETT', float(p[1]), int(p[2]), parse_view(p[3]), parse_view(p[4]), parse_view(p[5]), tag))
             k += 1
         elif p[0] == 'ASSEMBLE':
@@ -62,6 +63,27 @@ def parse_plan(text):
             plan['ops'].append(tuple(p))
             k += 1
     return plan
+
+
+def check_written_before_read(plan):
+    """Every work buffer (Z*, X*) must be overwritten (beta=0) before it is read."""
+    written = set()
+    for op in plan['ops']:
+        if op[0] == 'GETT':
+            _, alpha, beta, cv, av, bv, tag = op
+            for v in (av, bv):
+                if v[0][0] in 'ZX' and v[0] not in written:
+                    raise ValueError(f'{v[0]} read before written')
+            if cv[0][0] in 'ZX':
+                if beta and cv[0] not in written:
+                    raise ValueError(f'{cv[0]} accumulated before written')
+                written.add(cv[0])
+        elif op[0] == 'ASSEMBLE':
+            for _, v in op[3]:
+                if v[0][0] in 'ZX' and v[0] not in written:
+                    raise ValueError(f'{v[0]} read by assemble before written')
+        elif op[0] == 'PHASE':
+            written = set()
 
 
 class BlockCC:
@@ -96,6 +118,7 @@ class BlockCC:
         self.fdiag_b = np.diag(fb).copy()
         self.flops = 0
         self.count_flops = count_flops
+        check_written_before_read(self.plan)
 
     def _array(self, name, tvec):
         if name in self.layout.shape:

@@ -46,6 +46,31 @@ def test_sweep_parity(method, rhf, n, oa, ob, plan_text):
     ctx.close()
 
 
+@pytest.mark.parametrize('rhf', [False, True])
+def test_sweep_parity_ccsdtq(plan_text, rhf):
+    s = random_system(5, 2, 2, seed=17)
+    ctx = make_ctx(s, 'CCSDTQ', rhf, shift=0.05)
+    bc = BlockCC(plan_text('CCSDTQ', rhf), s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], s['dims'],
+                 'CCSDTQ', shift=0.05)
+    t, t4 = random_t(s['dims'], seed=4, scale=0.03, nmax=4)
+    ctx.set_t(t)
+    for b, v in t4.items():
+        ctx.set_block(b, v)
+        bc.buf[b][...] = v
+    tc = t.copy()
+    for sweep in range(2):
+        ctx.update()
+        bc.update(tc)
+        tg = ctx.get_t()
+        lay = I.TLayout(s['dims'])
+        for b in I.T_VEC_ORDER:
+            np.testing.assert_allclose(lay.view(tg, b), lay.view(tc, b), atol=1e-12, rtol=0, err_msg=f'{b} sweep {sweep}')
+        for b in t4:
+            np.testing.assert_allclose(ctx.get_block(b, t4[b].shape), bc.buf[b], atol=1e-12, rtol=0,
+                                       err_msg=f'{b} sweep {sweep}')
+    ctx.close()
+
+
 def _cfg(method, tol=1e-10, ds=5, rhf=False, graph=True, max_iter=100):
     c = config.Config(calc_type=method, tol=tol, diis_space=ds, rhf=rhf, max_iter=max_iter, gpu_graph=graph)
     return c.calc_macros()
