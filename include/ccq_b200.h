@@ -79,6 +79,22 @@ void egemm_(const int64_t *k1, const int64_t *k2, const int64_t *k3,
 void egemm1_(const int64_t *k1, const int64_t *k3, const double *A, const double *B, double *C);
 void egemm2_(const int64_t *k2, const int64_t *k3, const double *A, const double *B, double *C);
 
+/* egemm on device buffers for callers that cannot allocate device memory.
+ * No counterpart in the reference.  Some hosts own all of the GPU's memory
+ * through their own pool allocator, or run a time-critical loop in which a
+ * cudaMalloc/cudaFree would synchronise the device; this entry point makes no
+ * allocation of any kind.  A, B, C are device pointers in the column-major
+ * layout of ccq_b200_egemm (C(k2,k1) = B(k3,k2)^T A(k3,k1)); stream is a
+ * cudaStream_t (NULL: legacy default stream) and the call only enqueues work
+ * on it.  Its scratch (GETT offset tables) is a fixed 1.5 MiB array that each
+ * GPU holds from library load until process exit, so k1, k2 and k3 must each
+ * be at most 65536 (else CCQ_B200_ERANGE, nothing enqueued).  The first call on
+ * a device looks up that array's address; make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (different streams, no ordering between them) race on it. */
+int ccq_b200_egemm_dev_noalloc(int64_t k1, int64_t k2, int64_t k3,
+                               const double *A, const double *B, double *C, void *stream);
+
 /* ---- level 2: resident solver ------------------------------------------- */
 
 /* Builds a context for calc_type "CCSD", "CCSDT" or "CCSDTQ"
