@@ -58,62 +58,46 @@ __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *
     }
 }
 
+// K loop of one contraction term over [kbeg, kend): 2-stage cp.async pipeline.
 template <bool AK, bool BKM>
-__global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
-    constexpr int TILE = BKT * (BM + PADS);
-    __shared__ __align__(16) double smem[4 * TILE];
-    double (*As)[BKT][BM + PADS] = reinterpret_cast<double (*)[BKT][BM + PADS]>(smem);
-    double (*Bs)[BKT][BN + PADS] = reinterpret_cast<double (*)[BKT][BN + PADS]>(smem + 2 * TILE);
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int gid = lane >> 2, tig = lane & 3;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-    const int kbeg = blockIdx.z * g.kchunk;
-    const int kend = min(g.K, kbeg + g.kchunk);
-
+__device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*As)[BKT][BM + PADS],
+                                              double (*Bs)[BKT][BN + PADS], const double *A, const double *B,
+                                              const int *offA_m, const int *offA_k, const int *offB_n,
+                                              const int *offB_k, int M, int N, int m0, int n0, int kbeg, int kend,
+                                              int tid, int wm, int wn, int gid, int tig) {
     int offa[8], offb[8];
     if (AK) {
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
             int m = m0 + (tid >> 4) + 8 * p;
-            offa[p] = m < g.M ? __ldg(g.offA_m + m) : 0;
+            offa[p] = m < M ? __ldg(offA_m + m) : 0;
         }
     } else {
         int m = m0 + (tid & 63);
-        offa[0] = m < g.M ? __ldg(g.offA_m + m) : 0;
+        offa[0] = m < M ? __ldg(offA_m + m) : 0;
     }
     if (BKM) {
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
             int n = n0 + (tid >> 4) + 8 * p;
-            offb[p] = n < g.N ? __ldg(g.offB_n + n) : 0;
+            offb[p] = n < N ? __ldg(offB_n + n) : 0;
         }
     } else {
         int n = n0 + (tid & 63);
-        offb[0] = n < g.N ? __ldg(g.offB_n + n) : 0;
+        offb[0] = n < N ? __ldg(offB_n + n) : 0;
     }
-
-    double acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
-
     const int ntiles = kend > kbeg ? (kend - kbeg + BKT - 1) / BKT : 0;
     if (ntiles > 0) {
-        load_tile<AK>(As[0], g.A, offa, g.offA_k, m0, g.M, kbeg, kend, tid);
-        load_tile<BKM>(Bs[0], g.B, offb, g.offB_k, n0, g.N, kbeg, kend, tid);
+        load_tile<AK>(As[0], A, offa, offA_k, m0, M, kbeg, kend, tid);
+        load_tile<BKM>(Bs[0], B, offb, offB_k, n0, N, kbeg, kend, tid);
         cp_async_commit();
     }
     for (int t = 0; t < ntiles; ++t) {
         const int st = t & 1;
         if (t + 1 < ntiles) {
             int k0 = kbeg + (t + 1) * BKT;
-            load_tile<AK>(As[st ^ 1], g.A, offa, g.offA_k, m0, g.M, k0, kend, tid);
-            load_tile<BKM>(Bs[st ^ 1], g.B, offb, g.offB_k, n0, g.N, k0, kend, tid);
+            load_tile<AK>(As[st ^ 1], A, offa, offA_k, m0, M, k0, kend, tid);
+            load_tile<BKM>(Bs[st ^ 1], B, offb, offB_k, n0, N, k0, kend, tid);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
@@ -137,6 +121,52 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
         }
         __syncthreads();
     }
+}
+
+template <bool AK, bool BKM>
+__global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
+    constexpr int TILE = BKT * (BM + PADS);
+    __shared__ __align__(16) double smem[4 * TILE];
+    double (*As)[BKT][BM + PADS] = reinterpret_cast<double (*)[BKT][BM + PADS]>(smem);
+    double (*Bs)[BKT][BN + PADS] = reinterpret_cast<double (*)[BKT][BN + PADS]>(smem + 2 * TILE);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+
+    double acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+    double alpha = g.alpha;
+    if (g.segs) {
+        // grouped: sum_s alpha_s A_s B_s^T, rescaling the running sum between terms
+        for (int sgi = 0; sgi < g.nseg; ++sgi) {
+            const GettSeg sg = g.segs[sgi];
+            if (sgi > 0) {
+                double r = g.segs[sgi - 1].alpha / sg.alpha;
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[i][j][q] *= r;
+            }
+            gett_mainloop<AK, BKM>(acc, As, Bs, sg.A, sg.B, sg.offA_m, sg.offA_k, sg.offB_n, sg.offB_k, g.M, g.N, m0,
+                                   n0, 0, sg.K, tid, wm, wn, gid, tig);
+            alpha = sg.alpha;
+        }
+    } else {
+        const int kbeg = blockIdx.z * g.kchunk;
+        const int kend = min(g.K, kbeg + g.kchunk);
+        gett_mainloop<AK, BKM>(acc, As, Bs, g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k, g.M, g.N, m0, n0, kbeg,
+                               kend, tid, wm, wn, gid, tig);
+    }
 
     // epilogue: stage the tile in shared memory, then write along the output's
     // contiguous mode (g.c_nfast) so that stores and the beta read coalesce
@@ -150,7 +180,7 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
             for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
                 for (int j = 0; j < 2; ++j)
-                    Cs[wm + mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = g.alpha * acc[mi][ni][2 * h + j];
+                    Cs[wm + mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = alpha * acc[mi][ni][2 * h + j];
     __syncthreads();
     const bool atomic = gridDim.z > 1;
     const int fast = tid & 63, slow0 = tid >> 6;
@@ -171,7 +201,7 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
 }
 
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
-    dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, (a.K + a.kchunk - 1) / a.kchunk);
+    dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, a.segs ? 1 : (a.K + a.kchunk - 1) / a.kchunk);
     if (grid.z == 0) grid.z = 1;
     if (a_kmajor && b_kmajor)
         gett_f64_kernel<true, true><<<grid, 128, 0, s>>>(a);
@@ -208,14 +238,12 @@ __global__ void assemble_kernel(AsmArgs a) {
          lin += (long long)gridDim.x * blockDim.x) {
         int x[MAXR];
         long long r = lin;
-        for (int d = a.rank - 1; d >= 0; --d) {
-            x[d] = (int)(r % a.dims[d]);
-            r /= a.dims[d];
+        for (int q = a.nruns - 1; q >= 0; --q) {
+            int c = (int)(r % a.run_count[q]);
+            r /= a.run_count[q];
+            const unsigned char *tup = a.combos + a.run_off[q] + c * a.run_len[q];
+            for (int l = 0; l < a.run_len[q]; ++l) x[a.run_axis0[q] + l] = tup[l];
         }
-        bool canon = true;
-        for (int d = 1; d < a.rank; ++d)
-            if (!a.runstart[d] && x[d] <= x[d - 1]) canon = false;
-        if (!canon) continue;
         double R = 0.0;
         for (int t = 0; t < a.nterms; ++t) {
             const AsmTerm &tm = a.terms[t];

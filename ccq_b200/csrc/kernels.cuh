@@ -19,6 +19,16 @@ namespace ccqb {
 constexpr int MAXR = 8;        // max tensor rank (T4 blocks)
 constexpr int MAX_TERMS = 65536; // max views gathered by one assemble
 
+// One (A, B, K, alpha) term of a grouped GETT: several contractions that add
+// into the same output view run as one launch, so the output is read and
+// written once instead of once per contraction.
+struct GettSeg {
+    const double *A, *B;
+    const int *offA_m, *offA_k, *offB_n, *offB_k;
+    int K;
+    double alpha;
+};
+
 struct GettArgs {
     const double *A;
     const double *B;
@@ -29,6 +39,8 @@ struct GettArgs {
     int beta;       // 0: overwrite, 1: accumulate
     int kchunk;     // K range handled by one blockIdx.z (split-K, atomic epilogue)
     int c_nfast;    // 1: output contiguous along n (write-out walks n), 0: along m
+    const GettSeg *segs;  // grouped launch: nseg terms (A, B, tables, K, alpha above unused)
+    int nseg;
 };
 
 constexpr int MAXG = 4;  // antisymmetric axis groups per source view
@@ -64,7 +76,13 @@ struct AsmArgs {
     int nperm;                // orbit permutations of a canonical element
     const signed char *perm;  // nperm x rank axis maps
     const signed char *psign; // nperm signs
-    long long total;
+    long long total;          // number of canonical elements
+    // canonical elements are enumerated run by run (a run = same-spin axes of one
+    // half); run r covers axes [run_axis0[r], run_axis0[r] + run_len[r]) and has
+    // run_count[r] increasing tuples stored at combos + run_off[r]
+    int nruns;
+    int run_axis0[MAXR], run_len[MAXR], run_count[MAXR], run_off[MAXR];
+    const unsigned char *combos;
 };
 
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s);

@@ -102,6 +102,10 @@ struct Op {
     bool zero_first = false;
     bool split = false;        // eligible for split precision
     long long mnk[3] = {0, 0, 0};
+    bool skip = false;         // member of a grouped GETT run by a later op
+    double group_flops = 0.0;  // FLOPs of a grouped launch (leader only)
+    int group_size = 0;
+    std::vector<int> hcm, hcn; // output offset tables (grouping key)
     AsmArgs asmargs{};
 };
 
@@ -472,6 +476,7 @@ void instantiate(ccq_b200_ctx *c) {
     std::vector<Pend> pend;
     std::vector<AsmTerm> hterms;
     std::vector<signed char> hperm, hsign;
+    std::vector<unsigned char> hcomb;
     struct PendA {
         size_t op, t0, p0;
     };
@@ -501,6 +506,29 @@ void instantiate(ccq_b200_ctx *c) {
             }
             for (auto &l : kl)
                 if (B.extent[l] != A.extent[l]) throw Error(CCQ_B200_EPLAN, "extent mismatch for label " + l);
+            // Order each mode's labels so that the tensor dominating that mode's traffic is
+            // walked along its contiguous axis: C for the small-K updates of large
+            // outputs, the operands otherwise (the last label of a mode varies fastest).
+            {
+                auto prod = [&](const std::vector<std::string> &v) {
+                    double x = 1;
+                    for (auto &l : v) x *= (double)ext[l];
+                    return x;
+                };
+                double Mx = prod(ml), Nx = prod(nl), Kx = prod(kl);
+                auto by = [&](std::vector<std::string> &v, const Resolved &X) {
+                    std::stable_sort(v.begin(), v.end(), [&](const std::string &a, const std::string &b) {
+                        return X.stride.at(a) > X.stride.at(b);
+                    });
+                };
+                double tC = Mx * Nx * (o.beta ? 2.0 : 1.0);
+                // large-K contractions are operand bound (and may run split, whose
+                // slicers read rows along the operand's contiguous axis)
+                bool opnd = Kx >= 256;
+                if (!opnd && tC >= Mx * Kx) by(ml, C); else by(ml, A);
+                if (!opnd && tC >= Nx * Kx) by(nl, C); else by(nl, B);
+                if (Mx >= Nx) by(kl, A); else by(kl, B);
+            }
             // restriction groups: each must lie entirely in one index mode
             double kscale = 1.0;
             for (auto &g : o.restrict_groups) {
@@ -521,6 +549,8 @@ void instantiate(ccq_b200_ctx *c) {
             build_table(ml, ext, A, &C, o.restrict_groups, am, cm);
             build_table(kl, ext, A, &B, o.restrict_groups, ak, bk);
             build_table(nl, ext, B, &C, o.restrict_groups, bn, cn);
+            o.hcm = cm;
+            o.hcn = cn;
             if (ml.empty()) { am.assign(1, 0); cm.assign(1, 0); }
             if (nl.empty()) { bn.assign(1, 0); cn.assign(1, 0); }
             if (kl.empty()) { ak.assign(1, 0); bk.assign(1, 0); }
@@ -682,6 +712,32 @@ void instantiate(ccq_b200_ctx *c) {
                 if (r == rp.size()) break;
             }
             a.nperm = np;
+            // canonical enumeration tables: increasing tuples of every run
+            a.nruns = (int)runs.size();
+            a.total = 1;
+            for (size_t r = 0; r < runs.size(); ++r) {
+                int L = (int)runs[r].size(), n = a.dims[runs[r][0]];
+                if (n > 255) throw Error(CCQ_B200_ERANGE, "orbital extent above 255");
+                a.run_axis0[r] = runs[r][0];
+                a.run_len[r] = L;
+                a.run_off[r] = (int)hcomb.size();
+                std::vector<int> t(L);
+                for (int l = 0; l < L; ++l) t[l] = l;
+                int cnt = 0;
+                if (L <= n) {
+                    while (true) {
+                        for (int l = 0; l < L; ++l) hcomb.push_back((unsigned char)t[l]);
+                        ++cnt;
+                        int l = L - 1;
+                        while (l >= 0 && t[l] == n - L + l) --l;
+                        if (l < 0) break;
+                        ++t[l];
+                        for (int q = l + 1; q < L; ++q) t[q] = t[q - 1] + 1;
+                    }
+                }
+                a.run_count[r] = cnt;
+                a.total *= cnt;
+            }
             penda.push_back(pa);
         }
     }
@@ -696,15 +752,83 @@ void instantiate(ccq_b200_ctx *c) {
         o.g.offC_m = dtab + p.cm;
         o.g.offC_n = dtab + p.cn;
     }
+    // Group small-K contractions that add into the same Z view (consecutive writers
+    // of that Z within one block phase, identical output tables): one launch per
+    // group at the position of its last member.  Their operands are not modified
+    // later in the phase and Z is only read by the closing assemble, so moving the
+    // earlier members later is safe.
+    {
+        std::vector<GettSeg> hsegs;
+        std::vector<std::pair<size_t, size_t>> leaders;
+        auto groupable = [&](const Op &o) {
+            return o.kind == OP_GETT && o.g.M > 0 && o.g.N > 0 && o.g.K > 0 && o.g.K < 256 && !o.zero_first &&
+                   (o.g.K + o.g.kchunk - 1) / o.g.kchunk == 1 && o.c.buf[0] == 'Z';
+        };
+        size_t b = 0;
+        while (b < c->plan.ops.size()) {
+            size_t e = b + 1;
+            while (e < c->plan.ops.size() && c->plan.ops[e].kind != OP_PHASE) ++e;
+            std::map<std::string, std::vector<size_t>> writers;
+            for (size_t i = b; i < e; ++i) {
+                Op &o = c->plan.ops[i];
+                if (o.kind == OP_GETT && o.c.buf[0] == 'Z') writers[o.c.buf].push_back(i);
+            }
+            for (auto &wz : writers) {
+                auto &lst = wz.second;
+                size_t k = 0;
+                while (k < lst.size()) {
+                    size_t j = k + 1;
+                    Op &f = c->plan.ops[lst[k]];
+                    if (groupable(f)) {
+                        while (j < lst.size()) {
+                            Op &q = c->plan.ops[lst[j]];
+                            if (!groupable(q) || q.g.C != f.g.C || q.hcm != f.hcm || q.hcn != f.hcn ||
+                                q.g.c_nfast != f.g.c_nfast)
+                                break;
+                            ++j;
+                        }
+                    }
+                    if (j - k >= 2) {
+                        size_t off = hsegs.size();
+                        double fl = 0.0;
+                        for (size_t q = k; q < j; ++q) {
+                            Op &m = c->plan.ops[lst[q]];
+                            hsegs.push_back(GettSeg{m.g.A, m.g.B, m.g.offA_m, m.g.offA_k, m.g.offB_n, m.g.offB_k,
+                                                    m.g.K, m.g.alpha});
+                            fl += 2.0 * m.mnk[0] * m.mnk[1] * m.mnk[2];
+                            if (q + 1 < j) m.skip = true;
+                        }
+                        Op &lead = c->plan.ops[lst[j - 1]];
+                        lead.g.beta = f.beta;
+                        lead.g.nseg = (int)(j - k);
+                        lead.group_flops = fl;
+                        lead.group_size = (int)(j - k);
+                        leaders.push_back({lst[j - 1], off});
+                    }
+                    k = j;
+                }
+            }
+            b = e;
+        }
+        if (!hsegs.empty()) {
+            GettSeg *dsegs = (GettSeg *)c->dalloc(sizeof(GettSeg) * hsegs.size());
+            CK(cudaMemcpyAsync(dsegs, hsegs.data(), sizeof(GettSeg) * hsegs.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+            for (auto &l : leaders) c->plan.ops[l.first].g.segs = dsegs + l.second;
+        }
+    }
     AsmTerm *dterms = (AsmTerm *)c->dalloc(sizeof(AsmTerm) * std::max<size_t>(hterms.size(), 1));
     CK(cudaMemcpyAsync(dterms, hterms.data(), sizeof(AsmTerm) * hterms.size(), cudaMemcpyHostToDevice, c->stream));
     signed char *dperm = (signed char *)c->dalloc(std::max<size_t>(hperm.size(), 1));
     signed char *dsign = (signed char *)c->dalloc(std::max<size_t>(hsign.size(), 1));
     CK(cudaMemcpyAsync(dperm, hperm.data(), hperm.size(), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(dsign, hsign.data(), hsign.size(), cudaMemcpyHostToDevice, c->stream));
+    unsigned char *dcomb = (unsigned char *)c->dalloc(std::max<size_t>(hcomb.size(), 1));
+    CK(cudaMemcpyAsync(dcomb, hcomb.data(), hcomb.size(), cudaMemcpyHostToDevice, c->stream));
     {
         size_t signs_before = 0;
         for (auto &p : penda) {
+            c->plan.ops[p.op].asmargs.combos = dcomb;
             Op &o = c->plan.ops[p.op];
             o.asmargs.terms = dterms + p.t0;
             o.asmargs.perm = dperm + p.p0;
@@ -737,7 +861,7 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
         if (prof) CK(cudaEventRecord(c->pev[2 * i], c->stream));
         switch (o.kind) {
             case OP_GETT:
-                if (o.g.M == 0 || o.g.N == 0) break;
+                if (o.skip || o.g.M == 0 || o.g.N == 0) break;
                 if (o.zero_first) {
                     launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, c->stream);
                     ++c->launches;
@@ -784,17 +908,18 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
         FILE *df = dump ? fopen(dump, "a") : nullptr;
         for (size_t i = from; i < to; ++i) {
             Op &o = c->plan.ops[i];
-            if (o.kind == OP_PHASE) continue;
+            if (o.kind == OP_PHASE || (o.kind == OP_GETT && o.skip)) continue;
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, c->pev[2 * i], c->pev[2 * i + 1]));
             int k = op_class(c, o);
             c->prof_ms[k] += ms;
             c->prof_launch[k] += 1;
-            if (o.kind == OP_GETT) c->prof_flops[k] += 2.0 * o.mnk[0] * o.mnk[1] * o.mnk[2];
+            if (o.kind == OP_GETT)
+                c->prof_flops[k] += o.group_size ? o.group_flops : 2.0 * o.mnk[0] * o.mnk[1] * o.mnk[2];
             if (df) {
                 if (o.kind == OP_GETT)
-                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f\n", i, k, o.tag.c_str(), o.mnk[0], o.mnk[1],
-                            o.mnk[2], o.akm, o.bkm, o.beta, ms);
+                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f %d\n", i, k, o.tag.c_str(), o.mnk[0],
+                            o.mnk[1], o.mnk[2], o.akm, o.bkm, o.beta, ms, o.group_size);
                 else if (o.kind == OP_ASM)
                     fprintf(df, "%zu ASM %d %s %d %.6f\n", i, k, o.block.c_str(), o.asmargs.nterms, ms);
                 else
@@ -831,7 +956,7 @@ void sweep(ccq_b200_ctx *c) {
 long long count_sweep_launches(ccq_b200_ctx *c) {
     long long n = 0;
     for (auto &o : c->plan.ops) {
-        if (o.kind == OP_GETT && o.g.M && o.g.N) {
+        if (o.kind == OP_GETT && o.g.M && o.g.N && !o.skip) {
             if (o.zero_first || o.g.K == 0) ++n;
             if (o.g.K)
                 n += (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g))

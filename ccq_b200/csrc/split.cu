@@ -60,6 +60,67 @@ __global__ void slice_rows_kernel(const double *base, const int *offr, const int
     }
 }
 
+// Rows contiguous in memory (consecutive r -> consecutive addresses): a CTA
+// takes 32 rows, reads them 32 at a time (coalesced), reduces the row maxima in
+// shared memory, then slices 64-wide K chunks through a shared-memory tile so
+// that every row's K-major int8 bytes are written as contiguous 64 B segments.
+constexpr int SR = 32;    // rows per CTA
+constexpr int SK = 64;    // K per chunk
+__global__ void __launch_bounds__(256) slice_rows_tiled_kernel(const double *base, const int *offr, const int *offk,
+                                                               int R, int K, int Kp, int S, signed char *out,
+                                                               long long slice_stride, int *expo) {
+    __shared__ double red[8][SR];
+    __shared__ int esh[SR];
+    __shared__ __align__(16) signed char tile[MAX_SLICES][SR][SK];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int r0 = blockIdx.x * SR; r0 < R; r0 += gridDim.x * SR) {
+        const int r = r0 + lane;
+        const bool rin = r < R;
+        const long long orow = rin ? offr[r] : 0;
+        double mx = 0.0;
+        if (rin)
+            for (int k = w; k < K; k += 8) mx = fmax(mx, fabs(base[orow + offk[k]]));
+        red[w][lane] = mx;
+        __syncthreads();
+        if (w == 0) {
+            double m = red[0][lane];
+            for (int q = 1; q < 8; ++q) m = fmax(m, red[q][lane]);
+            int e = 0;
+            if (m > 0.0) frexp(m, &e);
+            esh[lane] = e;
+            if (rin) expo[r] = e;
+        }
+        __syncthreads();
+        const double scale = ldexp(1.0, -esh[lane]);
+        for (int k0 = 0; k0 < Kp; k0 += SK) {
+            for (int j = 0; j < SK / 8; ++j) {
+                int kk = w + 8 * j;
+                int k = k0 + kk;
+                double x = (rin && k < K) ? base[orow + offk[k]] * scale : 0.0;
+                double t = x * 64.0;
+                for (int q = 0; q < S; ++q) {
+                    double sv = rint(t);
+                    tile[q][lane][kk] = (signed char)sv;
+                    t = (t - sv) * 128.0;
+                }
+            }
+            __syncthreads();
+            // write-out: each row's 64 bytes per slice, as 16 words of 4 bytes
+            for (int idx = threadIdx.x; idx < S * SR * (SK / 4); idx += blockDim.x) {
+                int q = idx / (SR * (SK / 4));
+                int rem = idx % (SR * (SK / 4));
+                int rr = rem / (SK / 4), wd = rem % (SK / 4);
+                if (r0 + rr < R && k0 + wd * 4 < Kp) {
+                    const int *src = reinterpret_cast<const int *>(&tile[q][rr][wd * 4]);
+                    int *dst = reinterpret_cast<int *>(out + q * slice_stride + (long long)(r0 + rr) * Kp + k0 + wd * 4);
+                    *dst = *src;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // PTX helpers
 // ---------------------------------------------------------------------------
@@ -141,7 +202,7 @@ struct SplitArgs {
 // One CTA per 128 x NT output tile; warp 0 lane 0 issues TMA, warp 1 lane 0
 // issues MMAs, all four warps read TMEM in the epilogue.
 template <int S, int NT, int STAGES>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     split_gett_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, SplitArgs p) {
     constexpr int A_BYTES = TM * BKB;           // one slice tile of A
     constexpr int B_BYTES = NT * BKB;
@@ -315,7 +376,7 @@ void launch_split(const CUtensorMap &ta, const CUtensorMap &tb, const SplitArgs 
     split_gett_kernel<S, NT, STAGES><<<grid, 128, smem, s>>>(ta, tb, a);
 }
 
-int tile_n(int S) { return S <= 4 ? 128 : 64; }
+int tile_n(int S) { return S <= 2 ? 128 : 64; }
 
 template <int S, int NT, int STAGES>
 void set_smem_attr() {
@@ -343,9 +404,9 @@ void split_reserve(SplitWorkspace &w, SplitSizes sz, int nslices) {
         throw std::runtime_error("split workspace allocation failed");
     }
     cudaMemset(w.err, 0, sizeof(int));
-    set_smem_attr<2, 128, 4>();
-    set_smem_attr<3, 128, 4>();
-    set_smem_attr<4, 128, 3>();
+    set_smem_attr<2, 128, 3>();
+    set_smem_attr<3, 64, 2>();
+    set_smem_attr<4, 64, 2>();
     w.cap_a = ca;
     w.cap_b = cb;
     w.cap_mn = sz.mn;
@@ -364,7 +425,7 @@ void split_free(SplitWorkspace &w) {
 bool split_eligible(const GettArgs &g) {
     // enough 128 x 128 tiles to fill the GPU and enough K to amortise slicing
     long long tiles = ((g.M + 127LL) / 128) * ((g.N + 127LL) / 128);
-    return g.M >= 64 && g.N >= 64 && g.K >= 64 && tiles >= 64;
+    return g.M >= 64 && g.N >= 64 && g.K >= 256 && tiles >= 64;
 }
 
 int split_launch_count(const GettArgs &, int) { return 3; }
@@ -375,23 +436,32 @@ int split_error(const SplitWorkspace &w) {
     return h;
 }
 
-int split_gett(SplitWorkspace &w, const GettArgs &g, int, int, int S, cudaStream_t s) {
+void slice_operand(const double *base, const int *offr, const int *offk, int R, int K, int Kp, int S, signed char *out,
+                   long long stride, int *expo, bool kmajor, cudaStream_t s) {
+    if (kmajor) {
+        int blocks = (int)std::min<long long>(((long long)R * 32 + 255) / 256, 148 * 16);
+        slice_rows_kernel<<<blocks, 256, 0, s>>>(base, offr, offk, R, K, Kp, S, out, stride, expo);
+    } else {
+        int blocks = (int)std::min<long long>((R + SR - 1) / SR, 148 * 8);
+        slice_rows_tiled_kernel<<<blocks, 256, 0, s>>>(base, offr, offk, R, K, Kp, S, out, stride, expo);
+    }
+}
+
+int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor, int S, cudaStream_t s) {
     if (S < 2 || S > 4) throw std::runtime_error("split GETT supports 2..4 slices");
     long long Kp = ((long long)g.K + BKB - 1) / BKB * BKB;
     long long Mr = g.M, Nr = g.N;
     if (Mr * Kp * S > w.cap_a || Nr * Kp * S > w.cap_b || Mr > w.cap_mn || Nr > w.cap_mn)
         throw std::runtime_error("split workspace too small");
-    int blocks_a = (int)std::min<long long>((Mr * 32 + 255) / 256, 148 * 16);
-    int blocks_b = (int)std::min<long long>((Nr * 32 + 255) / 256, 148 * 16);
-    slice_rows_kernel<<<blocks_a, 256, 0, s>>>(g.A, g.offA_m, g.offA_k, g.M, g.K, (int)Kp, S, w.a, Mr * Kp, w.ea);
-    slice_rows_kernel<<<blocks_b, 256, 0, s>>>(g.B, g.offB_n, g.offB_k, g.N, g.K, (int)Kp, S, w.b, Nr * Kp, w.eb);
+    slice_operand(g.A, g.offA_m, g.offA_k, g.M, g.K, (int)Kp, S, w.a, Mr * Kp, w.ea, a_kmajor != 0, s);
+    slice_operand(g.B, g.offB_n, g.offB_k, g.N, g.K, (int)Kp, S, w.b, Nr * Kp, w.eb, b_kmajor != 0, s);
     CUtensorMap ta = make_map(w.a, Mr, Kp, S, TM);
     CUtensorMap tb = make_map(w.b, Nr, Kp, S, tile_n(S));
     SplitArgs a{g.C, g.offC_m, g.offC_n, w.ea, w.eb, g.M, g.N, g.K, (int)Kp, g.alpha, g.beta, w.err};
     switch (S) {
-        case 2: launch_split<2, 128, 4>(ta, tb, a, s); break;
-        case 3: launch_split<3, 128, 4>(ta, tb, a, s); break;
-        case 4: launch_split<4, 128, 3>(ta, tb, a, s); break;
+        case 2: launch_split<2, 128, 3>(ta, tb, a, s); break;
+        case 3: launch_split<3, 64, 2>(ta, tb, a, s); break;
+        case 4: launch_split<4, 64, 2>(ta, tb, a, s); break;
     }
     return 3;
 }

@@ -384,6 +384,21 @@ class PlanBuilder:
         self.flops += f
         self.ops.append(Gett(c, a, b, float(alpha), beta, tag))
 
+    @staticmethod
+    def _z_order(labels, mem):
+        """Axis order of a Z buffer: the assemble step reads Z once per permutation
+        tau of its member list, so put last the Z labels that most permutations
+        send to the target's last axes (those reads then walk Z contiguously)."""
+        target = list(labels)               # target axis order i0.., a0..
+        rest = list(labels)
+        order = []
+        for pos in reversed(range(len(target))):
+            t = target[pos]
+            best = max(rest, key=lambda l: (sum(1 for tau, _ in mem if tau[l] == t), -rest.index(l)))
+            order.insert(0, best)
+            rest.remove(best)
+        return order
+
     # -- residual of one block -------------------------------------------------
     def emit_block(self, block):
         level = int(block[1])
@@ -421,8 +436,8 @@ class PlanBuilder:
                             direct_order.append(key)
                         direct[key][0] += c * sign
                     continue
-                zaxes = [Axis(l, SIZE[(_sp(l), espin[l])]) for l in ext_o + ext_v]
                 mem_sorted = sorted(mem, key=lambda tc: tuple(tc[0][l] for l in ext_o + ext_v))
+                zaxes = [Axis(l, SIZE[(_sp(l), espin[l])]) for l in self._z_order(ext_o + ext_v, mem_sorted)]
                 c0 = mem_sorted[0][1]
                 norm = (pat, tuple((tuple(tc[0][l] for l in ext_o + ext_v), tc[1] / c0) for tc in mem_sorted))
                 if norm in zshare:
