@@ -157,6 +157,7 @@ int egemm_split_impl(long long k1, long long k2, long long k3, const double *A, 
     g.beta = 0;
     g.c_nfast = 1;
     g.kchunk = (int)k3;
+    g.c_nfast = 1;
     try {
         long long kp = (k3 + 63) / 64 * 64;
         ccqb::split_reserve(g_split, ccqb::SplitSizes{k1 * kp, k2 * kp, std::max(k1, k2)}, S);

@@ -123,7 +123,7 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
     }
 }
 
-template <bool AK, bool BKM>
+template <bool AK, bool BKM, bool GROUPED>
 __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
     constexpr int TILE = BKT * (BM + PADS);
     __shared__ __align__(16) double smem[4 * TILE];
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
     double alpha = g.alpha;
-    if (g.segs) {
+    if (GROUPED) {
         // grouped: sum_s alpha_s A_s B_s^T, rescaling the running sum between terms
         for (int sgi = 0; sgi < g.nseg; ++sgi) {
             const GettSeg sg = g.segs[sgi];
@@ -184,33 +184,56 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
     __syncthreads();
     const bool atomic = gridDim.z > 1;
     const int fast = tid & 63, slow0 = tid >> 6;
-#pragma unroll 4
-    for (int p = 0; p < 32; ++p) {
-        int slow = slow0 + 2 * p;
-        int ml = g.c_nfast ? slow : fast;
-        int nl = g.c_nfast ? fast : slow;
-        int m = m0 + ml, n = n0 + nl;
-        if (m >= g.M || n >= g.N) continue;
-        double *c = g.C + (long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + n);
-        double v = Cs[ml][nl];
-        if (atomic)
-            atomicAdd(c, v);
-        else
-            *c = g.beta ? *c + v : v;
+    // all of this thread's output reads are issued before any write (memory-level
+    // parallelism for the beta = 1 updates of large intermediates)
+#pragma unroll 8
+    for (int p0 = 0; p0 < 32; p0 += 8) {
+        double *cp[8];
+        double cv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            int slow = slow0 + 2 * (p0 + u);
+            int ml = g.c_nfast ? slow : fast;
+            int nl = g.c_nfast ? fast : slow;
+            int m = m0 + ml, n = n0 + nl;
+            bool in = m < g.M && n < g.N;
+            cp[u] = in ? g.C + (long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + n) : nullptr;
+            cv[u] = Cs[ml][nl];
+        }
+        if (atomic) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (cp[u]) atomicAdd(cp[u], cv[u]);
+        } else {
+            double old[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) old[u] = (cp[u] && g.beta) ? *cp[u] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (cp[u]) *cp[u] = old[u] + cv[u];
+        }
     }
+}
+
+template <bool G>
+void launch_gett_v(const GettArgs &a, int a_kmajor, int b_kmajor, dim3 grid, cudaStream_t s) {
+    if (a_kmajor && b_kmajor)
+        gett_f64_kernel<true, true, G><<<grid, 128, 0, s>>>(a);
+    else if (a_kmajor)
+        gett_f64_kernel<true, false, G><<<grid, 128, 0, s>>>(a);
+    else if (b_kmajor)
+        gett_f64_kernel<false, true, G><<<grid, 128, 0, s>>>(a);
+    else
+        gett_f64_kernel<false, false, G><<<grid, 128, 0, s>>>(a);
 }
 
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
     dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, a.segs ? 1 : (a.K + a.kchunk - 1) / a.kchunk);
     if (grid.z == 0) grid.z = 1;
-    if (a_kmajor && b_kmajor)
-        gett_f64_kernel<true, true><<<grid, 128, 0, s>>>(a);
-    else if (a_kmajor)
-        gett_f64_kernel<true, false><<<grid, 128, 0, s>>>(a);
-    else if (b_kmajor)
-        gett_f64_kernel<false, true><<<grid, 128, 0, s>>>(a);
+    if (a.segs)
+        launch_gett_v<true>(a, a_kmajor, b_kmajor, grid, s);
     else
-        gett_f64_kernel<false, false><<<grid, 128, 0, s>>>(a);
+        launch_gett_v<false>(a, a_kmajor, b_kmajor, grid, s);
 }
 
 __global__ void zero_view_kernel(double *C, const int *offm, const int *offn, int M, int N) {

@@ -60,6 +60,56 @@ __global__ void slice_rows_kernel(const double *base, const int *offr, const int
     }
 }
 
+// K-major rows with K <= 512: the row stays in registers (4 consecutive k per
+// lane and 128-wide chunk), one pass over memory, slices stored as packed words.
+__global__ void __launch_bounds__(256) slice_rows_reg_kernel(const double *base, const int *offr, const int *offk,
+                                                             int R, int K, int Kp, int S, signed char *out,
+                                                             long long slice_stride, int *expo) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nch = (Kp + 127) / 128;
+    for (int r = warp; r < R; r += nwarps) {
+        const double *row = base + offr[r];
+        double xv[16];
+        double mx = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                int k = 128 * j + 4 * lane + u;
+                double x = (j < nch && k < K) ? row[offk[k]] : 0.0;
+                xv[4 * j + u] = x;
+                mx = fmax(mx, fabs(x));
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        int e = 0;
+        if (mx > 0.0) frexp(mx, &e);
+        if (lane == 0) expo[r] = e;
+        const double scale = ldexp(1.0, -e);
+        signed char *dst = out + (long long)r * Kp;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int k0 = 128 * j + 4 * lane;
+            if (j >= nch || k0 >= Kp) continue;
+            double t[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) t[u] = xv[4 * j + u] * scale * 64.0;
+            for (int q = 0; q < S; ++q) {
+                unsigned word = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    double sv = rint(t[u]);
+                    word |= ((unsigned)(int)sv & 0xFFu) << (8 * u);
+                    t[u] = (t[u] - sv) * 128.0;
+                }
+                *reinterpret_cast<unsigned *>(dst + q * slice_stride + k0) = word;
+            }
+        }
+    }
+}
+
 // Rows contiguous in memory (consecutive r -> consecutive addresses): a CTA
 // takes 32 rows, reads them 32 at a time (coalesced), reduces the row maxima in
 // shared memory, then slices 64-wide K chunks through a shared-memory tile so
@@ -196,6 +246,7 @@ struct SplitArgs {
     int M, N, K, Kp;
     double alpha;
     int beta;
+    int c_nfast;
     int *err;
 };
 
@@ -299,33 +350,64 @@ __global__ void __launch_bounds__(128, 2)
     if (!good || abort_flag) {
         if (threadIdx.x == 0) atomicExch(p.err, 1);
     } else {
+        // Stage 64 output columns at a time in shared memory (the pipeline buffers
+        // are free once every MMA has completed), then write them out along C's
+        // contiguous mode with all reads of a batch in flight before its writes.
+        constexpr int CW = 64;
+        double (*Cs)[CW + 1] = reinterpret_cast<double (*)[CW + 1]>(smem);
+        int *eas = reinterpret_cast<int *>(smem + TM * (CW + 1) * sizeof(double));
+        int *ebs = eas + TM;
         const int row = warp * 32 + lane;
-        const int m = m0 + row;
-        const long long om = m < p.M ? (long long)p.offC_m[m] : 0;
-        const int em = m < p.M ? p.ea[m] : 0;
+        for (int t = threadIdx.x; t < TM; t += blockDim.x) eas[t] = (m0 + t < p.M) ? p.ea[m0 + t] : 0;
+        for (int t = threadIdx.x; t < NT; t += blockDim.x) ebs[t] = (n0 + t < p.N) ? p.eb[n0 + t] : 0;
 #pragma unroll 1
-        for (int c0 = 0; c0 < NT; c0 += 32) {
-            double val[32];
+        for (int cb = 0; cb < NT; cb += CW) {
 #pragma unroll
-            for (int q = 0; q < 32; ++q) val[q] = 0.0;
-#pragma unroll 1
-            for (int lev = NLEV - 1; lev >= 0; --lev) {
-                int v[32];
-                tmem_ld32<NT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(lev * NT + c0), v);
-                double w = ldexp(1.0, -7 * lev);
+            for (int c0 = 0; c0 < CW; c0 += 32) {
+                double val[32];
 #pragma unroll
-                for (int q = 0; q < 32; ++q) val[q] += (double)v[q] * w;
-            }
-            if (m < p.M) {
-#pragma unroll 4
-                for (int q = 0; q < 32; ++q) {
-                    int n = n0 + c0 + q;
-                    if (n >= p.N) break;
-                    double x = p.alpha * ldexp(val[q], em + p.eb[n] - 12);
-                    double *c = p.C + om + p.offC_n[n];
-                    *c = p.beta ? *c + x : x;
+                for (int q = 0; q < 32; ++q) val[q] = 0.0;
+#pragma unroll
+                for (int lev = NLEV - 1; lev >= 0; --lev) {
+                    int v[32];
+                    tmem_ld32<NT>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(lev * NT + cb + c0), v);
+                    const double w = ldexp(1.0, -7 * lev);
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) val[q] += (double)v[q] * w;
                 }
+#pragma unroll
+                for (int q = 0; q < 32; ++q) Cs[row][c0 + q] = val[q];
             }
+            __syncthreads();
+            const int tid = threadIdx.x;
+#pragma unroll 1
+            for (int p0 = 0; p0 < TM * CW / 128; p0 += 8) {
+                double *cp[8];
+                double cv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    int idx = (p0 + u) * 128 + tid;
+                    int ml, nl;
+                    if (p.c_nfast) {
+                        nl = idx % CW;
+                        ml = idx / CW;
+                    } else {
+                        ml = idx % TM;
+                        nl = idx / TM;
+                    }
+                    int m = m0 + ml, n = n0 + cb + nl;
+                    bool in = m < p.M && n < p.N;
+                    cp[u] = in ? p.C + (long long)p.offC_m[m] + p.offC_n[n] : nullptr;
+                    cv[u] = p.alpha * ldexp(Cs[ml][nl], eas[ml] + ebs[cb + nl] - 12);
+                }
+                double old[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) old[u] = (cp[u] && p.beta) ? *cp[u] : 0.0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (cp[u]) *cp[u] = old[u] + cv[u];
+            }
+            __syncthreads();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n");
@@ -438,7 +520,10 @@ int split_error(const SplitWorkspace &w) {
 
 void slice_operand(const double *base, const int *offr, const int *offk, int R, int K, int Kp, int S, signed char *out,
                    long long stride, int *expo, bool kmajor, cudaStream_t s) {
-    if (kmajor) {
+    if (kmajor && Kp <= 512) {
+        int blocks = (int)std::min<long long>(((long long)R * 32 + 255) / 256, 148 * 32);
+        slice_rows_reg_kernel<<<blocks, 256, 0, s>>>(base, offr, offk, R, K, Kp, S, out, stride, expo);
+    } else if (kmajor) {
         int blocks = (int)std::min<long long>(((long long)R * 32 + 255) / 256, 148 * 16);
         slice_rows_kernel<<<blocks, 256, 0, s>>>(base, offr, offk, R, K, Kp, S, out, stride, expo);
     } else {
@@ -457,7 +542,7 @@ int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor,
     slice_operand(g.B, g.offB_n, g.offB_k, g.N, g.K, (int)Kp, S, w.b, Nr * Kp, w.eb, b_kmajor != 0, s);
     CUtensorMap ta = make_map(w.a, Mr, Kp, S, TM);
     CUtensorMap tb = make_map(w.b, Nr, Kp, S, tile_n(S));
-    SplitArgs a{g.C, g.offC_m, g.offC_n, w.ea, w.eb, g.M, g.N, g.K, (int)Kp, g.alpha, g.beta, w.err};
+    SplitArgs a{g.C, g.offC_m, g.offC_n, w.ea, w.eb, g.M, g.N, g.K, (int)Kp, g.alpha, g.beta, g.c_nfast, w.err};
     switch (S) {
         case 2: launch_split<2, 128, 3>(ta, tb, a, s); break;
         case 3: launch_split<3, 64, 2>(ta, tb, a, s); break;

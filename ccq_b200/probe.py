@@ -28,6 +28,17 @@ def main(argv):
         err = float(np.abs(C[:64, :64] - ref).max())
         print(f'egemm {k1}x{k2}x{k3}: wall {dt * 1e3:.2f} ms (incl. copies), max err {err:.2e}')
         assert err < 1e-9
+    elif kind == 'egemm_split':
+        k1, k2, k3 = (int(x) for x in argv[1:4])
+        S = int(argv[4]) if len(argv) > 4 else 4
+        rng = np.random.default_rng(0)
+        A = np.asfortranarray(rng.normal(size=(k3, k1)))
+        B = np.asfortranarray(rng.normal(size=(k3, k2)))
+        C = lib.egemm_split(k1, k2, k3, A, B, S)
+        ref = B[:, :64].T @ A[:, :64]
+        err = float(np.abs(C[:64, :64] - ref).max())
+        print(f'egemm_split {k1}x{k2}x{k3} S={S}: max err {err:.2e}')
+        assert err < 1e-5
     elif kind == 'sweep':
         # per-operation device times of one CCSDT sweep on the 40-orbital workload
         import os
