@@ -357,9 +357,19 @@ __global__ void __launch_bounds__(128, 2)
         double (*Cs)[CW + 1] = reinterpret_cast<double (*)[CW + 1]>(smem);
         int *eas = reinterpret_cast<int *>(smem + TM * (CW + 1) * sizeof(double));
         int *ebs = eas + TM;
+        long long *oms = reinterpret_cast<long long *>(ebs + NT);   // output row offsets (-1: outside)
+        long long *ons = oms + TM;                                   // output column offsets
         const int row = warp * 32 + lane;
-        for (int t = threadIdx.x; t < TM; t += blockDim.x) eas[t] = (m0 + t < p.M) ? p.ea[m0 + t] : 0;
-        for (int t = threadIdx.x; t < NT; t += blockDim.x) ebs[t] = (n0 + t < p.N) ? p.eb[n0 + t] : 0;
+        for (int t = threadIdx.x; t < TM; t += blockDim.x) {
+            bool in = m0 + t < p.M;
+            eas[t] = in ? p.ea[m0 + t] : 0;
+            oms[t] = in ? (long long)p.offC_m[m0 + t] : -1;
+        }
+        for (int t = threadIdx.x; t < NT; t += blockDim.x) {
+            bool in = n0 + t < p.N;
+            ebs[t] = in ? p.eb[n0 + t] : 0;
+            ons[t] = in ? (long long)p.offC_n[n0 + t] : -1;
+        }
 #pragma unroll 1
         for (int cb = 0; cb < NT; cb += CW) {
 #pragma unroll
@@ -381,11 +391,11 @@ __global__ void __launch_bounds__(128, 2)
             __syncthreads();
             const int tid = threadIdx.x;
 #pragma unroll 1
-            for (int p0 = 0; p0 < TM * CW / 128; p0 += 8) {
-                double *cp[8];
-                double cv[8];
+            for (int p0 = 0; p0 < TM * CW / 128; p0 += 16) {
+                double *cp[16];
+                double cv[16];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
+                for (int u = 0; u < 16; ++u) {
                     int idx = (p0 + u) * 128 + tid;
                     int ml, nl;
                     if (p.c_nfast) {
@@ -395,16 +405,15 @@ __global__ void __launch_bounds__(128, 2)
                         ml = idx % TM;
                         nl = idx / TM;
                     }
-                    int m = m0 + ml, n = n0 + cb + nl;
-                    bool in = m < p.M && n < p.N;
-                    cp[u] = in ? p.C + (long long)p.offC_m[m] + p.offC_n[n] : nullptr;
+                    long long om = oms[ml], on = ons[cb + nl];
+                    cp[u] = (om >= 0 && on >= 0) ? p.C + om + on : nullptr;
                     cv[u] = p.alpha * ldexp(Cs[ml][nl], eas[ml] + ebs[cb + nl] - 12);
                 }
-                double old[8];
+                double old[16];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) old[u] = (cp[u] && p.beta) ? *cp[u] : 0.0;
+                for (int u = 0; u < 16; ++u) old[u] = (cp[u] && p.beta) ? *cp[u] : 0.0;
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
+                for (int u = 0; u < 16; ++u)
                     if (cp[u]) *cp[u] = old[u] + cv[u];
             }
             __syncthreads();
