@@ -357,7 +357,7 @@ def main():
     if not args.no_converge:
         from ccq_b200 import config, driver
         c2 = new_ctx()
-        cfg = config.Config(calc_type='CCSDT', tol=1e-8, diis_space=5, max_iter=100,
+        cfg = config.Config(calc_type='CCSDT', tol=1e-10, diis_space=5, max_iter=100,
                             gpu_precision=headline, gpu_slices=args.slices).calc_macros()
         r = driver.solve_cc(c2, cfg, out=lambda x: None)
         c2.close()

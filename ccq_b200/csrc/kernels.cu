@@ -256,59 +256,158 @@ void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N,
 // ---------------------------------------------------------------------------
 // assemble: residual gather + Jacobi + antisymmetric fill
 // ---------------------------------------------------------------------------
-__global__ void assemble_kernel(AsmArgs a) {
-    for (long long lin = blockIdx.x * (long long)blockDim.x + threadIdx.x; lin < a.total;
-         lin += (long long)gridDim.x * blockDim.x) {
-        int x[MAXR];
-        long long r = lin;
-        for (int q = a.nruns - 1; q >= 0; --q) {
-            int c = (int)(r % a.run_count[q]);
-            r /= a.run_count[q];
-            const unsigned char *tup = a.combos + a.run_off[q] + c * a.run_len[q];
-            for (int l = 0; l < a.run_len[q]; ++l) x[a.run_axis0[q] + l] = tup[l];
+// Term descriptor as staged in shared memory: pm has bit j*RK+k set when Z
+// axes j < k belong to one antisymmetric group (sorted-with-sign reads);
+// tst are the strides per target axis (used when pm == 0), zs per Z axis.
+template <int RK>
+struct SmTerm {
+    const double *p;
+    double coef;
+    unsigned long long pm;
+    int zs[RK];
+    int tst[RK];
+    unsigned char src[RK];
+};
+
+template <int RK>
+__device__ __forceinline__ int pick(const int (&v)[RK], int i) {
+    int r = 0;
+#pragma unroll
+    for (int e = 0; e < RK; ++e)
+        if (e == i) r = v[e];
+    return r;
+}
+
+template <int RK>
+__global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
+    constexpr int CH = 128;
+    __shared__ SmTerm<RK> st[CH];
+    const int nch = (a.nterms + CH - 1) / CH;
+    for (long long base = blockIdx.x * (long long)blockDim.x; base < a.total;
+         base += (long long)gridDim.x * blockDim.x) {
+        const long long lin = base + threadIdx.x;
+        const bool act = lin < a.total;
+        int x[RK];
+#pragma unroll
+        for (int d = 0; d < RK; ++d) x[d] = 0;
+        if (act) {
+            // canonical element from its per-run combination indices
+            int cq[RK];
+            long long r = lin;
+#pragma unroll
+            for (int q = RK - 1; q >= 0; --q) {
+                cq[q] = 0;
+                if (q < a.nruns) {
+                    cq[q] = (int)(r % a.run_count[q]);
+                    r /= a.run_count[q];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < RK; ++q) {
+                if (q < a.nruns) {
+                    const unsigned char *tup = a.combos + a.run_off[q] + cq[q] * a.run_len[q];
+#pragma unroll
+                    for (int d = 0; d < RK; ++d) {
+                        int l = d - a.run_axis0[q];
+                        if (l >= 0 && l < a.run_len[q]) x[d] = tup[l];
+                    }
+                }
+            }
         }
         double R = 0.0;
-        for (int t = 0; t < a.nterms; ++t) {
-            const AsmTerm &tm = a.terms[t];
-            int y[MAXR];
-            for (int j = 0; j < tm.rank; ++j) y[j] = x[tm.src[j]];
-            double sg = 1.0;
-            bool zero = false;
-            for (int g = 0; g < tm.ng; ++g) {
-                const signed char *gp = tm.gpos[g];
-                int L = tm.glen[g];
-                // insertion sort of the group's indices, one sign flip per swap
-                for (int i = 1; i < L; ++i)
-                    for (int j = i; j > 0 && y[gp[j - 1]] > y[gp[j]]; --j) {
-                        int tmp = y[gp[j]];
-                        y[gp[j]] = y[gp[j - 1]];
-                        y[gp[j - 1]] = tmp;
-                        sg = -sg;
-                    }
-                for (int i = 1; i < L; ++i)
-                    if (y[gp[i]] == y[gp[i - 1]]) zero = true;
+        for (int c = 0; c < nch; ++c) {
+            __syncthreads();
+            const int nt = min(CH, a.nterms - c * CH);
+            for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+                const AsmTerm &g = a.terms[c * CH + t];
+                SmTerm<RK> q;
+                q.p = g.p;
+                q.coef = g.coef;
+                unsigned long long pm = 0;
+                for (int gi = 0; gi < g.ng; ++gi)
+                    for (int u = 0; u < g.glen[gi]; ++u)
+                        for (int v = u + 1; v < g.glen[gi]; ++v) {
+                            int j = g.gpos[gi][u], k = g.gpos[gi][v];
+                            if (j > k) {
+                                int tmp = j;
+                                j = k;
+                                k = tmp;
+                            }
+                            pm |= 1ull << (j * RK + k);
+                        }
+                q.pm = pm;
+#pragma unroll
+                for (int d = 0; d < RK; ++d) {
+                    q.zs[d] = g.zstride[d];
+                    q.src[d] = (unsigned char)g.src[d];
+                    q.tst[d] = 0;
+                }
+#pragma unroll
+                for (int j = 0; j < RK; ++j) q.tst[g.src[j]] += g.zstride[j];
+                st[t] = q;
             }
-            if (zero) continue;
-            long long off = 0;
-            for (int j = 0; j < tm.rank; ++j) off += (long long)tm.zstride[j] * y[j];
-            R += sg * tm.coef * tm.p[off];
+            __syncthreads();
+            if (act) {
+#pragma unroll 4
+                for (int t = 0; t < nt; ++t) {
+                    const SmTerm<RK> &q = st[t];
+                    long long off = 0;
+                    double sg = q.coef;
+                    if (q.pm == 0) {
+#pragma unroll
+                        for (int d = 0; d < RK; ++d) off += (long long)q.tst[d] * x[d];
+                    } else {
+                        int y[RK];
+#pragma unroll
+                        for (int j = 0; j < RK; ++j) y[j] = pick<RK>(x, q.src[j]);
+                        bool zero = false;
+                        // selection sort within groups: one sign flip per exchange
+#pragma unroll
+                        for (int j = 0; j < RK; ++j)
+#pragma unroll
+                            for (int k = j + 1; k < RK; ++k)
+                                if ((q.pm >> (j * RK + k)) & 1ull) {
+                                    if (y[j] > y[k]) {
+                                        int tmp = y[j];
+                                        y[j] = y[k];
+                                        y[k] = tmp;
+                                        sg = -sg;
+                                    } else if (y[j] == y[k]) {
+                                        zero = true;
+                                    }
+                                }
+                        if (zero) continue;
+#pragma unroll
+                        for (int j = 0; j < RK; ++j) off += (long long)q.zs[j] * y[j];
+                    }
+                    R += sg * __ldg(q.p + off);
+                }
+            }
         }
+        if (!act) continue;
         long long toff = 0;
-        for (int d = 0; d < a.rank; ++d) toff += (long long)a.tstride[d] * x[d];
+#pragma unroll
+        for (int d = 0; d < RK; ++d) toff += (long long)a.tstride[d] * x[d];
         double tnew;
         if (a.mode == 0) {
             double D = a.shift;
-            for (int d = 0; d < a.level; ++d) D -= a.fdiag[a.spin[d]][x[d]];
-            for (int d = a.level; d < a.rank; ++d) D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[d]];
+#pragma unroll
+            for (int d = 0; d < RK; ++d) {
+                if (d < RK / 2)
+                    D -= a.fdiag[a.spin[d]][x[d]];
+                else
+                    D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[d]];
+            }
             tnew = a.T[toff] - R / D;
         } else {
             tnew = R;
         }
-        for (int p = 0; p < a.nperm; ++p) {
-            const signed char *P = a.perm + p * a.rank;
+        for (int pidx = 0; pidx < a.nperm; ++pidx) {
+            const signed char *P = a.perm + pidx * RK;
             long long o = 0;
-            for (int d = 0; d < a.rank; ++d) o += (long long)a.tstride[d] * x[P[d]];
-            a.T[o] = a.psign[p] * tnew;
+#pragma unroll
+            for (int d = 0; d < RK; ++d) o += (long long)a.tstride[d] * pick<RK>(x, P[d]);
+            a.T[o] = a.psign[pidx] * tnew;
         }
     }
 }
@@ -317,7 +416,13 @@ void launch_assemble(const AsmArgs &a, cudaStream_t s) {
     long long blocks = (a.total + 255) / 256;
     if (blocks > 148 * 32) blocks = 148 * 32;
     if (blocks < 1) blocks = 1;
-    assemble_kernel<<<(int)blocks, 256, 0, s>>>(a);
+    switch (a.rank) {
+        case 2: assemble_kernel<2><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 4: assemble_kernel<4><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 6: assemble_kernel<6><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 8: assemble_kernel<8><<<(int)blocks, 256, 0, s>>>(a); break;
+        default: break;
+    }
 }
 
 __global__ void fill_kernel(double *p, double v, long long n) {
