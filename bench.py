@@ -70,13 +70,20 @@ def barrier(world):
 
 
 def allmax(x, world):
+    """Max of a per-rank device time over all ranks (the whole job waits for the slowest replica)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dev = 'cuda' if dist.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_seconds_per_iter(ms_total_rank, world, steps):
+    """Whole-job s/iter of independent replicas: slowest rank's time over all iterations of all ranks."""
+    return allmax(ms_total_rank, world) / 1e3 / (world * steps)
 
 
 class Clocks:
@@ -309,7 +316,7 @@ def main():
         it += args.steps
         st = ctx.stats()
         tot = allmax(sum(ms), world)
-        results[leg] = {'s_per_iter': tot / 1e3 / (world * args.steps), 'ms_total': tot,
+        results[leg] = {'s_per_iter': job_seconds_per_iter(sum(ms), world, args.steps), 'ms_total': tot,
                         'tflops': st['flops'] * world * args.steps / (tot * 1e-3) / 1e12,
                         'launches_per_iter': st['launches'], 'flops_per_iter': st['flops']}
     head = results[headline]
