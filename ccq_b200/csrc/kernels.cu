@@ -13,6 +13,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pre
     int sz = pred ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
 }
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    int sz = pred ? 16 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -29,7 +34,7 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1
 // else they walk m.  Rows beyond M or columns beyond kend are zero-filled.
 template <bool KMAJOR>
 __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *base, const int *offm_reg,
-                                          const int *offk, int m0, int M, int k0, int kend, int tid) {
+                                          const int *offk, int m0, int M, int k0, int kend, int tid, bool vec) {
     if (KMAJOR) {
         int kk = tid & 15;
         int mrow = tid >> 4;
@@ -42,6 +47,19 @@ __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *
             bool in = kin && (m0 + m < M);
             const double *src = in ? base + (long long)offm_reg[p] + ok : base;
             cp_async8(&S[kk][m], src, in);
+        }
+    } else if (vec) {
+        // pairs (m, m+1) are contiguous and 16-byte aligned: half the copies
+        int m = 2 * (tid & 31);
+        int krow = tid >> 5;
+        bool min_ = (m0 + m) < M;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            int kk = krow + 4 * p;
+            int k = k0 + kk;
+            bool in = min_ && k < kend;
+            const double *src = in ? base + (long long)offm_reg[0] + __ldg(offk + k) : base;
+            cp_async16(&S[kk][m], src, in);
         }
     } else {
         int m = tid & 63;
@@ -64,7 +82,7 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
                                               double (*Bs)[BKT][BN + PADS], const double *A, const double *B,
                                               const int *offA_m, const int *offA_k, const int *offB_n,
                                               const int *offB_k, int M, int N, int m0, int n0, int kbeg, int kend,
-                                              int tid, int wm, int wn, int gid, int tig) {
+                                              int tid, int wm, int wn, int gid, int tig, bool va, bool vb) {
     int offa[8], offb[8];
     if (AK) {
 #pragma unroll
@@ -73,7 +91,7 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
             offa[p] = m < M ? __ldg(offA_m + m) : 0;
         }
     } else {
-        int m = m0 + (tid & 63);
+        int m = m0 + (va ? 2 * (tid & 31) : (tid & 63));
         offa[0] = m < M ? __ldg(offA_m + m) : 0;
     }
     if (BKM) {
@@ -83,21 +101,21 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
             offb[p] = n < N ? __ldg(offB_n + n) : 0;
         }
     } else {
-        int n = n0 + (tid & 63);
+        int n = n0 + (vb ? 2 * (tid & 31) : (tid & 63));
         offb[0] = n < N ? __ldg(offB_n + n) : 0;
     }
     const int ntiles = kend > kbeg ? (kend - kbeg + BKT - 1) / BKT : 0;
     if (ntiles > 0) {
-        load_tile<AK>(As[0], A, offa, offA_k, m0, M, kbeg, kend, tid);
-        load_tile<BKM>(Bs[0], B, offb, offB_k, n0, N, kbeg, kend, tid);
+        load_tile<AK>(As[0], A, offa, offA_k, m0, M, kbeg, kend, tid, va);
+        load_tile<BKM>(Bs[0], B, offb, offB_k, n0, N, kbeg, kend, tid, vb);
         cp_async_commit();
     }
     for (int t = 0; t < ntiles; ++t) {
         const int st = t & 1;
         if (t + 1 < ntiles) {
             int k0 = kbeg + (t + 1) * BKT;
-            load_tile<AK>(As[st ^ 1], A, offa, offA_k, m0, M, k0, kend, tid);
-            load_tile<BKM>(Bs[st ^ 1], B, offb, offB_k, n0, N, k0, kend, tid);
+            load_tile<AK>(As[st ^ 1], A, offa, offA_k, m0, M, k0, kend, tid, va);
+            load_tile<BKM>(Bs[st ^ 1], B, offb, offB_k, n0, N, k0, kend, tid, vb);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
@@ -158,14 +176,14 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
                         for (int q = 0; q < 4; ++q) acc[i][j][q] *= r;
             }
             gett_mainloop<AK, BKM>(acc, As, Bs, sg.A, sg.B, sg.offA_m, sg.offA_k, sg.offB_n, sg.offB_k, g.M, g.N, m0,
-                                   n0, 0, sg.K, tid, wm, wn, gid, tig);
+                                   n0, 0, sg.K, tid, wm, wn, gid, tig, g.vec_a != 0, g.vec_b != 0);
             alpha = sg.alpha;
         }
     } else {
         const int kbeg = blockIdx.z * g.kchunk;
         const int kend = min(g.K, kbeg + g.kchunk);
         gett_mainloop<AK, BKM>(acc, As, Bs, g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k, g.M, g.N, m0, n0, kbeg,
-                               kend, tid, wm, wn, gid, tig);
+                               kend, tid, wm, wn, gid, tig, g.vec_a != 0, g.vec_b != 0);
     }
 
     // epilogue: stage the tile in shared memory, then write along the output's
@@ -183,6 +201,33 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
                     Cs[wm + mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = alpha * acc[mi][ni][2 * h + j];
     __syncthreads();
     const bool atomic = gridDim.z > 1;
+    if (g.vec_c && !atomic) {
+        // output pairs along the fast mode are contiguous and 16-byte aligned
+        const int fast = 2 * (tid & 31), slow0 = tid >> 5;
+#pragma unroll 4
+        for (int p0 = 0; p0 < 16; p0 += 4) {
+            double2 *cp[4];
+            double2 cv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                int slow = slow0 + 4 * (p0 + u);
+                int ml = g.c_nfast ? slow : fast;
+                int nl = g.c_nfast ? fast : slow;
+                int m = m0 + ml, n = n0 + nl;
+                bool in = m < g.M && n < g.N;
+                cp[u] = in ? reinterpret_cast<double2 *>(g.C + (long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + n))
+                           : nullptr;
+                cv[u] = g.c_nfast ? make_double2(Cs[ml][nl], Cs[ml][nl + 1]) : make_double2(Cs[ml][nl], Cs[ml + 1][nl]);
+            }
+            double2 old[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) old[u] = (cp[u] && g.beta) ? *cp[u] : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (cp[u]) *cp[u] = make_double2(old[u].x + cv[u].x, old[u].y + cv[u].y);
+        }
+        return;
+    }
     const int fast = tid & 63, slow0 = tid >> 6;
     // all of this thread's output reads are issued before any write (memory-level
     // parallelism for the beta = 1 updates of large intermediates)

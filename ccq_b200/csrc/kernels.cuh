@@ -39,6 +39,10 @@ struct GettArgs {
     int beta;       // 0: overwrite, 1: accumulate
     int kchunk;     // K range handled by one blockIdx.z (split-K, atomic epilogue)
     int c_nfast;    // 1: output contiguous along n (write-out walks n), 0: along m
+    // 16-byte paths, set by the host only where the tables pair up contiguous,
+    // 16-byte aligned elements: vec_a / vec_b for m- (n-) major operand loads,
+    // vec_c for the output write-out along its fast mode
+    int vec_a, vec_b, vec_c;
     const GettSeg *segs;  // grouped launch: nseg terms (A, B, tables, K, alpha above unused)
     int nseg;
 };

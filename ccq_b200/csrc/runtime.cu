@@ -589,6 +589,21 @@ void instantiate(ccq_b200_ctx *c) {
             o.g.A = A.base;
             o.g.B = B.base;
             o.g.C = C.base;
+            {
+                // 16-byte paths: the walked table pairs up contiguous elements, every
+                // element the pair starts at is even (16-byte aligned with the base)
+                auto paired = [](const std::vector<int> &w, const std::vector<int> &other, const double *base) {
+                    if (w.size() < 2 || w.size() % 2 || (reinterpret_cast<uintptr_t>(base) & 15)) return 0;
+                    for (size_t i = 0; i < w.size(); i += 2)
+                        if (w[i + 1] != w[i] + 1 || (w[i] & 1)) return 0;
+                    for (int x : other)
+                        if (x & 1) return 0;
+                    return 1;
+                };
+                o.g.vec_a = !o.akm ? paired(am, ak, A.base) : 0;
+                o.g.vec_b = !o.bkm ? paired(bn, bk, B.base) : 0;
+                o.g.vec_c = o.g.c_nfast ? paired(cn, cm, C.base) : paired(cm, cn, C.base);
+            }
             o.g.M = (int)M;
             o.g.N = (int)N;
             o.g.K = (int)K;
@@ -799,6 +814,11 @@ void instantiate(ccq_b200_ctx *c) {
                             if (q + 1 < j) m.skip = true;
                         }
                         Op &lead = c->plan.ops[lst[j - 1]];
+                        for (size_t q = k; q < j; ++q) {
+                            const Op &m = c->plan.ops[lst[q]];
+                            lead.g.vec_a = lead.g.vec_a && m.g.vec_a && m.akm == lead.akm;
+                            lead.g.vec_b = lead.g.vec_b && m.g.vec_b && m.bkm == lead.bkm;
+                        }
                         lead.g.beta = f.beta;
                         lead.g.nseg = (int)(j - k);
                         lead.group_flops = fl;
