@@ -7,6 +7,16 @@ namespace ccqb {
 // GETT, FP64 on the DMMA tensor pipe
 // ---------------------------------------------------------------------------
 constexpr int BM = 64, BN = 64, BKT = 16, PADS = 4;
+// Shared-memory operand tiles: m-major operands are stored [k][m] (row stride MS),
+// k-major ones [m][k] (row stride KS), so that each can be filled with 16-byte
+// copies along its contiguous mode; both strides keep the fragment reads of a
+// half-warp on 16 distinct banks.
+constexpr int MS = BM + PADS;   // 68
+constexpr int KS = BKT + 4;     // 20
+constexpr int TILE = BM * KS;   // doubles per tile buffer (>= BKT * MS)
+static_assert(BKT * MS <= TILE, "tile buffer");
+template <bool KMAJ>
+__device__ __forceinline__ int tix(int k, int m) { return KMAJ ? m * KS + k : k * MS + m; }
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -29,13 +39,27 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1
         : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// Loads one BKT x BM tile of a GETT operand into shared memory [k][m].
+// Loads one BKT x BM tile of a GETT operand into shared memory (layout tix).
 // kmajor: consecutive threads walk k (operand stride-1 along its k modes),
-// else they walk m.  Rows beyond M or columns beyond kend are zero-filled.
+// else they walk m.  vec: the walked mode pairs up contiguous, 16-byte aligned
+// elements, copied 16 bytes at a time.  Out-of-range elements are zero-filled.
 template <bool KMAJOR>
-__device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *base, const int *offm_reg,
-                                          const int *offk, int m0, int M, int k0, int kend, int tid, bool vec) {
-    if (KMAJOR) {
+__device__ __forceinline__ void load_tile(double *S, const double *base, const int *offm_reg, const int *offk, int m0,
+                                          int M, int k0, int kend, int tid, bool vec) {
+    if (KMAJOR && vec) {
+        int kk = 2 * (tid & 7);
+        int mrow = tid >> 3;
+        int k = k0 + kk;
+        bool kin = k < kend;
+        int ok = kin ? __ldg(offk + k) : 0;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            int m = mrow + 16 * p;
+            bool in = kin && (m0 + m < M);
+            const double *src = in ? base + (long long)offm_reg[p] + ok : base;
+            cp_async16(&S[tix<true>(kk, m)], src, in);
+        }
+    } else if (KMAJOR) {
         int kk = tid & 15;
         int mrow = tid >> 4;
         int k = k0 + kk;
@@ -46,7 +70,7 @@ __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *
             int m = mrow + 8 * p;
             bool in = kin && (m0 + m < M);
             const double *src = in ? base + (long long)offm_reg[p] + ok : base;
-            cp_async8(&S[kk][m], src, in);
+            cp_async8(&S[tix<true>(kk, m)], src, in);
         }
     } else if (vec) {
         // pairs (m, m+1) are contiguous and 16-byte aligned: half the copies
@@ -59,7 +83,7 @@ __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *
             int k = k0 + kk;
             bool in = min_ && k < kend;
             const double *src = in ? base + (long long)offm_reg[0] + __ldg(offk + k) : base;
-            cp_async16(&S[kk][m], src, in);
+            cp_async16(&S[tix<false>(kk, m)], src, in);
         }
     } else {
         int m = tid & 63;
@@ -71,15 +95,15 @@ __device__ __forceinline__ void load_tile(double (*S)[BM + PADS], const double *
             int k = k0 + kk;
             bool in = min_ && k < kend;
             const double *src = in ? base + (long long)offm_reg[0] + __ldg(offk + k) : base;
-            cp_async8(&S[kk][m], src, in);
+            cp_async8(&S[tix<false>(kk, m)], src, in);
         }
     }
 }
 
 // K loop of one contraction term over [kbeg, kend): 2-stage cp.async pipeline.
 template <bool AK, bool BKM>
-__device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*As)[BKT][BM + PADS],
-                                              double (*Bs)[BKT][BN + PADS], const double *A, const double *B,
+__device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As, double *Bs, const double *A,
+                                              const double *B,
                                               const int *offA_m, const int *offA_k, const int *offB_n,
                                               const int *offB_k, int M, int N, int m0, int n0, int kbeg, int kend,
                                               int tid, int wm, int wn, int gid, int tig, bool va, bool vb) {
@@ -87,8 +111,8 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
     if (AK) {
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
-            int m = m0 + (tid >> 4) + 8 * p;
-            offa[p] = m < M ? __ldg(offA_m + m) : 0;
+            int m = m0 + (va ? (tid >> 3) + 16 * p : (tid >> 4) + 8 * p);
+            offa[p] = (m < M && (!va || p < 4)) ? __ldg(offA_m + m) : 0;
         }
     } else {
         int m = m0 + (va ? 2 * (tid & 31) : (tid & 63));
@@ -97,8 +121,8 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
     if (BKM) {
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
-            int n = n0 + (tid >> 4) + 8 * p;
-            offb[p] = n < N ? __ldg(offB_n + n) : 0;
+            int n = n0 + (vb ? (tid >> 3) + 16 * p : (tid >> 4) + 8 * p);
+            offb[p] = (n < N && (!vb || p < 4)) ? __ldg(offB_n + n) : 0;
         }
     } else {
         int n = n0 + (vb ? 2 * (tid & 31) : (tid & 63));
@@ -106,16 +130,16 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
     }
     const int ntiles = kend > kbeg ? (kend - kbeg + BKT - 1) / BKT : 0;
     if (ntiles > 0) {
-        load_tile<AK>(As[0], A, offa, offA_k, m0, M, kbeg, kend, tid, va);
-        load_tile<BKM>(Bs[0], B, offb, offB_k, n0, N, kbeg, kend, tid, vb);
+        load_tile<AK>(As, A, offa, offA_k, m0, M, kbeg, kend, tid, va);
+        load_tile<BKM>(Bs, B, offb, offB_k, n0, N, kbeg, kend, tid, vb);
         cp_async_commit();
     }
     for (int t = 0; t < ntiles; ++t) {
         const int st = t & 1;
         if (t + 1 < ntiles) {
             int k0 = kbeg + (t + 1) * BKT;
-            load_tile<AK>(As[st ^ 1], A, offa, offA_k, m0, M, k0, kend, tid, va);
-            load_tile<BKM>(Bs[st ^ 1], B, offb, offB_k, n0, N, k0, kend, tid, vb);
+            load_tile<AK>(As + (st ^ 1) * TILE, A, offa, offA_k, m0, M, k0, kend, tid, va);
+            load_tile<BKM>(Bs + (st ^ 1) * TILE, B, offb, offB_k, n0, N, k0, kend, tid, vb);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
@@ -127,11 +151,11 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
             double a[2][2], b[4];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi) {
-                a[mi][0] = As[st][kk + tig][wm + mi * 16 + gid];
-                a[mi][1] = As[st][kk + tig][wm + mi * 16 + gid + 8];
+                a[mi][0] = As[st * TILE + tix<AK>(kk + tig, wm + mi * 16 + gid)];
+                a[mi][1] = As[st * TILE + tix<AK>(kk + tig, wm + mi * 16 + gid + 8)];
             }
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[st][kk + tig][wn + ni * 8 + gid];
+            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[st * TILE + tix<BKM>(kk + tig, wn + ni * 8 + gid)];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -143,10 +167,9 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double (*A
 
 template <bool AK, bool BKM, bool GROUPED>
 __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
-    constexpr int TILE = BKT * (BM + PADS);
     __shared__ __align__(16) double smem[4 * TILE];
-    double (*As)[BKT][BM + PADS] = reinterpret_cast<double (*)[BKT][BM + PADS]>(smem);
-    double (*Bs)[BKT][BN + PADS] = reinterpret_cast<double (*)[BKT][BN + PADS]>(smem + 2 * TILE);
+    double *As = smem;
+    double *Bs = smem + 2 * TILE;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;

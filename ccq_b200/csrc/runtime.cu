@@ -600,8 +600,8 @@ void instantiate(ccq_b200_ctx *c) {
                         if (x & 1) return 0;
                     return 1;
                 };
-                o.g.vec_a = !o.akm ? paired(am, ak, A.base) : 0;
-                o.g.vec_b = !o.bkm ? paired(bn, bk, B.base) : 0;
+                o.g.vec_a = o.akm ? paired(ak, am, A.base) : paired(am, ak, A.base);
+                o.g.vec_b = o.bkm ? paired(bk, bn, B.base) : paired(bn, bk, B.base);
                 o.g.vec_c = o.g.c_nfast ? paired(cn, cm, C.base) : paired(cm, cn, C.base);
             }
             o.g.M = (int)M;
