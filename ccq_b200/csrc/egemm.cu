@@ -88,11 +88,11 @@ int egemm_impl(long long k1, long long k2, long long k3, const double *A, const 
     g.alpha = 1.0;
     g.beta = 0;
     g.c_nfast = 1;
-    long long tiles = ((k1 + 63) / 64) * ((k2 + 63) / 64);
-    int splits = 1;
-    if (tiles < 296 && k3 >= 128) splits = (int)std::min<long long>(std::min<long long>((296 + tiles - 1) / tiles, (k3 + 63) / 64), 128);
-    long long chunk = ((k3 + splits - 1) / splits + 15) / 16 * 16;
-    g.kchunk = (int)std::max<long long>(chunk, 16);
+    // 16-byte operand / output paths: rows of A, B (C) start on even elements
+    g.vec_a = g.vec_b = (k3 % 2 == 0);
+    g.vec_c = (k2 % 2 == 0);
+    g.kchunk = ccqb::gett_f64_kchunk(k1, k2, k3);
+    if (ccqb::gett_f64_prepare() != cudaSuccess) return CCQ_B200_ECUDA;
     if (k3 == 0 || (k3 + g.kchunk - 1) / g.kchunk > 1) cudaMemsetAsync(g_st.c, 0, sizeof(double) * nc, s);
     if (k3 > 0) ccqb::launch_gett_f64(g, 1, 1, s);
     cudaMemcpyAsync(C, g_st.c, sizeof(double) * nc, cudaMemcpyDeviceToHost, s);

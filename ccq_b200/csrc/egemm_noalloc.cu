@@ -80,15 +80,8 @@ extern "C" int ccq_b200_egemm_dev_noalloc(int64_t k1, int64_t k2, int64_t k3, co
     int rc = table_address(&t);
     if (rc) return rc;
     const long long L = kNoAllocMaxDim;
-    long long tiles = ((k1 + 63) / 64) * ((k2 + 63) / 64);
-    int splits = 1;
-    if (tiles < 296 && k3 >= 128) {
-        long long want = (296 + tiles - 1) / tiles, maxs = (k3 + 63) / 64;
-        splits = (int)(want < maxs ? want : maxs);
-        if (splits > 128) splits = 128;
-    }
-    long long chunk = ((k3 + splits - 1) / splits + 15) / 16 * 16;
-    if (chunk < 16) chunk = 16;
+    const long long chunk = ccqb::gett_f64_kchunk(k1, k2, k3);
+    if (ccqb::gett_f64_prepare() != cudaSuccess) return CCQ_B200_ECUDA;
     // split-K partial sums are added atomically into C, which must start at zero
     if (k3 == 0 || (k3 + chunk - 1) / chunk > 1) {
         if (cudaMemsetAsync(C, 0, sizeof(double) * (size_t)(k1 * k2), s) != cudaSuccess) return CCQ_B200_ECUDA;
@@ -112,6 +105,11 @@ extern "C" int ccq_b200_egemm_dev_noalloc(int64_t k1, int64_t k2, int64_t k3, co
     g.alpha = 1.0;
     g.beta = 0;
     g.c_nfast = 1;
+    // 16-byte operand / output paths: 16-byte aligned bases, rows starting on even elements
+    auto al16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    g.vec_a = k3 % 2 == 0 && al16(A);
+    g.vec_b = k3 % 2 == 0 && al16(B);
+    g.vec_c = k2 % 2 == 0 && al16(C);
     g.kchunk = (int)chunk;
     ccqb::launch_gett_f64(g, 1, 1, s);
     return cudaGetLastError() == cudaSuccess ? 0 : CCQ_B200_ECUDA;

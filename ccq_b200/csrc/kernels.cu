@@ -1,6 +1,9 @@
 // Device kernels of libccq_b200; see kernels.cuh for the role of each.
 #include "kernels.cuh"
 
+#include <algorithm>
+#include <mutex>
+
 namespace ccqb {
 
 // ---------------------------------------------------------------------------
@@ -295,9 +298,382 @@ void launch_gett_v(const GettArgs &a, int a_kmajor, int b_kmajor, dim3 grid, cud
         gett_f64_kernel<false, false, G><<<grid, 128, 0, s>>>(a);
 }
 
+// ---------------------------------------------------------------------------
+// Skinny GETT: one side of C has at most 32 entries.  The 64 x 64 tiles above
+// would pad such a contraction to up to 64x its DMMA work; here a BMS x 128
+// tile (BMS = 16 or 32) streams the long operand through a 4-stage cp.async
+// ring, so these mostly memory-bound launches run near the HBM roof.  When N
+// is the short side the kernel runs the transposed problem C^T = B A^T
+// (operands, tables and the output's fast mode exchanged): its rows are always
+// the short side.  All offset tables a tile uses (its rows, columns, output
+// rows and columns, and the K slice's k offsets) are staged in shared memory
+// once, so no copy or store waits on a dependent global read.
+// ---------------------------------------------------------------------------
+constexpr int SBN = 128, SBK = 16, SST = 4;
+constexpr int SKS = SBK + 4;   // [row][k] stride of k-major tiles
+constexpr int SBNS = SBN + 4;  // [k][n] stride of the long operand's n-major tile
+constexpr int SKT = 512;       // k offsets staged per K slice (longer slices read them from global memory)
+template <int BMS>
+struct Skinny {
+    static constexpr int AMS = BMS + 4;  // [k][m] stride of the short operand's m-major tile
+    static constexpr int ATILE = SBK * AMS > BMS * SKS ? SBK * AMS : BMS * SKS;
+    static constexpr int BTILE = SBK * SBNS > SBN * SKS ? SBK * SBNS : SBN * SKS;
+    static constexpr int STAGE = ATILE + BTILE;
+    // dynamic shared memory: offset tables (ints), then the stage ring; a launch
+    // sizes the ring to the K slabs it has (small-K launches keep several CTAs
+    // per SM), but never below the staged C tile
+    static constexpr int OFFB = (2 * (BMS + SBN) + 2 * SKT) * 4;
+    static constexpr int CS_STAGES = (BMS * (SBN + 1) + STAGE - 1) / STAGE;
+    static constexpr int SMEM = OFFB + SST * STAGE * 8;
+    static int smem(int stages) { return OFFB + stages * STAGE * 8; }
+    static_assert(CS_STAGES <= SST, "C tile must fit in the stage ring");
+    static_assert(OFFB % 16 == 0 && ATILE % 2 == 0 && STAGE % 2 == 0, "16-byte aligned tiles");
+    template <bool KM>
+    static __device__ __forceinline__ int ai(int k, int m) { return KM ? m * SKS + k : k * AMS + m; }
+    template <bool KM>
+    static __device__ __forceinline__ int bi(int k, int n) { return KM ? n * SKS + k : k * SBNS + n; }
+};
+
+// One contraction term in the launched orientation (A short, B long).
+struct SkTerm {
+    const double *A, *B;
+    const int *am, *ak, *bn, *bk;
+};
+
+// Offset tables of the current tile and K slice in shared memory.  ka / kb are
+// indexed by k - kb0 (the staged slice, kb0 = its first k) or point at the
+// global tables (kb0 = 0) when the slice is longer than SKT.
+struct SkTabs {
+    int *a, *b, *cm, *cn, *ska, *skb;
+    const int *ka, *kb;
+    int kb0;
+};
+
+// Loads the k-slab [k0, k0 + SBK) of both operands into one ring stage.
+// Out-of-range elements are zero-filled.
+template <int BMS, bool AK, bool BKM>
+__device__ __forceinline__ void skinny_load(double *st, const SkTerm &p, const SkTabs &t, int M, int N, int m0, int n0,
+                                            int k0, int kend, int tid, bool vb) {
+    using T = Skinny<BMS>;
+    double *As = st, *Bs = st + T::ATILE;
+    if (AK) {
+        const int kk = tid & 15, k = k0 + kk;
+        const bool kin = k < kend;
+        const int ok = kin ? t.ka[k - t.kb0] : 0;
+#pragma unroll
+        for (int q = 0; q < BMS / 8; ++q) {
+            const int m = (tid >> 4) + 8 * q;
+            const bool in = kin && m0 + m < M;
+            cp_async8(&As[T::template ai<true>(kk, m)], in ? p.A + (long long)t.a[m] + ok : p.A, in);
+        }
+    } else {
+        constexpr int R = 128 / BMS;  // k rows per pass
+        const int m = tid % BMS;
+        const bool min_ = m0 + m < M;
+        const long long om = t.a[m];
+#pragma unroll
+        for (int q = 0; q < SBK / R; ++q) {
+            const int kk = tid / BMS + R * q, k = k0 + kk;
+            const bool in = min_ && k < kend;
+            cp_async8(&As[T::template ai<false>(kk, m)], in ? p.A + om + t.ka[k - t.kb0] : p.A, in);
+        }
+    }
+    if (BKM && vb) {
+        // k pairs are contiguous and 16-byte aligned
+        const int kk = 2 * (tid & 7), k = k0 + kk;
+        const bool kin = k < kend;
+        const int ok = kin ? t.kb[k - t.kb0] : 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int n = (tid >> 3) + 16 * q;
+            const bool in = kin && n0 + n < N;
+            cp_async16(&Bs[T::template bi<true>(kk, n)], in ? p.B + (long long)t.b[n] + ok : p.B, in);
+        }
+    } else if (BKM) {
+        const int kk = tid & 15, k = k0 + kk;
+        const bool kin = k < kend;
+        const int ok = kin ? t.kb[k - t.kb0] : 0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int n = (tid >> 4) + 8 * q;
+            const bool in = kin && n0 + n < N;
+            cp_async8(&Bs[T::template bi<true>(kk, n)], in ? p.B + (long long)t.b[n] + ok : p.B, in);
+        }
+    } else if (vb) {
+        // n pairs are contiguous and 16-byte aligned
+        const int n = 2 * (tid & 63);
+        const bool nin = n0 + n < N;
+        const long long on = t.b[n];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int kk = (tid >> 6) + 2 * q, k = k0 + kk;
+            const bool in = nin && k < kend;
+            cp_async16(&Bs[T::template bi<false>(kk, n)], in ? p.B + on + t.kb[k - t.kb0] : p.B, in);
+        }
+    } else {
+        const int n = tid;
+        const bool nin = n0 + n < N;
+        const long long on = t.b[n];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int k = k0 + q;
+            const bool in = nin && k < kend;
+            cp_async8(&Bs[T::template bi<false>(q, n)], in ? p.B + on + t.kb[k - t.kb0] : p.B, in);
+        }
+    }
+}
+
+// K loop of one term over [kbeg, kend): SST-stage ring, one barrier per slab
+// (the slab loaded at step t overwrites the stage computed at step t - 1).
+template <int BMS, bool AK, bool BKM>
+__device__ __forceinline__ void skinny_mainloop(double (&acc)[BMS / 16][4][4], double *sm, SkTabs &t,
+                                                const SkTerm &p, int M, int N, int m0, int n0, int kbeg, int kend,
+                                                int tid, int wn, int gid, int tig, bool vb) {
+    using T = Skinny<BMS>;
+    __syncthreads();  // earlier users of the tables and of the ring are done
+    for (int i = tid; i < BMS; i += 128) t.a[i] = m0 + i < M ? __ldg(p.am + m0 + i) : 0;
+    for (int i = tid; i < SBN; i += 128) t.b[i] = n0 + i < N ? __ldg(p.bn + n0 + i) : 0;
+    const int klen = kend - kbeg;
+    if (klen <= SKT) {
+        for (int i = tid; i < klen; i += 128) {
+            t.ska[i] = __ldg(p.ak + kbeg + i);
+            t.skb[i] = __ldg(p.bk + kbeg + i);
+        }
+        t.ka = t.ska;
+        t.kb = t.skb;
+        t.kb0 = kbeg;
+    } else {
+        t.ka = p.ak;
+        t.kb = p.bk;
+        t.kb0 = 0;
+    }
+    __syncthreads();
+    const int nt = kend > kbeg ? (kend - kbeg + SBK - 1) / SBK : 0;
+#pragma unroll
+    for (int s = 0; s < SST - 1; ++s) {
+        if (s < nt) skinny_load<BMS, AK, BKM>(sm + s * T::STAGE, p, t, M, N, m0, n0, kbeg + s * SBK, kend, tid, vb);
+        cp_async_commit();
+    }
+    for (int it = 0; it < nt; ++it) {
+        cp_async_wait<SST - 2>();
+        __syncthreads();
+        const int tn = it + SST - 1;
+        if (tn < nt)
+            skinny_load<BMS, AK, BKM>(sm + (tn % SST) * T::STAGE, p, t, M, N, m0, n0, kbeg + tn * SBK, kend, tid, vb);
+        cp_async_commit();
+        const double *As = sm + (it % SST) * T::STAGE, *Bs = As + T::ATILE;
+#pragma unroll
+        for (int kk = 0; kk < SBK; kk += 4) {
+            double a[BMS / 16][2], b[4];
+#pragma unroll
+            for (int mi = 0; mi < BMS / 16; ++mi) {
+                a[mi][0] = As[T::template ai<AK>(kk + tig, mi * 16 + gid)];
+                a[mi][1] = As[T::template ai<AK>(kk + tig, mi * 16 + gid + 8)];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[T::template bi<BKM>(kk + tig, wn + ni * 8 + gid)];
+#pragma unroll
+            for (int mi = 0; mi < BMS / 16; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], a[mi][0], a[mi][1], b[ni]);
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+template <int BMS, bool AK, bool BKM, bool GROUPED>
+__global__ void __launch_bounds__(128) gett_f64_skinny_kernel(GettArgs g) {
+    using T = Skinny<BMS>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    SkTabs t;
+    t.a = reinterpret_cast<int *>(smraw);
+    t.b = t.a + BMS;
+    t.cm = t.b + SBN;
+    t.cn = t.cm + BMS;
+    t.ska = t.cn + SBN;
+    t.skb = t.ska + SKT;
+    double *sm = reinterpret_cast<double *>(smraw + T::OFFB);
+    const bool sw = g.N < g.M;  // transposed launch: N is the short side
+    const int M = sw ? g.N : g.M, N = sw ? g.M : g.N;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gid = lane >> 2, tig = lane & 3, wn = warp * 32;
+    const int n0 = blockIdx.x * SBN, m0 = blockIdx.y * BMS;
+    const bool vb = (sw ? g.vec_a : g.vec_b) != 0;
+    // output offsets in the launched orientation (read after the mainloop's barriers)
+    {
+        const int *offm = sw ? g.offC_n : g.offC_m, *offn = sw ? g.offC_m : g.offC_n;
+        for (int i = tid; i < BMS; i += 128) t.cm[i] = m0 + i < M ? __ldg(offm + m0 + i) : 0;
+        for (int i = tid; i < SBN; i += 128) t.cn[i] = n0 + i < N ? __ldg(offn + n0 + i) : 0;
+    }
+
+    double acc[BMS / 16][4][4];
+#pragma unroll
+    for (int i = 0; i < BMS / 16; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+    double alpha = g.alpha;
+    if (GROUPED) {
+        for (int sgi = 0; sgi < g.nseg; ++sgi) {
+            const GettSeg sg = g.segs[sgi];
+            if (sgi > 0) {
+                const double r = g.segs[sgi - 1].alpha / sg.alpha;
+#pragma unroll
+                for (int i = 0; i < BMS / 16; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[i][j][q] *= r;
+            }
+            const SkTerm p = sw ? SkTerm{sg.B, sg.A, sg.offB_n, sg.offB_k, sg.offA_m, sg.offA_k}
+                                : SkTerm{sg.A, sg.B, sg.offA_m, sg.offA_k, sg.offB_n, sg.offB_k};
+            skinny_mainloop<BMS, AK, BKM>(acc, sm, t, p, M, N, m0, n0, 0, sg.K, tid, wn, gid, tig, vb);
+            alpha = sg.alpha;
+        }
+    } else {
+        const SkTerm p = sw ? SkTerm{g.B, g.A, g.offB_n, g.offB_k, g.offA_m, g.offA_k}
+                            : SkTerm{g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k};
+        const int kbeg = blockIdx.z * g.kchunk;
+        const int kend = min(g.K, kbeg + g.kchunk);
+        skinny_mainloop<BMS, AK, BKM>(acc, sm, t, p, M, N, m0, n0, kbeg, kend, tid, wn, gid, tig, vb);
+    }
+
+    // epilogue: stage the tile, then write along the output's contiguous mode
+    double (*Cs)[SBN + 1] = reinterpret_cast<double (*)[SBN + 1]>(sm);
+#pragma unroll
+    for (int mi = 0; mi < BMS / 16; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    Cs[mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = alpha * acc[mi][ni][2 * h + j];
+    __syncthreads();
+    const bool atomic = gridDim.z > 1;
+    const bool nfast = sw ? !g.c_nfast : g.c_nfast;
+    constexpr int R = 128 / BMS;
+    // nfast: a thread owns column n = tid and walks the BMS rows; else BMS
+    // consecutive threads cover the rows of one column, R columns per pass
+    const int fl = nfast ? tid : tid % BMS;
+    const int sl0 = nfast ? 0 : tid / BMS;
+    const int sstep = nfast ? 1 : R;
+    const int nsl = nfast ? BMS : SBN / R;
+    const bool fin = nfast ? n0 + fl < N : m0 + fl < M;
+    const long long ofix = nfast ? t.cn[fl] : t.cm[fl];
+    for (int s0 = 0; s0 < nsl; s0 += 8) {
+        double *cp[8];
+        double cv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int sl = sl0 + sstep * (s0 + u);
+            const int ml = nfast ? sl : fl, nl = nfast ? fl : sl;
+            const bool in = fin && m0 + ml < M && n0 + nl < N;
+            cp[u] = in ? g.C + ofix + (nfast ? t.cm[ml] : t.cn[nl]) : nullptr;
+            cv[u] = Cs[ml][nl];
+        }
+        if (atomic) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (cp[u]) atomicAdd(cp[u], cv[u]);
+        } else {
+            double old[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) old[u] = (cp[u] && g.beta) ? *cp[u] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (cp[u]) *cp[u] = old[u] + cv[u];
+        }
+    }
+}
+
+template <int BMS, bool G>
+void launch_skinny_v(const GettArgs &a, int ak, int bk, dim3 grid, cudaStream_t s) {
+    // ring stages: every K slab of a slice when they fit below SST (all loaded
+    // in the prologue), else the full ring; grouped launches take the full ring
+    int stages = SST;
+    if (!G) {
+        const int nt = (std::min(a.K, a.kchunk) + SBK - 1) / SBK;
+        if (nt < SST) stages = std::max(nt, Skinny<BMS>::CS_STAGES);
+    }
+    const int sm = Skinny<BMS>::smem(stages);
+    if (ak && bk)
+        gett_f64_skinny_kernel<BMS, true, true, G><<<grid, 128, sm, s>>>(a);
+    else if (ak)
+        gett_f64_skinny_kernel<BMS, true, false, G><<<grid, 128, sm, s>>>(a);
+    else if (bk)
+        gett_f64_skinny_kernel<BMS, false, true, G><<<grid, 128, sm, s>>>(a);
+    else
+        gett_f64_skinny_kernel<BMS, false, false, G><<<grid, 128, sm, s>>>(a);
+}
+
+template <int BMS, bool G>
+cudaError_t skinny_attr() {
+    constexpr int sm = Skinny<BMS>::SMEM;
+    constexpr auto at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, true, true, G>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, true, false, G>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, false, true, G>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, false, false, G>, at, sm);
+    return e;
+}
+
+cudaError_t gett_f64_prepare() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        err = skinny_attr<16, false>();
+        if (err == cudaSuccess) err = skinny_attr<16, true>();
+        if (err == cudaSuccess) err = skinny_attr<32, false>();
+        if (err == cudaSuccess) err = skinny_attr<32, true>();
+    });
+    return err;
+}
+
+int gett_f64_family(long long M, long long N) {
+    if (M <= 32 && M <= N) return 1;
+    if (N <= 32 && N < M) return 2;
+    return 0;
+}
+
+int gett_f64_kchunk(long long M, long long N, long long K) {
+    if (M <= 0 || N <= 0 || K <= 0) return 16;  // nothing is launched
+    long long splits = 1;
+    if (gett_f64_family(M, N)) {
+        // stream the long operand with about two resident waves of CTAs
+        long long shrt = std::min(M, N), lng = std::max(M, N);
+        long long tiles = ((lng + SBN - 1) / SBN) * ((shrt + (shrt <= 16 ? 15 : 31)) / (shrt <= 16 ? 16 : 32));
+        if (tiles < 592 && K >= 64) splits = std::min<long long>(std::min<long long>((592 + tiles - 1) / tiles, (K + 63) / 64), 256);
+    } else {
+        long long tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+        if (tiles < 296 && K >= 128) splits = std::min<long long>(std::min<long long>((296 + tiles - 1) / tiles, (K + 31) / 32), 128);
+    }
+    if (splits < 1) splits = 1;
+    long long chunk = (K + splits - 1) / splits;
+    chunk = (chunk + 15) / 16 * 16;
+    return (int)std::max<long long>(chunk, 16);
+}
+
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
-    dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, a.segs ? 1 : (a.K + a.kchunk - 1) / a.kchunk);
-    if (grid.z == 0) grid.z = 1;
+    const int zsplit = a.segs ? 1 : std::max(1, (a.K + a.kchunk - 1) / a.kchunk);
+    const int fam = gett_f64_family(a.M, a.N);
+    if (fam) {
+        gett_f64_prepare();
+        const int shrt = std::min(a.M, a.N), lng = std::max(a.M, a.N);
+        const int ak = fam == 2 ? b_kmajor : a_kmajor, bk = fam == 2 ? a_kmajor : b_kmajor;
+        if (shrt <= 16) {
+            dim3 grid((lng + SBN - 1) / SBN, (shrt + 15) / 16, zsplit);
+            a.segs ? launch_skinny_v<16, true>(a, ak, bk, grid, s) : launch_skinny_v<16, false>(a, ak, bk, grid, s);
+        } else {
+            dim3 grid((lng + SBN - 1) / SBN, (shrt + 31) / 32, zsplit);
+            a.segs ? launch_skinny_v<32, true>(a, ak, bk, grid, s) : launch_skinny_v<32, false>(a, ak, bk, grid, s);
+        }
+        return;
+    }
+    dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, zsplit);
     if (a.segs)
         launch_gett_v<true>(a, a_kmajor, b_kmajor, grid, s);
     else

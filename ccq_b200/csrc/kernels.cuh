@@ -89,6 +89,15 @@ struct AsmArgs {
     const unsigned char *combos;
 };
 
+// FP64 GETT.  Tile family by output shape: 0 = 64 x 64 tiles; 1 = skinny rows
+// (M <= 32), 2 = skinny columns (N <= 32, run transposed).  kchunk is the K
+// range of one split-K slice that launch_gett_f64 expects in GettArgs::kchunk
+// (more than one slice adds into C atomically, so C must start at zero).
+int gett_f64_family(long long M, long long N);
+int gett_f64_kchunk(long long M, long long N, long long K);
+// Sets the shared-memory limits of the skinny kernels; call once before the
+// first launch (outside stream capture).
+cudaError_t gett_f64_prepare();
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s);
 void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N, cudaStream_t s);
 void launch_assemble(const AsmArgs &a, cudaStream_t s);

@@ -609,17 +609,7 @@ void instantiate(ccq_b200_ctx *c) {
             o.g.K = (int)K;
             o.g.alpha = o.alpha * kscale;
             o.g.beta = o.beta;
-            long long tiles = ((M + 63) / 64) * ((N + 63) / 64);
-            int splits = 1;
-            if (tiles < 296 && K >= 128) {
-                long long want = (296 + tiles - 1) / tiles;
-                long long maxs = (K + 63) / 64;
-                splits = (int)std::min<long long>(std::min<long long>(want, maxs), 128);
-                if (splits < 1) splits = 1;
-            }
-            long long chunk = (K + splits - 1) / splits;
-            chunk = (chunk + 15) / 16 * 16;
-            if (chunk < 16) chunk = 16;
+            long long chunk = gett_f64_kchunk(M, N, K);
             o.g.kchunk = (int)chunk;
             o.zero_first = (K + chunk - 1) / chunk > 1 && o.beta == 0;
             if (K == 0) o.g.kchunk = 16;
@@ -1033,6 +1023,7 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(CCQ_B200_ENODEV, "no CUDA device");
         c = new ccq_b200_ctx();
         CK(cudaGetDevice(&c->device));
+        CK(gett_f64_prepare());
         c->calc_type = ct;
         c->rhf = rhf != 0;
         c->shift = shift;

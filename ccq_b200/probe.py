@@ -1,6 +1,8 @@
 """Single-kernel probes for profiling (one GETT launch of a fixed shape).
 
     python -m ccq_b200.probe egemm K1 K2 K3 [repeats]
+    python -m ccq_b200.probe egemm_split K1 K2 K3 [slices]
+    python -m ccq_b200.probe sweep fp64|split OUTFILE [warm-up iterations]
 
 Runs ccq_b200_egemm (the FP64 GETT kernel) on random column-major operands;
 the vvvv ladder of the CCSDT T3 update at 40 orbitals is (1024, 16384, 1024).
@@ -45,18 +47,20 @@ def main(argv):
         from ccq_b200 import synth
         prec = argv[1] if len(argv) > 1 else 'fp64'
         out = argv[2] if len(argv) > 2 else 'ops_profile.txt'
+        warm = int(argv[3]) if len(argv) > 3 else 3
         s = synth.system(synth.C2)
         d = s['dims']
+        # a one-vector DIIS ring keeps the device footprint small for profiler captures
         ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CCSDT', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
-                          s['v_bb'])
+                          s['v_bb'], diis_space=1)
         ctx.set_precision(lib.PREC_SPLIT if prec == 'split' else lib.PREC_FP64, 4)
-        for it in range(1, 4):
+        for it in range(1, warm + 1):
             ctx.iterate(it)
         if os.path.exists(out):
             os.remove(out)
         os.environ['CCQ_B200_PROFILE_DUMP'] = out
         ctx.profile(True)
-        ctx.iterate(4)
+        ctx.iterate(warm + 1)
         print(ctx.profile_get())
         ctx.close()
     else:

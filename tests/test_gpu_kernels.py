@@ -5,7 +5,11 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 SHAPES = [(1, 1, 1), (7, 5, 3), (64, 64, 16), (100, 37, 513), (257, 3, 1000), (3, 300, 5000),
-          (1000, 1000, 64), (1024, 64, 1024), (65, 129, 17)]
+          (1000, 1000, 64), (1024, 64, 1024), (65, 129, 17),
+          # skinny tiles (one side <= 32): split-K, transposed launch, 16- and 32-row tiles,
+          # odd and even K (8- and 16-byte operand copies), long outputs without split-K
+          (8, 2048, 8192), (2048, 8, 4096), (16, 100000, 8), (32, 5000, 300), (1, 70000, 256),
+          (33, 40, 1000), (17, 3000, 64), (4000, 17, 130), (24, 24, 2001), (30, 1001, 7)]
 
 
 @pytest.mark.parametrize('k1,k2,k3', SHAPES)

@@ -64,6 +64,13 @@ def test_split_sweeps_then_fp64_converge_to_fp64_energy():
         assert not r.failed
         if prec == 'split':
             assert sum(1 for h in r.history if h['split']) >= 3
+            # the sliced kernels really ran on this system's ladder terms
+            ctx.set_precision(lib.PREC_SPLIT, 4)
+            ctx.profile(True)
+            ctx.iterate(r.iterations + 1)
+            prof = ctx.profile_get()
+            ctx.profile(False)
+            assert prof['gett_split']['launches'] > 0
         es[prec] = r.e_cor
         ctx.close()
     assert abs(es['split'] - es['fp64']) < 1e-10
