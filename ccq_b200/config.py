@@ -78,9 +78,12 @@ class Config:
             self.lvl_t, self.lvl_q = True, False
         elif ct == 'CCSDTQ':
             self.lvl_t, self.lvl_q = True, True
+        elif ct == 'CR-CC(2,3)':
+            # src/parser.f90:368-377: CCSD, then hbar, left CCSD and the MM(2,3) correction
+            self.lvl_t, self.lvl_q = False, False
         else:
             raise ValueError(f'calc_type {ct!r} is not served by this engine '
-                             '(CCSD, CCSDT, CCSDTQ are; the others stay on the CPU program)')
+                             '(CCSD, CCSDT, CCSDTQ, CR-CC(2,3) are; the others stay on the CPU program)')
         return self
 
 

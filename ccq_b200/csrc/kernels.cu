@@ -727,6 +727,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
     constexpr int CH = 128;
     __shared__ SmTerm<RK> st[CH];
     const int nch = (a.nterms + CH - 1) / CH;
+    double nacc = 0.0;
     for (long long base = blockIdx.x * (long long)blockDim.x; base < a.total;
          base += (long long)gridDim.x * blockDim.x) {
         const long long lin = base + threadIdx.x;
@@ -833,8 +834,12 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
 #pragma unroll
         for (int d = 0; d < RK; ++d) toff += (long long)a.tstride[d] * x[d];
         double tnew;
-        if (a.mode == 0) {
+        if (a.mode != 1) {
             double D = a.shift;
+            if (a.mode == 2) {
+                D -= *a.ecor;
+                nacc += a.nperm * R * R;
+            }
 #pragma unroll
             for (int d = 0; d < RK; ++d) {
                 if (d < RK / 2)
@@ -853,6 +858,10 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
             for (int d = 0; d < RK; ++d) o += (long long)a.tstride[d] * pick<RK>(x, P[d]);
             a.T[o] = a.psign[pidx] * tnew;
         }
+    }
+    if (a.mode == 2) {
+        for (int o = 16; o > 0; o >>= 1) nacc += __shfl_down_sync(0xffffffffu, nacc, o);
+        if ((threadIdx.x & 31) == 0 && nacc != 0.0) atomicAdd(a.norm, nacc);
     }
 }
 

@@ -71,10 +71,12 @@ struct AsmArgs {
     int tstride[MAXR];
     int spin[MAXR];           // 0 alpha, 1 beta per axis
     int runstart[MAXR];       // 1 if this axis starts a same-spin run within its half
-    const double *fdiag[2];   // undressed Fock diagonals (active range)
+    const double *fdiag[2];   // denominator diagonals (active range): Fock, or Hbar for mode 2
     int nocc[2];
     double shift;
-    int mode;                 // 0 jacobi, 1 copy
+    int mode;                 // 0 jacobi, 1 copy, 2 left jacobi (shift - *ecor, sum of R^2 into *norm)
+    const double *ecor;       // mode 2: correlation energy subtracted from the denominators
+    double *norm;             // mode 2: accumulates nperm * R^2 (every stored element's LH^2)
     int nterms;
     const AsmTerm *terms;
     int nperm;                // orbit permutations of a canonical element

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/ccq_b200.h"
+#include "crcc.cuh"
 #include "kernels.cuh"
 #include "plans_embedded.h"
 #include "split.cuh"
@@ -81,7 +82,7 @@ ViewSpec parse_view(const std::string &tok) {
     return v;
 }
 
-enum OpKind { OP_GETT, OP_ASM, OP_COPY, OP_ZERO, OP_PHASE };
+enum OpKind { OP_GETT, OP_ASM, OP_COPY, OP_ZERO, OP_PHASE, OP_CRDIAG, OP_LENERGY, OP_CRCC };
 
 struct Op {
     OpKind kind;
@@ -107,6 +108,7 @@ struct Op {
     int group_size = 0;
     std::vector<int> hcm, hcn; // output offset tables (grouping key)
     AsmArgs asmargs{};
+    CrccArgs crcc{};           // CRCC: one spin block's four-denominator sums
 };
 
 struct BufSpec {
@@ -198,6 +200,11 @@ Plan parse_plan(const char *text) {
                 o.terms.push_back({coef, parse_view(vv)});
             }
             p.ops.push_back(o);
+        } else if (w == "CRDIAG" || w == "LENERGY" || w == "CRCC") {
+            Op o;
+            o.kind = w == "CRDIAG" ? OP_CRDIAG : (w == "LENERGY" ? OP_LENERGY : OP_CRCC);
+            ls >> o.arg0;
+            p.ops.push_back(o);
         } else if (w == "COPY" || w == "ZERO" || w == "PHASE") {
             Op o;
             o.kind = w == "COPY" ? OP_COPY : (w == "ZERO" ? OP_ZERO : OP_PHASE);
@@ -213,7 +220,8 @@ Plan parse_plan(const char *text) {
 }
 
 const char *find_plan(const std::string &calc_type, bool rhf) {
-    std::string key = calc_type + (rhf ? "_rhf" : "");
+    // plan file names: the calc_type, with CR-CC(2,3) stored as CRCC23
+    std::string key = (calc_type == "CR-CC(2,3)" ? std::string("CRCC23") : calc_type) + (rhf ? "_rhf" : "");
     for (int i = 0; ccqb_plans[i].name; ++i)
         if (key == ccqb_plans[i].name) return ccqb_plans[i].text;
     return nullptr;
@@ -254,6 +262,14 @@ struct ccq_b200_ctx {
     double prof_flops[4] = {0, 0, 0, 0};
     long long prof_launch[4] = {0, 0, 0, 0};
     size_t energy_op = 0;
+    // CR-CC(2,3) plans: the CC sweep and energy end at the 'crcc' marker; the
+    // left solve and the triples corrections follow in their own phases
+    size_t cc_end = 0, lambda_op = 0, lenergy_op = 0, triples_op = 0;
+    bool has_crcc = false;
+    double *lvec = nullptr, *lring = nullptr;
+    long long l_size = 0;
+    CrDiagArgs crd{};
+    cudaGraphExec_t lgexec = nullptr;
     double flops = 0.0;
     long long launches = 0;
     double sweep_ms = 0.0;
@@ -272,6 +288,7 @@ struct ccq_b200_ctx {
     }
     ~ccq_b200_ctx() {
         if (gexec) cudaGraphExecDestroy(gexec);
+        if (lgexec) cudaGraphExecDestroy(lgexec);
         split_free(split);
         for (void *p : owned) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
@@ -387,7 +404,28 @@ void instantiate(ccq_b200_ctx *c) {
         off += ne;
     }
     c->t_size = off;
-    c->vec_size = (c->calc_type == "CCSD") ? tv_off["T3A"] : c->t_size;
+    // CR-CC(2,3) solves CCSD; its DIIS vector is T1 + T2 (the T3 slots stay zero)
+    c->vec_size = (c->calc_type == "CCSD" || c->calc_type == "CR-CC(2,3)") ? tv_off["T3A"] : c->t_size;
+    // left amplitudes (L1A..L2C) share the T1/T2 layout in their own vector
+    std::map<std::string, long long> lv_off;
+    {
+        static const char *lv_order[] = {"L1A", "L1B", "L2A", "L2B", "L2C"};
+        long long lo = 0;
+        for (auto *nm : lv_order) {
+            auto it = bdims.find(nm);
+            if (it == bdims.end()) continue;
+            long long ne = 1;
+            for (auto &d : it->second) ne *= tok(c, d);
+            lv_off[nm] = lo;
+            lo += ne;
+        }
+        c->l_size = lo;
+        if (lo) {
+            c->lvec = (double *)c->dalloc(sizeof(double) * lo);
+            c->lring = (double *)c->dalloc(sizeof(double) * (size_t)(c->ds + 1) * lo);
+            CK(cudaMemsetAsync(c->lvec, 0, sizeof(double) * lo, c->stream));
+        }
+    }
     c->tvec = (double *)c->dalloc(sizeof(double) * c->t_size);
     CK(cudaMemsetAsync(c->tvec, 0, sizeof(double) * c->t_size, c->stream));
 
@@ -457,6 +495,8 @@ void instantiate(ccq_b200_ctx *c) {
         d.groups = b.groups;
         if (tv_off.count(b.name)) {
             d.ptr = c->tvec + tv_off[b.name];
+        } else if (lv_off.count(b.name)) {
+            d.ptr = c->lvec + lv_off[b.name];
         } else if (b.kind == "work") {
             d.ptr = arena_ptr + work_off[b.name];
         } else {
@@ -482,9 +522,76 @@ void instantiate(ccq_b200_ctx *c) {
     };
     std::vector<PendA> penda;
     c->flops = 0.0;
+    c->cc_end = c->plan.ops.size();
     for (size_t i = 0; i < c->plan.ops.size(); ++i) {
         Op &o = c->plan.ops[i];
         if (o.kind == OP_PHASE && o.arg0 == "energy") c->energy_op = i;
+        if (o.kind == OP_PHASE && o.arg0 == "crcc") {
+            c->cc_end = i;
+            c->has_crcc = true;
+        }
+        if (o.kind == OP_PHASE && o.arg0 == "lambda") c->lambda_op = i;
+        if (o.kind == OP_PHASE && o.arg0 == "lenergy") c->lenergy_op = i;
+        if (o.kind == OP_PHASE && o.arg0 == "triplesA") c->triples_op = i;
+        if (o.kind == OP_CRCC) {
+            const std::string x = o.arg0;
+            if (x.size() != 1 || x[0] < 'A' || x[0] > 'D') throw Error(CCQ_B200_EPLAN, "CRCC block " + x);
+            const DevBuf &M = c->bufs.at("M3" + x), &L = c->bufs.at("L3" + x);
+            if (M.shape != L.shape || M.shape.size() != 6) throw Error(CCQ_B200_EPLAN, "CRCC block shapes");
+            CrccArgs &r = o.crcc;
+            r.M = M.ptr;
+            r.L = L.ptr;
+            r.total = M.numel;
+            for (int d = 0; d < 6; ++d) r.dims[d] = (int)M.shape[d];
+            const int nb = x[0] - 'A';
+            for (int k = 0; k < 3; ++k) r.spin[k] = k < 3 - nb ? 0 : 1;
+            r.off[0] = (int)c->oa;
+            r.off[1] = (int)c->ob;
+            r.n = (int)c->n;
+            r.fd[0] = c->fdiag_a;
+            r.fd[1] = c->fdiag_b;
+            r.hd[0] = c->bufs.at("HDA").ptr;
+            r.hd[1] = c->bufs.at("HDB").ptr;
+            r.h2aa = c->bufs.at("H2AA").ptr;
+            r.h2ab = c->bufs.at("H2AB").ptr;
+            r.h2bb = c->bufs.at("H2BB").ptr;
+            for (int q = 0; q < 4; ++q) {
+                r.w1[q] = c->bufs.at(std::string("W1") + char('A' + q)).ptr;
+                r.w2[q] = c->bufs.at(std::string("W2") + char('A' + q)).ptr;
+            }
+            r.e23 = c->bufs.at("E23").ptr;
+        }
+        if (o.kind == OP_CRDIAG) {
+            CrDiagArgs &g = c->crd;
+            g.FA = c->bufs.at("FA").ptr;
+            g.FB = c->bufs.at("FB").ptr;
+            g.VAA = c->bufs.at("VAA").ptr;
+            g.VAB = c->bufs.at("VAB").ptr;
+            g.VBB = c->bufs.at("VBB").ptr;
+            g.VAA0 = c->bufs.at("VAA0").ptr;
+            g.VAB0 = c->bufs.at("VAB0").ptr;
+            g.VBB0 = c->bufs.at("VBB0").ptr;
+            g.T2A = c->bufs.at("T2A").ptr;
+            g.T2B = c->bufs.at("T2B").ptr;
+            g.T2C = c->bufs.at("T2C").ptr;
+            g.HDA = c->bufs.at("HDA").ptr;
+            g.HDB = c->bufs.at("HDB").ptr;
+            g.H2AA = c->bufs.at("H2AA").ptr;
+            g.H2AB = c->bufs.at("H2AB").ptr;
+            g.H2BB = c->bufs.at("H2BB").ptr;
+            for (int q = 0; q < 4; ++q) {
+                g.W1[q] = c->bufs.at(std::string("W1") + char('A' + q)).ptr;
+                g.W2[q] = c->bufs.at(std::string("W2") + char('A' + q)).ptr;
+            }
+            g.n = (int)c->n;
+            g.oa = (int)c->oa;
+            g.ob = (int)c->ob;
+            g.va = (int)c->va;
+            g.vb = (int)c->vb;
+            // cal_d3's beta-beta-beta term sums e = occ_a + 2 .. orbs (src/mm_correct.f90:455-463):
+            // beta virtuals from relative index occ_a - occ_b + 1
+            g.w1d_e0 = (int)std::max(0LL, c->oa + 1 - c->ob);
+        }
         if (o.kind == OP_GETT) {
             Resolved C = resolve(c, o.c), A = resolve(c, o.a), B = resolve(c, o.b);
             std::vector<std::string> ml, nl, kl;
@@ -640,7 +747,20 @@ void instantiate(ccq_b200_ctx *c) {
             a.nocc[0] = (int)c->oa;
             a.nocc[1] = (int)c->ob;
             a.shift = c->shift;
-            a.mode = o.mode == "jacobi" ? 0 : 1;
+            if (o.mode == "jacobi") {
+                a.mode = 0;
+            } else if (o.mode == "copy") {
+                a.mode = 1;
+            } else if (o.mode == "ljacobi") {
+                // left Jacobi step: Hbar one-body diagonal, shift - E_cor, sum of LH^2 into LN
+                a.mode = 2;
+                a.fdiag[0] = c->bufs.at("HDA").ptr;
+                a.fdiag[1] = c->bufs.at("HDB").ptr;
+                a.ecor = c->bufs.at("ECOR").ptr;
+                a.norm = c->bufs.at("LN").ptr;
+            } else {
+                throw Error(CCQ_B200_EPLAN, "assemble mode " + o.mode);
+            }
             std::vector<std::string> target;
             for (int k = 0; k < level; ++k) target.push_back("i" + std::to_string(k));
             for (int k = 0; k < level; ++k) target.push_back("a" + std::to_string(k));
@@ -908,6 +1028,18 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
             }
             case OP_PHASE:
                 break;
+            case OP_CRDIAG:
+                launch_crdiag(c->crd, c->stream);
+                ++c->launches;
+                break;
+            case OP_LENERGY:
+                launch_lenergy(c->bufs.at("LN").ptr, c->bufs.at("ECOR").ptr, c->bufs.at("EL").ptr, c->stream);
+                ++c->launches;
+                break;
+            case OP_CRCC:
+                launch_crcc_sum(o.crcc, c->stream);
+                ++c->launches;
+                break;
         }
         if (prof) CK(cudaEventRecord(c->pev[2 * i + 1], c->stream));
     }
@@ -947,7 +1079,7 @@ void sweep(ccq_b200_ctx *c) {
             long long l0 = c->launches;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             try {
-                run_ops(c, 0, c->plan.ops.size());
+                run_ops(c, 0, c->cc_end);
             } catch (...) {
                 cudaStreamEndCapture(c->stream, &g);
                 throw;
@@ -959,13 +1091,14 @@ void sweep(ccq_b200_ctx *c) {
         }
         CK(cudaGraphLaunch(c->gexec, c->stream));
     } else {
-        run_ops(c, 0, c->plan.ops.size());
+        run_ops(c, 0, c->cc_end);
     }
 }
 
 long long count_sweep_launches(ccq_b200_ctx *c) {
     long long n = 0;
-    for (auto &o : c->plan.ops) {
+    for (size_t i = 0; i < c->cc_end; ++i) {
+        const Op &o = c->plan.ops[i];
         if (o.kind == OP_GETT && o.g.M && o.g.N && !o.skip) {
             if (o.zero_first || o.g.K == 0) ++n;
             if (o.g.K)
@@ -1014,8 +1147,8 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         if (fr < 0 || oa < 1 || ob < 1 || va < 1 || vb < 1)
             throw Error(CCQ_B200_EINVAL, "invalid dimensions (need at least one occupied and virtual per spin)");
         std::string ct(calc_type);
-        if (ct != "CCSD" && ct != "CCSDT" && ct != "CCSDTQ")
-            throw Error(CCQ_B200_EINVAL, "calc_type must be CCSD, CCSDT or CCSDTQ");
+        if (ct != "CCSD" && ct != "CCSDT" && ct != "CCSDTQ" && ct != "CR-CC(2,3)")
+            throw Error(CCQ_B200_EINVAL, "calc_type must be CCSD, CCSDT, CCSDTQ or CR-CC(2,3)");
         if (rhf && oa != ob) throw Error(CCQ_B200_EINVAL, "rhf requires occ_a == occ_b");
         const char *text = find_plan(ct, rhf != 0);
         if (!text) throw Error(CCQ_B200_EPLAN, "no plan for " + ct);
@@ -1034,7 +1167,7 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         c->vb = vb;
         c->n = n;
         c->froz = fr;
-        c->size = {{"oa", oa}, {"ob", ob}, {"va", va}, {"vb", vb}, {"n", n}, {"1", 1}, {"0", 0}};
+        c->size = {{"oa", oa}, {"ob", ob}, {"va", va}, {"vb", vb}, {"n", n}, {"1", 1}, {"0", 0}, {"4", 4}};
         CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
@@ -1171,7 +1304,7 @@ int ccq_b200_energy(ccq_b200_ctx *c, double *e) {
     try {
         if (!c || !e) throw Error(CCQ_B200_EINVAL, "null argument");
         CK(cudaSetDevice(c->device));
-        run_ops(c, c->energy_op, c->plan.ops.size());
+        run_ops(c, c->energy_op, c->cc_end);
         CK(cudaMemcpyAsync(e, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         return 0;
@@ -1227,6 +1360,134 @@ int ccq_b200_iterate(ccq_b200_ctx *c, int64_t iter, double *e_cor, double *res, 
         if (e_cor) *e_cor = hs[0];
         if (res) *res = std::sqrt(std::sqrt(hs[1]));
         if (did_diis) *did_diis = diis;
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+// ---- CR-CC(2,3): left CCSD and the triples corrections ----------------------
+
+static void need_crcc(const ccq_b200_ctx *c) {
+    if (!c->has_crcc) throw Error(CCQ_B200_EINVAL, "context was not created with calc_type CR-CC(2,3)");
+}
+
+int ccq_b200_lambda_init(ccq_b200_ctx *c, double e_cor) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        need_crcc(c);
+        CK(cudaSetDevice(c->device));
+        CK(cudaMemcpy(c->bufs.at("ECOR").ptr, &e_cor, sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemsetAsync(c->lvec, 0, sizeof(double) * c->l_size, c->stream));
+        CK(cudaMemsetAsync(c->lring, 0, sizeof(double) * (size_t)(c->ds + 1) * c->l_size, c->stream));
+        run_ops(c, c->cc_end, c->lambda_op);
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_lambda_iterate(ccq_b200_ctx *c, int64_t iter, double *e_left, double *res, int64_t *did_diis) {
+    try {
+        if (!c || iter < 1) throw Error(CCQ_B200_EINVAL, "lambda_iterate: bad argument");
+        need_crcc(c);
+        CK(cudaSetDevice(c->device));
+        CK(cudaEventRecord(c->ev0, c->stream));
+        if (c->use_graph && !c->profile) {
+            if (!c->lgexec) {
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    run_ops(c, c->lambda_op, c->triples_op);
+                } catch (...) {
+                    cudaStreamEndCapture(c->stream, &g);
+                    throw;
+                }
+                CK(cudaStreamEndCapture(c->stream, &g));
+                CK(cudaGraphInstantiate(&c->lgexec, g, 0));
+                CK(cudaGraphDestroy(g));
+            }
+            CK(cudaGraphLaunch(c->lgexec, c->stream));
+        } else {
+            run_ops(c, c->lambda_op, c->triples_op);
+        }
+        CK(cudaEventRecord(c->ev1, c->stream));
+        // ring, residuum and DIIS on the lambda vector (jacobi_iter on l_vec, src/solve_cc.f90:175-269)
+        const int ds = c->ds;
+        const long long vs = c->l_size;
+        auto slot = [&](long long it) {
+            long long q = it % (ds + 1);
+            return q == 0 ? ds + 1 : q;
+        };
+        double *cur = c->lring + (slot(iter) - 1) * vs;
+        CK(cudaMemcpyAsync(cur, c->lvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
+        const double *prev = iter == 1 ? nullptr : c->lring + (slot(iter - 1) - 1) * vs;
+        launch_sqdiff(prev, cur, vs, c->scratch, c->stream);
+        const int diis = (iter % (ds + 1)) == 0;
+        if (diis) {
+            launch_diis_gram(c->lring, vs, ds, vs, c->scratch + 8, c->stream);
+            launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
+            launch_diis_extrap(c->lring, vs, ds, vs, c->scratch + 8 + 169, c->lvec, c->stream);
+        }
+        CK(cudaEventRecord(c->ev2, c->stream));
+        double hs[2];
+        int info = 0;
+        CK(cudaMemcpyAsync(&hs[0], c->bufs.at("EL").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(&hs[1], c->scratch, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (diis) CK(cudaMemcpyAsync(&info, c->dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->sweep_ms = ms;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev2));
+        c->iter_ms = ms;
+        if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
+        if (e_left) *e_left = hs[0];
+        if (res) *res = std::sqrt(std::sqrt(hs[1]));
+        if (did_diis) *did_diis = diis;
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_crcc23(ccq_b200_ctx *c, double *e) {
+    try {
+        if (!c || !e) throw Error(CCQ_B200_EINVAL, "null argument");
+        need_crcc(c);
+        CK(cudaSetDevice(c->device));
+        CK(cudaEventRecord(c->ev0, c->stream));
+        CK(cudaMemsetAsync(c->bufs.at("E23").ptr, 0, 4 * sizeof(double), c->stream));
+        run_ops(c, c->triples_op, c->plan.ops.size());
+        CK(cudaEventRecord(c->ev1, c->stream));
+        CK(cudaMemcpyAsync(e, c->bufs.at("E23").ptr, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->sweep_ms = ms;
+        return 0;
+    } catch (const Error &e2) {
+        return fail(e2);
+    } catch (const std::exception &e2) {
+        return fail(Error(CCQ_B200_EINVAL, e2.what()));
+    }
+}
+
+int ccq_b200_get_l(ccq_b200_ctx *c, double *l_vec, int64_t n) {
+    try {
+        if (!c || !l_vec) throw Error(CCQ_B200_EINVAL, "null argument");
+        need_crcc(c);
+        if (n != c->l_size) throw Error(CCQ_B200_EINVAL, "l_vec length must be the T1 + T2 size");
+        CK(cudaSetDevice(c->device));
+        CK(cudaMemcpyAsync(l_vec, c->lvec, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         return 0;
     } catch (const Error &e) {
         return fail(e);

@@ -92,6 +92,51 @@ def solve_cc(ctx, cfg, out=print, precision=None):
     return Result(e_cor=en_cor, iterations=it, failed=failed, history=hist)
 
 
+def solve_lcc(ctx, cfg, e_cor, out=print):
+    """solve_lcc (``src/solve_cc.f90:101-173``): jacobi_iter on lambda with the
+    left energy sqrt(sum LH^2) + E_cor and the same convergence rule."""
+    ctx.lambda_init(e_cor)
+    out('Left Coupled cluster')
+    out('--------------------')
+    conv = [1.0, 1.0, 1.0]
+    en = 0.0
+    failed = False
+    hist = []
+    prev = time.time()
+    print_iter_head(out)
+    it = 0
+    for it in range(1, cfg.max_iter + 1):
+        e_new, res, did = ctx.lambda_iterate(it)
+        diff = en - e_new
+        conv = [conv[1], conv[2], diff]
+        en = e_new
+        if did:
+            out('      DIIS cycle')
+        now = time.time()
+        print_iteration(out, it, e_new, diff, res, now - prev)
+        hist.append(dict(e=e_new, de=diff, res=res))
+        prev = now
+        if all(abs(c) < cfg.tol for c in conv):
+            break
+        if math.isnan(e_new):
+            out('FAILED TO CONVERGE')
+            failed = True
+            break
+        if it == cfg.max_iter:
+            out(f'FAILED TO CONVERGE IN {cfg.max_iter} ITERATIONS. KEEPING LAST T VECTOR.')
+            failed = True
+    return Result(e_left=en, iterations=it, failed=failed, history=hist)
+
+
+def print_cct3(out, e_ref, e_cor, e23):
+    """print_cct3 (``src/printing.F90:234-258``)."""
+    out(f"\n{'Method':>20}{'Correlation (Eh)':>18}{'Total Energy (Eh)':>18}")
+    out(' ' * 10 + '-' * 46)
+    out(f"{'CCSDt':>20}{e_cor:18.12f}{e_ref + e_cor:18.12f}")
+    for lab, x in zip(('CC(t;3),A', 'CC(t;3),B', 'CC(t;3),C', 'CC(t;3)'), e23):
+        out(f'{lab:>20}{e_cor + x:18.12f}{e_ref + e_cor + x:18.12f}')
+
+
 def load_system(cfg, base_dir='.'):
     def path(p):
         return p if os.path.isabs(p) else os.path.join(base_dir, p)
@@ -115,6 +160,14 @@ def run(input_path, out=print, base_dir='.'):
                       diis_space=cfg.diis_space)
     try:
         r = solve_cc(ctx, cfg, out)
+        if cfg.calc_type == 'CR-CC(2,3)':
+            # hbar2 + solve_lcc + crcc23 (src/calc_driver.f90:55-73)
+            r.left = solve_lcc(ctx, cfg, r.e_cor, out)
+            r.e23 = ctx.crcc23()
+            print_cct3(out, sysd['e_ref'], r.e_cor, r.e23)
+            r.e_ccsd = r.e_cor
+            r.e_cor = r.e_cor + r.e23[3]
+            r.failed = r.failed or r.left.failed
     finally:
         ctx.close()
     out('\nCalculation Summary (Eh)')

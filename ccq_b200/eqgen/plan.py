@@ -106,6 +106,13 @@ BLOCK_DIMS = {
     'T4C': ('oa', 'oa', 'ob', 'ob', 'va', 'va', 'vb', 'vb'), 'T4D': ('oa', 'ob', 'ob', 'ob', 'va', 'vb', 'vb', 'vb'),
     'T4E': ('ob',) * 4 + ('vb',) * 4,
 }
+# left (lambda) amplitudes share the layout of T1/T2; the triples moments M3x and
+# left projections L3x of CR-CC(2,3) that of T3x
+for _b in ('1A', '1B', '2A', '2B', '2C'):
+    BLOCK_DIMS['L' + _b] = BLOCK_DIMS['T' + _b]
+for _b in ('A', 'B', 'C', 'D'):
+    BLOCK_DIMS['M3' + _b] = BLOCK_DIMS['T3' + _b]
+    BLOCK_DIMS['L3' + _b] = BLOCK_DIMS['T3' + _b]
 
 
 def block_spins(name):
@@ -170,7 +177,7 @@ def map_factor(name, labels, spin, undressed=False):
     vs, sv = _stable_spin_sort(vl, spin)
     os_, so = _stable_spin_sort(ol, spin)
     nb = sum(spin[l] for l in vl)
-    block = f'T{n}' + 'ABCDE'[nb]
+    block = name[0].upper() + f'{n}' + 'ABCDE'[nb]   # t<n> -> T blocks, l<n> -> L blocks
     axes = [Axis(l, SIZE[('o', spin[l])]) for l in os_] + [Axis(l, SIZE[('v', spin[l])]) for l in vs]
     return sv * so, View(block, axes)
 
@@ -187,7 +194,7 @@ def antisym_groups(view):
         return []
     b = view.buf
     out = []
-    if b.startswith('T') and len(b) == 3:
+    if b[0] in 'TL' and len(b) == 3 and b[1].isdigit():
         n = int(b[1])
         spins = block_spins(b)
         for half in (0, n):
@@ -400,21 +407,29 @@ class PlanBuilder:
         return order
 
     # -- residual of one block -------------------------------------------------
-    def emit_block(self, block):
+    def emit_block(self, block, terms=None, undressed=False, mode='jacobi', defer=False):
+        """GETTs of one block's residual and its closing ASSEMBLE.
+
+        ``terms`` defaults to the CC residual of the block's level; ``defer``
+        leaves out the PHASE marker and returns the ASSEMBLE instead of
+        appending it (Jacobi updates that must follow every residual).
+        """
         level = int(block[1])
         spins_t = block_spins(block)
         ext_o = [f'i{k}' for k in range(level)]
         ext_v = [f'a{k}' for k in range(level)]
         tspin = {l: s for l, s in zip(ext_o, spins_t)}
         tspin.update({l: s for l, s in zip(ext_v, spins_t)})
-        terms = wick.residual_terms(level, self.tranks)
+        if terms is None:
+            terms = wick.residual_terms(level, self.tranks)
         groups = wick.orbit_groups(level, terms, workers=self.workers)
-        asm = Assemble(block, 'jacobi')
+        asm = Assemble(block, mode)
         block_start = len(self.ops)
         direct = {}
         direct_order = []
         zshare = {}
-        self.ops.append(Simple('PHASE', (block,)))
+        if not defer:
+            self.ops.append(Simple('PHASE', (block,)))
         for gi, (base, members) in enumerate(groups):
             bypat = {}
             for tau, c in members:
@@ -424,7 +439,7 @@ class PlanBuilder:
                 espin = dict(zip(ext_o + ext_v, pat))
                 if len(base) == 1:
                     name, ls = base[0]
-                    r = map_factor(name, ls, espin)
+                    r = map_factor(name, ls, espin, undressed)
                     if r is None:
                         continue
                     sign, v = r
@@ -443,12 +458,14 @@ class PlanBuilder:
                 if norm in zshare:
                     z, cref, state = zshare[norm]
                     scale = c0 / cref
-                    state[0] = self.emit_chain(base, espin, View(z, zaxes), scale, f'{block}.g{gi}', state[0])
+                    state[0] = self.emit_chain(base, espin, View(z, zaxes), scale, f'{block}.g{gi}', state[0],
+                                               undressed)
                 else:
                     nz, nx, nops = self.nz, self.nx, len(self.ops)
                     z = self.new_z([a.size for a in zaxes])
                     state = [0]
-                    state[0] = self.emit_chain(base, espin, View(z, zaxes), Fraction(1), f'{block}.g{gi}', 0)
+                    state[0] = self.emit_chain(base, espin, View(z, zaxes), Fraction(1), f'{block}.g{gi}', 0,
+                                               undressed)
                     if state[0] == 0:
                         # every spin term of this group vanishes: no buffer, no assemble terms
                         assert len(self.ops) == nops
@@ -464,6 +481,8 @@ class PlanBuilder:
             if c != 0:
                 asm.terms.append((c, v))
         self._restrict_block(block_start, asm)
+        if defer:
+            return asm
         self.ops.append(asm)
 
     def _op_groups(self, op, zl):
@@ -623,7 +642,7 @@ class PlanBuilder:
         self.buf('ONES', 'ones', (n,))
         self.buf('E', 'scalar', ())
         for b, d in BLOCK_DIMS.items():
-            if int(b[1]) <= max(3, self.nmax):
+            if b[0] == 'T' and int(b[1]) <= max(3, self.nmax):
                 self.buf(b, 'amp', d)
         order = ['T2A', 'T2C', 'T2B', 'T1A', 'T1B']
         if self.nmax >= 3:
@@ -643,6 +662,58 @@ class PlanBuilder:
         self.emit_energy()
         return self
 
+    def build_crcc(self):
+        """CCSD sweep followed by the CR-CC(2,3) phases (``src/calc_driver.f90:55-73``).
+
+        crcc     marker: ops before it form the CC sweep and energy
+        dress    T1 dressing at the converged CCSD amplitudes
+        CRDIAG   Hbar(CCSD) one- and two-body diagonals, three-body ``cal_d3`` sums
+        lambda   every left residual LH (bare f, v; T1, T2, L1, L2), then the
+                 Jacobi step of all five L blocks (``update_l2``): the residual
+                 of every block is taken from the old lambda
+        lenergy  sqrt(sum LH^2) + E_cor (``calculate_left_energy``)
+        triplesX moments M3X and left projections L3X of spin block X, then
+                 the four-denominator sums of ``crcc23`` into E23
+        """
+        from . import lagrange
+        assert self.method == 'CCSD'
+        self.build()
+        n = 'n'
+        for b in ('L1A', 'L1B', 'L2A', 'L2B', 'L2C'):
+            self.buf(b, 'lamp', BLOCK_DIMS[b])
+        for x in 'ABCD':
+            self.buf('M3' + x, 'tri', BLOCK_DIMS['M3' + x])
+            self.buf('L3' + x, 'tri', BLOCK_DIMS['L3' + x])
+        for b in ('HDA', 'HDB'):
+            self.buf(b, 'crd', (n,))
+        for b in ('H2AA', 'H2AB', 'H2BB'):
+            self.buf(b, 'crd', (n, n))
+        for b in ('W1A', 'W1B', 'W1C', 'W1D', 'W2A', 'W2B', 'W2C', 'W2D'):
+            self.buf(b, 'crd', (n, n, n))
+        for b in ('LN', 'EL', 'ECOR'):
+            self.buf(b, 'scalar', ())
+        self.buf('E23', 'scalar', ('4',))
+        self.ops.append(Simple('PHASE', ('crcc',)))
+        self.emit_dress()
+        self.ops.append(Simple('CRDIAG', ()))
+        self.ops.append(Simple('PHASE', ('lambda',)))
+        self.ops.append(Simple('ZERO', ('LN',)))
+        asms = []
+        for b in ('L1A', 'L1B', 'L2A', 'L2B', 'L2C'):
+            terms = lagrange.left_residual_terms(int(b[1]))
+            asms.append(self.emit_block(b, terms=terms, undressed=True, mode='ljacobi', defer=True))
+        self.ops += asms
+        self.ops.append(Simple('PHASE', ('lenergy',)))
+        self.ops.append(Simple('LENERGY', ()))
+        for x in 'ABCD':
+            self.ops.append(Simple('PHASE', ('triples' + x,)))
+            self.ops.append(self.emit_block('M3' + x, terms=lagrange.triples_moment_terms(), mode='copy',
+                                            defer=True))
+            self.ops.append(self.emit_block('L3' + x, terms=lagrange.triples_left_terms(), mode='copy',
+                                            defer=True))
+            self.ops.append(Simple('CRCC', (x,)))
+        return self
+
     def text(self):
         lines = [f'PLAN {self.method} rhf={int(self.rhf)}']
         for name, (kind, dims) in self.buffers.items():
@@ -658,6 +729,10 @@ class PlanBuilder:
 
 
 def build_plan(method, rhf=False, workers=None):
+    if method == 'CR-CC(2,3)':
+        b = PlanBuilder('CCSD', rhf, workers=workers).build_crcc()
+        b.method = 'CR-CC(2,3)'
+        return b
     return PlanBuilder(method, rhf, workers=workers).build()
 
 

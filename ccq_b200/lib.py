@@ -47,6 +47,10 @@ SIGNATURES = {
     'ccq_b200_update': (C.c_int, [C.c_void_p]),
     'ccq_b200_energy': (C.c_int, [C.c_void_p, DP]),
     'ccq_b200_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
+    'ccq_b200_lambda_init': (C.c_int, [C.c_void_p, C.c_double]),
+    'ccq_b200_lambda_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
+    'ccq_b200_crcc23': (C.c_int, [C.c_void_p, DP]),
+    'ccq_b200_get_l': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_set_precision': (C.c_int, [C.c_void_p, I64, I64]),
     'ccq_b200_use_graph': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), DP, DP]),
@@ -171,6 +175,25 @@ class Context:
         e, r, d = C.c_double(), C.c_double(), I64()
         _err(self._lib.ccq_b200_iterate(self.ptr, it, C.byref(e), C.byref(r), C.byref(d)))
         return e.value, r.value, bool(d.value)
+
+    # -- CR-CC(2,3) (contexts created with calc_type 'CR-CC(2,3)') ---------------
+    def lambda_init(self, e_cor):
+        _err(self._lib.ccq_b200_lambda_init(self.ptr, float(e_cor)))
+
+    def lambda_iterate(self, it):
+        e, r, d = C.c_double(), C.c_double(), I64()
+        _err(self._lib.ccq_b200_lambda_iterate(self.ptr, it, C.byref(e), C.byref(r), C.byref(d)))
+        return e.value, r.value, bool(d.value)
+
+    def crcc23(self):
+        e = np.zeros(4)
+        _err(self._lib.ccq_b200_crcc23(self.ptr, _p(e)))
+        return e
+
+    def get_l(self):
+        out = np.empty(self.vec_size)
+        _err(self._lib.ccq_b200_get_l(self.ptr, _p(out), out.size))
+        return out
 
     def set_precision(self, mode, nslices=4):
         _err(self._lib.ccq_b200_set_precision(self.ptr, mode, nslices))

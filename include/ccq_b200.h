@@ -137,6 +137,34 @@ int ccq_b200_energy(ccq_b200_ctx *ctx, double *e_cor);
 int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
                      double *residuum, int64_t *did_diis);
 
+/* ---- CR-CC(2,3) (calc_type "CR-CC(2,3)") -------------------------------------
+ * After the CCSD solve of a context created with calc_type "CR-CC(2,3)", the
+ * reference runs hbar2, solve_lcc and crcc23 (src/calc_driver.f90:55-73).
+ *
+ * ccq_b200_lambda_init replaces hbar2 (src/hbar.f90:10-720) and the setup of
+ * solve_lcc (src/solve_cc.f90:101-173): it dresses the Hamiltonian with the
+ * current T1, builds the Hbar(CCSD) diagonals used by the left Jacobi step and
+ * by crcc23, stores e_cor (the converged CCSD correlation energy, cc%en_cor) and
+ * zeroes lambda and its DIIS ring.  Lambda has the T1 + T2 layout of t_vec. */
+int ccq_b200_lambda_init(ccq_b200_ctx *ctx, double e_cor);
+
+/* One left-CCSD iteration: update_l2 (every LH from the old lambda, then the
+ * Jacobi step with h(a,a) - h(i,i) - E_cor + shift, src/update_lcc.f90:10-280),
+ * calculate_left_energy (sqrt(sum LH^2) + E_cor, src/energy.f90:103-136), the
+ * ring write, residuum and DIIS of jacobi_iter on l_vec (src/solve_cc.f90:175-269).
+ * Outputs as ccq_b200_iterate, with *e_left the left energy. */
+int ccq_b200_lambda_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_left,
+                            double *res, int64_t *did_diis);
+
+/* crcc23 (src/mm_correct.f90:11-344): e[0..3] = the triples corrections with
+ * denominators A (Fock), B (Hbar one-body), C (+ two-body), D (+ three-body),
+ * summed over the unique triples of the four spin blocks.  The reference adds
+ * e[3] to the correlation energy (src/mm_correct.f90:342). */
+int ccq_b200_crcc23(ccq_b200_ctx *ctx, double e[4]);
+
+/* Copies lambda (T1 + T2 layout, n = T1 + T2 size) to the host. */
+int ccq_b200_get_l(ccq_b200_ctx *ctx, double *l_vec, int64_t n);
+
 /* Precision of the bulk contractions; nslices = int8 slices per operand
  * (2..7) for CCQ_B200_PREC_SPLIT. */
 int ccq_b200_set_precision(ccq_b200_ctx *ctx, int64_t mode, int64_t nslices);

@@ -29,9 +29,15 @@ def test_defaults():
 
 
 def test_unknown_calc_type():
-    c = config.Config(calc_type='CR-CC(2,3)')
+    # active-space CCSDt stays on the reference's CPU program
+    c = config.Config(calc_type='CCSDt')
     with pytest.raises(ValueError):
         c.calc_macros()
+
+
+def test_crcc23_macros():
+    c = config.Config(calc_type='CR-CC(2,3)').calc_macros()
+    assert not c.lvl_t and not c.lvl_q
 
 
 def test_integral_round_trip(tmp_path):
