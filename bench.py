@@ -45,6 +45,7 @@ def parse():
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-converge', action='store_true')
     p.add_argument('--no-peaks', action='store_true', help='use MEASURED_PEAKS.json / fallback only')
+    p.add_argument('--no-crcc', action='store_true', help='skip the CR-CC(2,3) leg (32 orbitals)')
     return p.parse_args()
 
 
@@ -250,6 +251,80 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def golden(name):
+    p = os.path.join(ROOT, 'tests', 'golden', 'synthetic.json')
+    if not os.path.exists(p):
+        return None
+    return json.load(open(p)).get(name)
+
+
+def crcc_leg(cpu_sample=True):
+    """CR-CC(2,3) on the 32-orbital system (nel=14, nvir=50, L=64, sigma=0.03, seed=1).
+
+    The whole calculation of ``calc_type=CR-CC(2,3)``: CCSD to tol 1e-10, the
+    left CCSD solve to the same tol, and the four corrections; device times per
+    phase (CUDA events on the library's stream) and the wall time of the
+    complete call sequence.  The CPU sample times one CCSD iteration, one left
+    iteration and the corrections with the numpy executor of the same plan.
+    """
+    from ccq_b200 import config, driver, lib, synth
+    s = synth.system(synth.C1)
+    d = s['dims']
+    cfg = config.Config(calc_type='CR-CC(2,3)', tol=1e-10, diis_space=5, max_iter=200).calc_macros()
+    t0 = time.perf_counter()
+    ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CR-CC(2,3)', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                      s['v_bb'], diis_space=5)
+    ctx.use_graph(True)
+    r = driver.solve_cc(ctx, cfg, out=lambda x: None)
+    cc_ms = sum(h['ms'] for h in r.history)
+    ctx.lambda_init(r.e_cor)
+    lms, en, conv, itl = [], 0.0, [1.0, 1.0, 1.0], 0
+    for itl in range(1, cfg.max_iter + 1):
+        e_new, res, did = ctx.lambda_iterate(itl)
+        lms.append(ctx.timing()[1])
+        conv = [conv[1], conv[2], en - e_new]
+        en = e_new
+        if all(abs(c) < cfg.tol for c in conv):
+            break
+    e23 = ctx.crcc23()
+    tri_ms = ctx.timing()[0]
+    wall = time.perf_counter() - t0
+    lstat = ctx.stats()
+    ctx.close()
+    g = golden('c1_crcc23')
+    out = {'workload': 'CR-CC(2,3), 32 spatial orbitals, nel=14, nvir=50, L=64, sigma=0.03, seed=1, UHF spin blocks',
+           'wall_s': wall, 'ccsd_iterations': r.iterations, 'ccsd_device_ms': cc_ms,
+           'left_iterations': itl, 'left_device_ms': float(sum(lms)), 'left_ms_per_iter': float(np.mean(lms)),
+           'triples_device_ms': tri_ms, 'e_ccsd': r.e_cor, 'e23': [float(x) for x in e23],
+           'dE23_vs_oracle': ([abs(a - b) for a, b in zip(e23, g['e23'])] if g else None),
+           'dE_ccsd_vs_oracle': (abs(r.e_cor - g['e_cor']) if g else None),
+           'iterations_match_oracle': ((r.iterations, itl) == (g['iterations'], g['left_iterations']) if g else None),
+           'oracle': 'tests/golden/synthetic.json c1_crcc23 (numpy executor of the same plan)' if g else None}
+    if cpu_sample:
+        from oracle.blockcc import BlockCRCC
+        text = open(os.path.join(ROOT, 'ccq_b200', 'plans', 'CRCC23.plan')).read()
+        bc = BlockCRCC(text, s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d)
+        tvec = np.zeros(bc.layout.t_size)
+        t1 = time.perf_counter()
+        bc.update(tvec)
+        bc.energy(tvec)
+        t_cc = time.perf_counter() - t1
+        bc.lambda_init(tvec, -0.1)
+        t1 = time.perf_counter()
+        bc.lambda_update(bc.lvec, tvec)
+        bc.lambda_energy(bc.lvec, tvec)
+        t_l = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        bc.crcc23(tvec)
+        t_t = time.perf_counter() - t1
+        est = t_cc * r.iterations + t_l * itl + t_t
+        out['cpu_baseline'] = {'value': est, 'unit': 's per CR-CC(2,3) calculation (estimated)', 'cores': os.cpu_count(),
+                               'kind': 'port', 'sample': f'one CCSD iteration ({t_cc:.2f} s), one left iteration '
+                               f'({t_l:.2f} s) and the corrections ({t_t:.2f} s) with the numpy executor, scaled by '
+                               f'the GPU run\'s iteration counts'}
+    return out
+
+
 def time_leg(ctx, it0, steps, world):
     """Run `steps` iterations; returns (device ms list, energies)."""
     import torch
@@ -397,6 +472,10 @@ def main():
                 'oracle': 'tests/golden/synthetic.json c2_ccsdt' if g else 'fixture missing',
                 'split_iterations': sum(1 for h in r.history if h['split'])}
 
+    crcc = None
+    if rank == 0 and not args.no_crcc:
+        crcc = crcc_leg(cpu_sample=(world == 1 and not args.no_cpu_baseline))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference(s, 1, 0, budget_s=60.0)
@@ -420,7 +499,7 @@ def main():
             'e2e': {'value': e2e_s, 'unit': 's/iter', 'h2d_bytes_per_step': bytes_t,
                     'd2h_bytes_per_step': bytes_t + 16},
             'gpu_launches': head['launches_per_iter'] * args.steps,
-            'clocks': clk, 'convergence': conv,
+            'clocks': clk, 'convergence': conv, 'crcc23': crcc,
             'peaks': {'live': peaks_live, 'file': peaks_file, 'file_kind': peaks_kind},
         }
         print(json.dumps(line), flush=True)

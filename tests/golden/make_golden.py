@@ -1,6 +1,6 @@
 """Converged FP64 oracle energies for the synthetic workloads (writes synthetic.json).
 
-    python tests/golden/make_golden.py [--c2]
+    python tests/golden/make_golden.py [--c2] [--force]
 
 The oracle is the numpy executor of the contraction plan (oracle/blockcc.py),
 itself pinned against the determinant-space residuals and the H4 known answers.
@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 from ccq_b200 import synth  # noqa: E402
-from oracle.blockcc import BlockCC  # noqa: E402
+from oracle.blockcc import BlockCC, BlockCRCC  # noqa: E402
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'synthetic.json')
 
@@ -25,6 +25,28 @@ CASES = {
     'small_ccsdtq': (synth.SynthSpec(8, 4, 16, 0.05, 9), 'CCSDTQ', False),
 }
 C2_CASES = {'c2_ccsdt': (synth.C2, 'CCSDT', True)}
+CRCC_CASES = {
+    'small_crcc23': (synth.SynthSpec(12, 8, 24, 0.05, 11), False),
+    'c1_crcc23': (synth.C1, False),
+}
+
+
+def run_crcc(name, spec, rhf, tol=1e-10):
+    """CCSD, left CCSD and the four CR-CC(2,3) corrections with the plan's numpy executor."""
+    s = synth.system(spec)
+    plan = os.path.join(ROOT, 'ccq_b200', 'plans', 'CRCC23' + ('_rhf' if rhf else '') + '.plan')
+    t0 = time.time()
+    bc = BlockCRCC(open(plan).read(), s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], s['dims'])
+    e, it, failed, hist, tvec = bc.solve(tol=tol, max_iter=200)
+    assert not failed
+    el, itl, fl, hl = bc.solve_left(tvec, e, tol=tol, max_iter=200)
+    assert not fl
+    e23 = bc.crcc23(tvec)
+    d = s['dims']
+    return dict(spec=spec.__dict__, method='CR-CC(2,3)', rhf=rhf, occ_a=d.occ_a, occ_b=d.occ_b, e_cor=e,
+                e_ref=s['e_ref'], iterations=it, tol=tol, left_iterations=itl, e_left=el,
+                e23=[float(x) for x in e23], seconds=time.time() - t0,
+                history=[h[0] for h in hist], left_history=[h[0] for h in hl])
 
 
 def run(name, spec, method, rhf, tol=1e-10):
@@ -58,6 +80,13 @@ def main():
             continue
         data[name] = run(name, spec, method, rhf)
         print(name, data[name]['e_cor'], data[name]['iterations'], f"{data[name]['seconds']:.1f}s", flush=True)
+        json.dump(data, open(OUT, 'w'), indent=1)
+    for name, (spec, rhf) in CRCC_CASES.items():
+        if name in data and '--force' not in sys.argv:
+            continue
+        data[name] = run_crcc(name, spec, rhf)
+        print(name, data[name]['e_cor'], data[name]['e23'], data[name]['iterations'], data[name]['left_iterations'],
+              f"{data[name]['seconds']:.1f}s", flush=True)
         json.dump(data, open(OUT, 'w'), indent=1)
 
 

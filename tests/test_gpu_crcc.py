@@ -55,6 +55,28 @@ def test_crcc23_matches_plan_executor(norb, nel, rhf):
         ctx.close()
 
 
+def test_crcc23_matches_oracle_fixture():
+    """12 orbitals (nel=8): iteration counts and the four corrections of tests/golden/synthetic.json."""
+    import json
+    from ccq_b200 import config, driver, lib, synth
+    g = json.load(open(os.path.join(ROOT, 'tests', 'golden', 'synthetic.json')))['small_crcc23']
+    spec = synth.SynthSpec(**g['spec'])
+    s = synth.system(spec)
+    d = s['dims']
+    ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CR-CC(2,3)', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                      s['v_bb'])
+    try:
+        cfg = config.Config(calc_type='CR-CC(2,3)', tol=g['tol'], max_iter=200).calc_macros()
+        r = driver.solve_cc(ctx, cfg, out=lambda x: None)
+        left = driver.solve_lcc(ctx, cfg, r.e_cor, out=lambda x: None)
+        e23 = ctx.crcc23()
+    finally:
+        ctx.close()
+    assert r.iterations == g['iterations'] and left.iterations == g['left_iterations']
+    assert abs(r.e_cor - g['e_cor']) < 1e-10
+    np.testing.assert_allclose(e23, g['e23'], rtol=1e-7, atol=0)
+
+
 def test_crcc23_repeatable_and_graph_free_agree():
     """The left iterations replayed from a CUDA graph and launched one by one agree."""
     from ccq_b200 import driver
