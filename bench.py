@@ -46,6 +46,9 @@ def parse():
     p.add_argument('--no-converge', action='store_true')
     p.add_argument('--no-peaks', action='store_true', help='use MEASURED_PEAKS.json / fallback only')
     p.add_argument('--no-crcc', action='store_true', help='skip the CR-CC(2,3) leg (32 orbitals)')
+    p.add_argument('--no-batch', action='store_true', help='skip the batched CCSD leg (64 Hamiltonians)')
+    p.add_argument('--warmstart', action='store_true',
+                   help='add the learned warm-start study (200 CCSDT Hamiltonians, about two minutes)')
     return p.parse_args()
 
 
@@ -325,6 +328,43 @@ def crcc_leg(cpu_sample=True):
     return out
 
 
+def batch_leg(rank, world):
+    """64 CCSD Hamiltonians of 16-48 spatial orbitals to tol 1e-8 (ccq_b200.batch.c3_specs).
+
+    Instances are sharded over the ranks (no collective on the data path; a host
+    gather of the results).  solves/s = 64 / the slowest rank's wall time of the
+    iterations; context creation (integral upload, plan instantiation) is
+    reported beside it.
+    """
+    from ccq_b200 import batch
+
+    def gather(obj):
+        if world == 1:
+            return [obj]
+        import torch.distributed as dist
+        objs = [None] * world
+        dist.all_gather_object(objs, obj)
+        return objs
+    specs = batch.c3_specs()
+    barrier(world)
+    res, tims = batch.solve_sharded(specs, rank, world, gather, tol=1e-8)
+    solve_s = max(t['solve_s'] for t in tims)
+    setup_s = max(t['setup_s'] for t in tims)
+    g = golden('c3_batched_ccsd')
+    de = it_ok = None
+    if g:
+        de = max(abs(r['e_cor'] - x['e_cor']) for r, x in zip(res, g['instances']))
+        it_ok = sum(r['iterations'] == x['iterations'] for r, x in zip(res, g['instances']))
+    return {'workload': '64 x CCSD, norb ~ U{16..48} (seed 1000+i), nel = 2 floor(norb/5), L = 2 norb, sigma 0.03, '
+                        'tol 1e-8', 'solves_per_s': len(specs) / solve_s, 'solve_wall_s': solve_s,
+            'setup_wall_s': setup_s, 'e2e_solves_per_s': len(specs) / (solve_s + setup_s),
+            'failed': sum(r['failed'] for r in res), 'iterations_total': sum(r['iterations'] for r in res),
+            'device_ms_sum': sum(r['device_ms'] for r in res),
+            'max_dE_vs_oracle': de, 'iterations_match_oracle': it_ok,
+            'oracle': 'tests/golden/synthetic.json c3_batched_ccsd (numpy executor, each instance alone)' if g else None,
+            'cpu_oracle_seconds': g['seconds'] if g else None}
+
+
 def time_leg(ctx, it0, steps, world):
     """Run `steps` iterations; returns (device ms list, energies)."""
     import torch
@@ -472,6 +512,14 @@ def main():
                 'oracle': 'tests/golden/synthetic.json c2_ccsdt' if g else 'fixture missing',
                 'split_iterations': sum(1 for h in r.history if h['split'])}
 
+    batched = None if args.no_batch else batch_leg(rank, world)
+
+    warm = None
+    if rank == 0 and args.warmstart:
+        from ccq_b200 import warmstart
+        warm = warmstart.study('CCSDT', 24, 10)
+        warm.pop('loss_history', None)
+
     crcc = None
     if rank == 0 and not args.no_crcc:
         crcc = crcc_leg(cpu_sample=(world == 1 and not args.no_cpu_baseline))
@@ -499,7 +547,7 @@ def main():
             'e2e': {'value': e2e_s, 'unit': 's/iter', 'h2d_bytes_per_step': bytes_t,
                     'd2h_bytes_per_step': bytes_t + 16},
             'gpu_launches': head['launches_per_iter'] * args.steps,
-            'clocks': clk, 'convergence': conv, 'crcc23': crcc,
+            'clocks': clk, 'convergence': conv, 'crcc23': crcc, 'batched_ccsd': batched, 'warm_start': warm,
             'peaks': {'live': peaks_live, 'file': peaks_file, 'file_kind': peaks_kind},
         }
         print(json.dumps(line), flush=True)

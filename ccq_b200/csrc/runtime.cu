@@ -270,6 +270,9 @@ struct ccq_b200_ctx {
     long long l_size = 0;
     CrDiagArgs crd{};
     cudaGraphExec_t lgexec = nullptr;
+    long long t_dev = 0;        // t_vec elements resident on the device (T1+T2 for CCSD-level methods)
+    double *hpin = nullptr;     // pinned host slots for an iteration's results (E, residuum, DIIS info)
+    int64_t async_iter = 0;     // iteration launched by iterate_async, 0 when none is pending
     double flops = 0.0;
     long long launches = 0;
     double sweep_ms = 0.0;
@@ -290,6 +293,7 @@ struct ccq_b200_ctx {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (lgexec) cudaGraphExecDestroy(lgexec);
         split_free(split);
+        if (hpin) cudaFreeHost(hpin);
         for (void *p : owned) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -426,8 +430,11 @@ void instantiate(ccq_b200_ctx *c) {
             CK(cudaMemsetAsync(c->lvec, 0, sizeof(double) * lo, c->stream));
         }
     }
-    c->tvec = (double *)c->dalloc(sizeof(double) * c->t_size);
-    CK(cudaMemsetAsync(c->tvec, 0, sizeof(double) * c->t_size, c->stream));
+    // CCSD-level methods never touch the T3 slots of t_vec: they stay on the host side of the
+    // boundary (zeros in get_t), and only T1 + T2 are resident
+    c->t_dev = (c->calc_type == "CCSD" || c->calc_type == "CR-CC(2,3)") ? tv_off["T3A"] : c->t_size;
+    c->tvec = (double *)c->dalloc(sizeof(double) * c->t_dev);
+    CK(cudaMemsetAsync(c->tvec, 0, sizeof(double) * c->t_dev, c->stream));
 
     // work buffers: one arena, each phase packs its Z/X buffers from offset 0
     std::map<std::string, std::string> first_phase;
@@ -494,7 +501,7 @@ void instantiate(ccq_b200_ctx *c) {
         for (auto s : d.shape) d.numel *= s;
         d.groups = b.groups;
         if (tv_off.count(b.name)) {
-            d.ptr = c->tvec + tv_off[b.name];
+            d.ptr = tv_off[b.name] < c->t_dev ? c->tvec + tv_off[b.name] : nullptr;
         } else if (lv_off.count(b.name)) {
             d.ptr = c->lvec + lv_off[b.name];
         } else if (b.kind == "work") {
@@ -1169,6 +1176,7 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         c->froz = fr;
         c->size = {{"oa", oa}, {"ob", ob}, {"va", va}, {"vb", vb}, {"n", n}, {"1", 1}, {"0", 0}, {"4", 4}};
         CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        CK(cudaMallocHost(&c->hpin, 4 * sizeof(double)));
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
         CK(cudaEventCreate(&c->ev2));
@@ -1243,7 +1251,7 @@ int ccq_b200_sizes(const ccq_b200_ctx *c, int64_t *t_size, int64_t *vec_size) {
 int ccq_b200_set_t(ccq_b200_ctx *c, const double *t, int64_t n) {
     try {
         if (!c || !t || n != c->t_size) throw Error(CCQ_B200_EINVAL, "set_t: size must equal t_size");
-        CK(cudaMemcpyAsync(c->tvec, t, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->tvec, t, sizeof(double) * c->t_dev, cudaMemcpyHostToDevice, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         return 0;
     } catch (const Error &e) {
@@ -1256,7 +1264,8 @@ int ccq_b200_set_t(ccq_b200_ctx *c, const double *t, int64_t n) {
 int ccq_b200_get_t(const ccq_b200_ctx *c, double *t, int64_t n) {
     try {
         if (!c || !t || n != c->t_size) throw Error(CCQ_B200_EINVAL, "get_t: size must equal t_size");
-        CK(cudaMemcpyAsync(t, c->tvec, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(t, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost, c->stream));
+        if (c->t_dev < n) std::fill(t + c->t_dev, t + n, 0.0);
         CK(cudaStreamSynchronize(c->stream));
         return 0;
     } catch (const Error &e) {
@@ -1274,6 +1283,7 @@ int ccq_b200_block(ccq_b200_ctx *c, const char *name, double *host, int64_t n, i
         auto it = c->bufs.find(nm);
         if (it == c->bufs.end()) throw Error(CCQ_B200_EINVAL, "block: unknown block " + nm);
         if (n != it->second.numel) throw Error(CCQ_B200_EINVAL, "block: size mismatch");
+        if (!it->second.ptr) throw Error(CCQ_B200_EINVAL, "block: " + nm + " is not resident for " + c->calc_type);
         CK(cudaMemcpyAsync(to_device ? (void *)it->second.ptr : (void *)host,
                            to_device ? (const void *)host : (const void *)it->second.ptr, sizeof(double) * n,
                            to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, c->stream));
@@ -1315,51 +1325,95 @@ int ccq_b200_energy(ccq_b200_ctx *c, double *e) {
     }
 }
 
+// One jacobi_iter step split in two: the launch enqueues the sweep, the ring
+// write, the residuum and (on schedule) DIIS, and copies the results to pinned
+// host slots; the finish waits for them.  Many contexts on their own streams
+// can be launched before any is waited for.
+static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
+    CK(cudaSetDevice(c->device));
+    c->launches = 0;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    sweep(c);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    c->launches = count_sweep_launches(c);
+    const int ds = c->ds;
+    const long long vs = c->vec_size;
+    auto slot = [&](long long it) {
+        long long q = it % (ds + 1);
+        return q == 0 ? ds + 1 : q;
+    };
+    double *cur = c->ring + (slot(iter) - 1) * vs;
+    CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
+    const double *prev = iter == 1 ? nullptr : c->ring + (slot(iter - 1) - 1) * vs;
+    launch_sqdiff(prev, cur, vs, c->scratch, c->stream);
+    c->launches += 1;
+    const int diis = (iter % (ds + 1)) == 0;
+    if (diis) {
+        launch_diis_gram(c->ring, vs, ds, vs, c->scratch + 8, c->stream);
+        launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
+        launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
+        c->launches += 3;
+    }
+    CK(cudaEventRecord(c->ev2, c->stream));
+    CK(cudaMemcpyAsync(c->hpin, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->hpin + 1, c->scratch, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->hpin[2] = 0.0;
+    if (diis) CK(cudaMemcpyAsync(c->hpin + 2, c->dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    c->async_iter = iter;
+}
+
+static void iterate_finish(ccq_b200_ctx *c, double *e_cor, double *res, int64_t *did_diis) {
+    const int64_t iter = c->async_iter;
+    if (iter < 1) throw Error(CCQ_B200_EINVAL, "iterate_wait: no iteration was launched");
+    c->async_iter = 0;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->sweep_ms = ms;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev2));
+    c->iter_ms = ms;
+    const int diis = (iter % (c->ds + 1)) == 0;
+    int info = 0;
+    memcpy(&info, c->hpin + 2, sizeof(int));
+    if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
+    if (c->precision == CCQ_B200_PREC_SPLIT && split_error(c->split))
+        throw Error(CCQ_B200_ECUDA, "split GETT pipeline wait expired");
+    if (e_cor) *e_cor = c->hpin[0];
+    if (res) *res = std::sqrt(std::sqrt(c->hpin[1]));
+    if (did_diis) *did_diis = diis;
+}
+
 int ccq_b200_iterate(ccq_b200_ctx *c, int64_t iter, double *e_cor, double *res, int64_t *did_diis) {
     try {
         if (!c || iter < 1) throw Error(CCQ_B200_EINVAL, "iterate: bad argument");
-        CK(cudaSetDevice(c->device));
-        c->launches = 0;
-        CK(cudaEventRecord(c->ev0, c->stream));
-        sweep(c);
-        CK(cudaEventRecord(c->ev1, c->stream));
-        c->launches = count_sweep_launches(c);
-        int ds = c->ds;
-        long long vs = c->vec_size;
-        auto slot = [&](long long it) {
-            long long s = it % (ds + 1);
-            return s == 0 ? ds + 1 : s;
-        };
-        double *cur = c->ring + (slot(iter) - 1) * vs;
-        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
-        const double *prev = iter == 1 ? nullptr : c->ring + (slot(iter - 1) - 1) * vs;
-        launch_sqdiff(prev, cur, vs, c->scratch, c->stream);
-        c->launches += 1;
-        int diis = (iter % (ds + 1)) == 0;
-        if (diis) {
-            launch_diis_gram(c->ring, vs, ds, vs, c->scratch + 8, c->stream);
-            launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
-            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
-            c->launches += 3;
-        }
-        CK(cudaEventRecord(c->ev2, c->stream));
-        double hs[2];
-        int info = 0;
-        CK(cudaMemcpyAsync(&hs[0], c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(&hs[1], c->scratch, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        if (diis) CK(cudaMemcpyAsync(&info, c->dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-        c->sweep_ms = ms;
-        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev2));
-        c->iter_ms = ms;
-        if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
-        if (c->precision == CCQ_B200_PREC_SPLIT && split_error(c->split))
-            throw Error(CCQ_B200_ECUDA, "split GETT pipeline wait expired");
-        if (e_cor) *e_cor = hs[0];
-        if (res) *res = std::sqrt(std::sqrt(hs[1]));
-        if (did_diis) *did_diis = diis;
+        iterate_launch(c, iter);
+        iterate_finish(c, e_cor, res, did_diis);
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_iterate_async(ccq_b200_ctx *c, int64_t iter) {
+    try {
+        if (!c || iter < 1) throw Error(CCQ_B200_EINVAL, "iterate_async: bad argument");
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "iterate_async: the previous iteration was not waited for");
+        iterate_launch(c, iter);
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_iterate_wait(ccq_b200_ctx *c, double *e_cor, double *res, int64_t *did_diis) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        iterate_finish(c, e_cor, res, did_diis);
         return 0;
     } catch (const Error &e) {
         return fail(e);

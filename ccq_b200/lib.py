@@ -47,6 +47,8 @@ SIGNATURES = {
     'ccq_b200_update': (C.c_int, [C.c_void_p]),
     'ccq_b200_energy': (C.c_int, [C.c_void_p, DP]),
     'ccq_b200_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
+    'ccq_b200_iterate_async': (C.c_int, [C.c_void_p, I64]),
+    'ccq_b200_iterate_wait': (C.c_int, [C.c_void_p, DP, DP, C.POINTER(I64)]),
     'ccq_b200_lambda_init': (C.c_int, [C.c_void_p, C.c_double]),
     'ccq_b200_lambda_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
     'ccq_b200_crcc23': (C.c_int, [C.c_void_p, DP]),
@@ -174,6 +176,14 @@ class Context:
     def iterate(self, it):
         e, r, d = C.c_double(), C.c_double(), I64()
         _err(self._lib.ccq_b200_iterate(self.ptr, it, C.byref(e), C.byref(r), C.byref(d)))
+        return e.value, r.value, bool(d.value)
+
+    def iterate_async(self, it):
+        _err(self._lib.ccq_b200_iterate_async(self.ptr, it))
+
+    def iterate_wait(self):
+        e, r, d = C.c_double(), C.c_double(), I64()
+        _err(self._lib.ccq_b200_iterate_wait(self.ptr, C.byref(e), C.byref(r), C.byref(d)))
         return e.value, r.value, bool(d.value)
 
     # -- CR-CC(2,3) (contexts created with calc_type 'CR-CC(2,3)') ---------------

@@ -3,6 +3,7 @@
     python -m ccq_b200.probe egemm K1 K2 K3 [repeats]
     python -m ccq_b200.probe egemm_split K1 K2 K3 [slices]
     python -m ccq_b200.probe sweep fp64|split OUTFILE [warm-up iterations]
+    python -m ccq_b200.probe warmstart CCSDT|CCSDTQ NORB NEL [COUNT TRAIN EPOCHS]
 
 Runs ccq_b200_egemm (the FP64 GETT kernel) on random column-major operands;
 the vvvv ladder of the CCSDT T3 update at 40 orbitals is (1024, 16384, 1024).
@@ -63,6 +64,16 @@ def main(argv):
         ctx.iterate(warm + 1)
         print(ctx.profile_get())
         ctx.close()
+    elif kind == 'warmstart':
+        # the learned warm start on a lambda-swept family: METHOD NORB NEL [COUNT TRAIN EPOCHS]
+        import json
+        from ccq_b200 import warmstart
+        method, norb, nel = argv[1], int(argv[2]), int(argv[3])
+        count = int(argv[4]) if len(argv) > 4 else 200
+        train = int(argv[5]) if len(argv) > 5 else 150
+        epochs = int(argv[6]) if len(argv) > 6 else 600
+        r = warmstart.study(method, norb, nel, count, train, epochs=epochs, log=print)
+        print(json.dumps(r))
     else:
         raise SystemExit(f'unknown probe {kind}')
 

@@ -137,6 +137,32 @@ int ccq_b200_energy(ccq_b200_ctx *ctx, double *e_cor);
 int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
                      double *residuum, int64_t *did_diis);
 
+/* ccq_b200_iterate in two halves, for many independent solves at once (one
+ * context per Hamiltonian, each on its own stream): _async enqueues the
+ * iteration and returns; _wait blocks until it is done and returns its
+ * outputs.  A context takes one pending iteration at a time. */
+int ccq_b200_iterate_async(ccq_b200_ctx *ctx, int64_t iter);
+int ccq_b200_iterate_wait(ccq_b200_ctx *ctx, double *e_cor, double *residuum, int64_t *did_diis);
+
+/* ---- learned warm start ---------------------------------------------------------
+ * A per-amplitude multilayer perceptron (no counterpart in the reference, which
+ * starts every solve from T = 0): y = w3 . tanh(W2 tanh(W1 x + b1) + b2) + b3 with
+ * x in R^nfeat (nfeat <= CCQ_B200_MLP_MAXF) and CCQ_B200_MLP_HIDDEN hidden units, FP32.
+ * Parameters are one array: W1[H][F] | b1[H] | W2[H][H] | b2[H] | w3[H] | b3.
+ * All pointers are device pointers; stream may be NULL (the legacy stream).
+ * _params returns the number of parameters for nfeat (or a negative error). */
+#define CCQ_B200_MLP_HIDDEN 32
+#define CCQ_B200_MLP_MAXF 8
+int ccq_b200_mlp_params(int64_t nfeat);
+/* y[n] = network(x[n][nfeat]) */
+int ccq_b200_mlp_forward(const float *params, int64_t nfeat, const float *x, int64_t n, float *y, void *stream);
+/* grad[nparams] = d/dparams of (1/n) sum (y - target)^2, *loss = that mean (both overwritten) */
+int ccq_b200_mlp_grad(const float *params, int64_t nfeat, const float *x, const float *target, int64_t n,
+                      float *grad, float *loss, void *stream);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected; step counts from 1) */
+int ccq_b200_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t nparams, double lr,
+                      int64_t step, void *stream);
+
 /* ---- CR-CC(2,3) (calc_type "CR-CC(2,3)") -------------------------------------
  * After the CCSD solve of a context created with calc_type "CR-CC(2,3)", the
  * reference runs hbar2, solve_lcc and crcc23 (src/calc_driver.f90:55-73).

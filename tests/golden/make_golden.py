@@ -70,6 +70,21 @@ def run(name, spec, method, rhf, tol=1e-10):
                 history=[h[0] for h in hist])
 
 
+def run_c3(tol=1e-8):
+    """The 64 batched CCSD instances (ccq_b200.batch.c3_specs), each solved on its own."""
+    from ccq_b200 import batch
+    out = []
+    t0 = time.time()
+    plan = open(os.path.join(ROOT, 'ccq_b200', 'plans', 'CCSD.plan')).read()
+    for spec in batch.c3_specs():
+        s = synth.system(spec)
+        bc = BlockCC(plan, s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], s['dims'], 'CCSD')
+        e, it, failed, hist, _ = bc.solve(tol=tol, max_iter=200)
+        assert not failed
+        out.append(dict(spec=spec.__dict__, e_cor=e, iterations=it))
+    return dict(method='CCSD', tol=tol, instances=out, seconds=time.time() - t0)
+
+
 def main():
     data = json.load(open(OUT)) if os.path.exists(OUT) else {}
     cases = dict(CASES)
@@ -80,6 +95,10 @@ def main():
             continue
         data[name] = run(name, spec, method, rhf)
         print(name, data[name]['e_cor'], data[name]['iterations'], f"{data[name]['seconds']:.1f}s", flush=True)
+        json.dump(data, open(OUT, 'w'), indent=1)
+    if 'c3_batched_ccsd' not in data or '--force' in sys.argv:
+        data['c3_batched_ccsd'] = run_c3()
+        print('c3_batched_ccsd', f"{data['c3_batched_ccsd']['seconds']:.1f}s", flush=True)
         json.dump(data, open(OUT, 'w'), indent=1)
     for name, (spec, rhf) in CRCC_CASES.items():
         if name in data and '--force' not in sys.argv:
