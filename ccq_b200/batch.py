@@ -90,6 +90,25 @@ class Instance:
         self.ctx.close()
 
 
+def create_instances(specs, calc_type='CCSD', diis_space=5, graph=True, threads=None):
+    """One context per spec, created by a pool of host threads (integral generation,
+    plan instantiation and upload of different instances overlap) on the calling
+    thread's CUDA device."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    import torch
+    dev = torch.cuda.current_device()
+
+    def make(sp):
+        torch.cuda.set_device(dev)
+        return Instance(sp, calc_type, diis_space, graph)
+    n = threads or min(16, os.cpu_count() or 1, max(1, len(specs)))
+    if n <= 1 or len(specs) <= 1:
+        return [make(sp) for sp in specs]
+    with ThreadPoolExecutor(max_workers=n) as ex:
+        return list(ex.map(make, specs))
+
+
 def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, graph=True, t_init=None,
                 keep_t=False):
     """Solve every instance; returns (results, timings).
@@ -100,7 +119,7 @@ def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, g
     of the iterations.
     """
     t0 = time.perf_counter()
-    insts = [Instance(sp, calc_type, diis_space, graph) for sp in specs]
+    insts = create_instances(specs, calc_type, diis_space, graph)
     if t_init is not None:
         for x, t in zip(insts, t_init):
             if t is not None:

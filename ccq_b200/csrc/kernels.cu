@@ -878,6 +878,25 @@ void launch_assemble(const AsmArgs &a, cudaStream_t s) {
     }
 }
 
+// out[p][q][r][s] = f[p + n (q + n (r + n s))]: column-major (Fortran) n^4 array to
+// C order; writes coalesce, reads gather
+__global__ void f2c4_kernel(const double *__restrict__ f, double *__restrict__ out, long long n) {
+    const long long total = n * n * n * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long s = i % n, r = (i / n) % n, q = (i / (n * n)) % n, p = i / (n * n * n);
+        out[i] = __ldg(f + p + n * (q + n * (r + n * s)));
+    }
+}
+
+void launch_f2c4(const double *f, double *out, long long n, cudaStream_t s) {
+    const long long total = n * n * n * n;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (blocks < 1) blocks = 1;
+    f2c4_kernel<<<(int)blocks, 256, 0, s>>>(f, out, n);
+}
+
 __global__ void fill_kernel(double *p, double v, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         p[i] = v;

@@ -104,6 +104,7 @@ void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t
 void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N, cudaStream_t s);
 void launch_assemble(const AsmArgs &a, cudaStream_t s);
 void launch_fill(double *p, double v, long long n, cudaStream_t s);
+void launch_f2c4(const double *f, double *out, long long n, cudaStream_t s);
 void launch_sqdiff(const double *a, const double *b, long long n, double *out, cudaStream_t s);
 void launch_diis_gram(const double *ring, long long stride, int ds, long long n, double *gram, cudaStream_t s);
 void launch_diis_solve(double *gram, int ds, double *coef, int *info, cudaStream_t s);

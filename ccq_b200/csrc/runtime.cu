@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -271,6 +272,8 @@ struct ccq_b200_ctx {
     CrDiagArgs crd{};
     cudaGraphExec_t lgexec = nullptr;
     long long t_dev = 0;        // t_vec elements resident on the device (T1+T2 for CCSD-level methods)
+    bool trace_init = false;    // stage times of context creation on stderr
+    std::chrono::steady_clock::time_point t_init0;
     double *hpin = nullptr;     // pinned host slots for an iteration's results (E, residuum, DIIS info)
     int64_t async_iter = 0;     // iteration launched by iterate_async, 0 when none is pending
     double flops = 0.0;
@@ -360,11 +363,19 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
         }
         if (pos.size() == g.size()) gidx.push_back(pos);
     }
-    std::vector<long long> idx(labels.size(), 0);
-    bool more = true;
+    const size_t nd = labels.size();
+    std::vector<long long> idx(nd, 0), ev(nd), sx(nd), sy(nd, 0);
     long long total = 1;
-    for (auto &l : labels) total *= extent.at(l);
+    for (size_t d = 0; d < nd; ++d) {
+        ev[d] = extent.at(labels[d]);
+        sx[d] = x.stride.at(labels[d]);
+        if (y) sy[d] = y->stride.at(labels[d]);
+        total *= ev[d];
+    }
     if (total == 0) return;
+    tx.reserve((size_t)total);
+    if (y) ty.reserve((size_t)total);
+    bool more = true;
     while (more) {
         bool ok = true;
         for (auto &g : gidx)
@@ -372,23 +383,29 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
                 if (idx[g[q]] <= idx[g[q - 1]]) ok = false;
         if (ok) {
             long long ox = 0, oy = 0;
-            for (size_t d = 0; d < labels.size(); ++d) {
-                ox += idx[d] * x.stride.at(labels[d]);
-                if (y) oy += idx[d] * y->stride.at(labels[d]);
+            for (size_t d = 0; d < nd; ++d) {
+                ox += idx[d] * sx[d];
+                oy += idx[d] * sy[d];
             }
             if (ox > INT32_MAX || oy > INT32_MAX) throw Error(CCQ_B200_ERANGE, "view offset beyond int32");
             tx.push_back((int)ox);
             if (y) ty.push_back((int)oy);
         }
         more = false;
-        for (int d = (int)labels.size() - 1; d >= 0; --d) {
-            if (++idx[d] < extent.at(labels[d])) {
+        for (int d = (int)nd - 1; d >= 0; --d) {
+            if (++idx[d] < ev[d]) {
                 more = true;
                 break;
             }
             idx[d] = 0;
         }
     }
+}
+
+void trace_stamp(const ccq_b200_ctx *c, const char *what) {
+    if (!c->trace_init) return;
+    double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c->t_init0).count();
+    fprintf(stderr, "ccq_b200_init %-14s %8.2f ms\n", what, ms);
 }
 
 void instantiate(ccq_b200_ctx *c) {
@@ -513,6 +530,7 @@ void instantiate(ccq_b200_ctx *c) {
         c->bufs[b.name] = d;
     }
     launch_fill(c->bufs.at("ONES").ptr, 1.0, c->bufs.at("ONES").numel, c->stream);
+    trace_stamp(c, "buffers");
 
     // ---- operations ----------------------------------------------------------
     std::vector<int> itab;
@@ -884,6 +902,7 @@ void instantiate(ccq_b200_ctx *c) {
         o.g.offC_m = dtab + p.cm;
         o.g.offC_n = dtab + p.cn;
     }
+    trace_stamp(c, "op tables");
     // Group small-K contractions that add into the same Z view (consecutive writers
     // of that Z within one block phase, identical output tables): one launch per
     // group at the position of its last member.  Their operands are not modified
@@ -954,6 +973,7 @@ void instantiate(ccq_b200_ctx *c) {
             for (auto &l : leaders) c->plan.ops[l.first].g.segs = dsegs + l.second;
         }
     }
+    trace_stamp(c, "grouping");
     AsmTerm *dterms = (AsmTerm *)c->dalloc(sizeof(AsmTerm) * std::max<size_t>(hterms.size(), 1));
     CK(cudaMemcpyAsync(dterms, hterms.data(), sizeof(AsmTerm) * hterms.size(), cudaMemcpyHostToDevice, c->stream));
     signed char *dperm = (signed char *)c->dalloc(std::max<size_t>(hperm.size(), 1));
@@ -1118,15 +1138,6 @@ long long count_sweep_launches(ccq_b200_ctx *c) {
     return n;
 }
 
-// Fortran column-major (n,n,n,n) -> C-order [p][q][r][s] of v(p,q,r,s)
-void fortran4_to_c(const double *f, std::vector<double> &out, long long n) {
-    out.resize((size_t)(n * n * n * n));
-    for (long long s = 0; s < n; ++s)
-        for (long long r = 0; r < n; ++r)
-            for (long long q = 0; q < n; ++q)
-                for (long long p = 0; p < n; ++p) out[((p * n + q) * n + r) * n + s] = f[p + n * (q + n * (r + n * s))];
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1180,7 +1191,12 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
         CK(cudaEventCreate(&c->ev2));
+        // CCQ_B200_TRACE_INIT=1: stage times of context creation on stderr
+        c->trace_init = getenv("CCQ_B200_TRACE_INIT") != nullptr;
+        c->t_init0 = std::chrono::steady_clock::now();
+        auto stamp = [&](const char *what) { trace_stamp(c, what); };
         c->plan = parse_plan(text);
+        stamp("parse");
         // host-side integral preparation
         long long orbs = dims->orbs;
         std::vector<double> FA(n * n), FB(n * n);
@@ -1189,21 +1205,18 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
                 FA[p * n + q] = f_a[(p + fr) + orbs * (q + fr)];
                 FB[p * n + q] = f_b[(p + fr) + orbs * (q + fr)];
             }
-        std::vector<double> VAA, VAB, VBB;
-        fortran4_to_c(v_aa, VAA, n);
-        fortran4_to_c(v_ab, VAB, n);
-        fortran4_to_c(v_bb, VBB, n);
         std::vector<double> HA(FA), HB(FB);
-        auto V = [&](const std::vector<double> &x, long long p, long long q, long long r, long long s) {
-            return x[((p * n + q) * n + r) * n + s];
+        // v(p,q,r,s) of the Fortran (column-major) arrays
+        auto V = [&](const double *x, long long p, long long q, long long r, long long s) {
+            return x[p + n * (q + n * (r + n * s))];
         };
         for (long long p = 0; p < n; ++p)
             for (long long q = 0; q < n; ++q) {
                 double a = 0, b = 0;
-                for (long long i = 0; i < oa; ++i) a += V(VAA, p, i, q, i);
-                for (long long i = 0; i < ob; ++i) a += V(VAB, p, i, q, i);
-                for (long long i = 0; i < ob; ++i) b += V(VBB, p, i, q, i);
-                for (long long i = 0; i < oa; ++i) b += V(VAB, i, p, i, q);
+                for (long long i = 0; i < oa; ++i) a += V(v_aa, p, i, q, i);
+                for (long long i = 0; i < ob; ++i) a += V(v_ab, p, i, q, i);
+                for (long long i = 0; i < ob; ++i) b += V(v_bb, p, i, q, i);
+                for (long long i = 0; i < oa; ++i) b += V(v_ab, i, p, i, q);
                 HA[p * n + q] -= a;
                 HB[p * n + q] -= b;
             }
@@ -1216,7 +1229,10 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         c->fdiag_b = (double *)c->dalloc(sizeof(double) * n);
         CK(cudaMemcpy(c->fdiag_a, da.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(c->fdiag_b, db.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        stamp("host prep");
         instantiate(c);
+        CK(cudaStreamSynchronize(c->stream));
+        stamp("instantiate");
         auto up = [&](const char *name, const std::vector<double> &h) {
             DevBuf &d = c->bufs.at(name);
             if ((size_t)d.numel != h.size()) throw Error(CCQ_B200_EPLAN, std::string("size of ") + name);
@@ -1226,10 +1242,23 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         up("FB0", FB);
         up("HA0", HA);
         up("HB0", HB);
-        up("VAA0", VAA);
-        up("VAB0", VAB);
-        up("VBB0", VBB);
+        // two-electron blocks: the column-major arrays go up as they are (staged in the
+        // dressed buffer of the same size, which the first dressing overwrites) and
+        // are reordered to [p][q][r][s] on the device
+        auto up4 = [&](const char *name, const char *stage, const double *f) {
+            DevBuf &d = c->bufs.at(name);
+            DevBuf &st = c->bufs.at(stage);
+            const long long ne = n * n * n * n;
+            if (d.numel != ne || st.numel != ne) throw Error(CCQ_B200_EPLAN, std::string("size of ") + name);
+            CK(cudaMemcpyAsync(st.ptr, f, sizeof(double) * ne, cudaMemcpyHostToDevice, c->stream));
+            launch_f2c4(st.ptr, d.ptr, n, c->stream);
+        };
+        up4("VAA0", "VAA", v_aa);
+        up4("VAB0", "VAB", v_ab);
+        up4("VBB0", "VBB", v_bb);
+        CK(cudaStreamSynchronize(c->stream));
         CK(cudaDeviceSynchronize());
+        stamp("upload");
         *out = c;
         return 0;
     } catch (const Error &e) {

@@ -260,6 +260,7 @@ class PlanBuilder:
         self.nx = 0
         self.flops = 0
         self.zgroups = {}
+        self.lam_last = False   # contract lambda factors last (their partners then form T-only intermediates)
 
     # -- buffers --------------------------------------------------------------
     def buf(self, name, kind, dims):
@@ -282,6 +283,8 @@ class PlanBuilder:
         so = {'o': 2 * self.sizes['oa'], 'v': 2 * self.sizes['va']}
         best = None
         for order in itertools.permutations(range(1, len(base))):
+            if self.lam_last and any(base[k][0][0] == 'l' for k in order[:-1]):
+                continue
             cur = set(base[0][1])
             cost = 0
             for k in order:
@@ -698,10 +701,14 @@ class PlanBuilder:
         self.ops.append(Simple('CRDIAG', ()))
         self.ops.append(Simple('PHASE', ('lambda',)))
         self.ops.append(Simple('ZERO', ('LN',)))
+        lam_start = len(self.ops)
         asms = []
+        self.lam_last = True
         for b in ('L1A', 'L1B', 'L2A', 'L2B', 'L2C'):
             terms = lagrange.left_residual_terms(int(b[1]))
             asms.append(self.emit_block(b, terms=terms, undressed=True, mode='ljacobi', defer=True))
+        self.lam_last = False
+        self._hoist_lambda_free(lam_start)
         self.ops += asms
         self.ops.append(Simple('PHASE', ('lenergy',)))
         self.ops.append(Simple('LENERGY', ()))
@@ -713,6 +720,36 @@ class PlanBuilder:
                                             defer=True))
             self.ops.append(Simple('CRCC', (x,)))
         return self
+
+    def _hoist_lambda_free(self, start):
+        """Move the intermediates of ops[start:] that do not depend on lambda ahead of
+        the ``lambda`` phase marker (they are computed once per left solve) and
+        give them dedicated buffers (kind ``hx``, names Y*)."""
+        lam = {'L1A', 'L1B', 'L2A', 'L2B', 'L2C'}
+        ops = self.ops[start:]
+        dep = {}
+        for op in ops:
+            if isinstance(op, Gett) and op.c.buf.startswith('X'):
+                d = op.a.buf in lam or op.b.buf in lam or dep.get(op.a.buf, False) or dep.get(op.b.buf, False)
+                dep[op.c.buf] = dep.get(op.c.buf, False) or d
+        hoist = {x for x, d in dep.items() if not d}
+        ren = {}
+        for x in sorted(hoist, key=lambda q: int(q[1:])):
+            ren[x] = f'Y{len(ren)}'
+            kind, dims = self.buffers.pop(x)
+            self.buffers[ren[x]] = ('hx', dims)
+        moved, kept = [], []
+        for op in ops:
+            if isinstance(op, Gett):
+                for v in (op.a, op.b, op.c):
+                    if v.buf in ren:
+                        v.buf = ren[v.buf]
+                (moved if op.c.buf.startswith('Y') else kept).append(op)
+            else:
+                kept.append(op)
+        k = max(i for i in range(start) if isinstance(self.ops[i], Simple) and self.ops[i].kind == 'PHASE'
+                and self.ops[i].args[0] == 'lambda')
+        self.ops[k:] = moved + self.ops[k:start] + kept
 
     def text(self):
         lines = [f'PLAN {self.method} rhf={int(self.rhf)}']
