@@ -226,7 +226,10 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
                 for (int j = 0; j < 2; ++j)
                     Cs[wm + mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = alpha * acc[mi][ni][2 * h + j];
     __syncthreads();
-    const bool atomic = gridDim.z > 1;
+    // split-K slices and beta = 1 updates add into C with fire-and-forget reductions
+    // (one add per element and slice: the same rounding as a read-add-write, with no
+    // dependent read in the epilogue)
+    const bool atomic = gridDim.z > 1 || g.beta;
     if (g.vec_c && !atomic) {
         // output pairs along the fast mode are contiguous and 16-byte aligned
         const int fast = 2 * (tid & 31), slow0 = tid >> 5;
@@ -553,7 +556,10 @@ __global__ void __launch_bounds__(128) gett_f64_skinny_kernel(GettArgs g) {
                 for (int j = 0; j < 2; ++j)
                     Cs[mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = alpha * acc[mi][ni][2 * h + j];
     __syncthreads();
-    const bool atomic = gridDim.z > 1;
+    // split-K slices and beta = 1 updates add into C with fire-and-forget reductions
+    // (one add per element and slice: the same rounding as a read-add-write, with no
+    // dependent read in the epilogue)
+    const bool atomic = gridDim.z > 1 || g.beta;
     const bool nfast = sw ? !g.c_nfast : g.c_nfast;
     constexpr int R = 128 / BMS;
     // nfast: a thread owns column n = tid and walks the BMS rows; else BMS

@@ -89,3 +89,24 @@ def test_plan_file_matches_generator():
     from ccq_b200.eqgen import plan as P
     text = open(os.path.join(ROOT, 'ccq_b200', 'plans', 'CRCC23.plan')).read()
     assert P.build_plan('CR-CC(2,3)').text() == text
+
+
+@pytest.mark.parametrize('n,oa,ob,froz', [(7, 4, 3, 0), (8, 4, 4, 1), (8, 5, 3, 1)])
+def test_open_shell_and_frozen_core_plan_matches_dense(n, oa, ob, froz):
+    """Open shell (the beta-beta-beta cal_d3 bound then skips occ_a - occ_b + 1 virtuals) and frozen core."""
+    from tests.helpers import random_system
+    text = open(os.path.join(ROOT, 'ccq_b200', 'plans', 'CRCC23.plan')).read()
+    s = random_system(n, oa, ob, seed=11, sigma=0.08, froz=froz)
+    d = s['dims']
+    bc = BlockCRCC(text, s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d)
+    e, it, failed, hist, tvec = bc.solve(tol=1e-12, max_iter=200)
+    assert not failed
+    cc = DenseCC(s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d, 'CCSD')
+    e2, it2, f2, h2, tvec2 = cc.solve(tol=1e-12, max_iter=200)
+    assert abs(e - e2) < 1e-12 and it == it2
+    dc = DenseCRCC(cc, tvec2, e2)
+    _, itl, _, hl = dc.solve_left(tol=1e-12, max_iter=300)
+    _, itl2, _, hl2 = bc.solve_left(tvec, e, tol=1e-12, max_iter=300)
+    assert itl == itl2
+    np.testing.assert_allclose([h[0] for h in hl2], [h[0] for h in hl], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(bc.crcc23(tvec), dc.energies(), rtol=1e-10, atol=1e-16)

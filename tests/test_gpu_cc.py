@@ -46,6 +46,24 @@ def test_sweep_parity(method, rhf, n, oa, ob, plan_text):
     ctx.close()
 
 
+@pytest.mark.parametrize('method,froz', [('CCSD', 1), ('CCSDT', 1), ('CCSDT', 2)])
+def test_sweep_parity_frozen_core(method, froz, plan_text):
+    # froz inactive occupied orbitals (spatial): the active range starts at froz in every block
+    s = random_system(8, 4, 3, seed=19, sigma=0.08, froz=froz)
+    ctx = make_ctx(s, method, False, shift=0.02)
+    bc = BlockCC(plan_text(method, False), s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], s['dims'], method,
+                 shift=0.02)
+    t, _ = random_t(s['dims'], seed=3, scale=0.03, nmax=3 if method != 'CCSD' else 2)
+    ctx.set_t(t)
+    tc = t.copy()
+    for _ in range(2):
+        ctx.update()
+        bc.update(tc)
+    np.testing.assert_allclose(ctx.get_t(), tc, atol=1e-12, rtol=0)
+    assert abs(ctx.energy() - bc.energy(tc)) < 1e-12
+    ctx.close()
+
+
 @pytest.mark.parametrize('rhf', [False, True])
 def test_sweep_parity_ccsdtq(plan_text, rhf):
     s = random_system(5, 2, 2, seed=17)

@@ -119,3 +119,30 @@ def test_lambda_calls_need_a_crcc_context():
             ctx.crcc23()
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize('n,oa,ob,froz', [(7, 4, 3, 0), (8, 5, 3, 1)])
+def test_open_shell_and_frozen_core(n, oa, ob, froz):
+    from ccq_b200 import config, driver, lib
+    from oracle.blockcc import BlockCRCC
+    from tests.helpers import random_system
+    s = random_system(n, oa, ob, seed=11, sigma=0.08, froz=froz)
+    d = s['dims']
+    text = open(os.path.join(ROOT, 'ccq_b200', 'plans', 'CRCC23.plan')).read()
+    bc = BlockCRCC(text, s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d)
+    ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CR-CC(2,3)', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                      s['v_bb'])
+    try:
+        cfg = config.Config(calc_type='CR-CC(2,3)', tol=1e-11, max_iter=200).calc_macros()
+        r = driver.solve_cc(ctx, cfg, out=lambda x: None)
+        e, it, failed, _, tvec = bc.solve(tol=cfg.tol, max_iter=200)
+        assert r.iterations == it and abs(r.e_cor - e) < 1e-11
+        left = driver.solve_lcc(ctx, cfg, r.e_cor, out=lambda x: None)
+        _, itl, _, hl = bc.solve_left(tvec, e, tol=cfg.tol, max_iter=200)
+        assert left.iterations == itl
+        np.testing.assert_allclose([h['e'] for h in left.history], [h[0] for h in hl], atol=1e-10, rtol=0)
+        e23 = ctx.crcc23()
+        bc.lvec[:ctx.vec_size] = ctx.get_l()
+        np.testing.assert_allclose(e23, bc.crcc23(ctx.get_t()), rtol=1e-11, atol=1e-16)
+    finally:
+        ctx.close()
