@@ -107,6 +107,7 @@ struct Op {
     bool skip = false;         // member of a grouped GETT run by a later op
     double group_flops = 0.0;  // FLOPs of a grouped launch (leader only)
     int group_size = 0;
+    std::vector<size_t> group_ops;   // every op of a grouped launch (leader only; members are skipped)
     std::vector<int> hcm, hcn; // output offset tables (grouping key)
     AsmArgs asmargs{};
     CrccArgs crcc{};           // CRCC: one spin block's four-denominator sums
@@ -271,6 +272,10 @@ struct ccq_b200_ctx {
     long long l_size = 0;
     CrDiagArgs crd{};
     cudaGraphExec_t lgexec = nullptr;
+    // graph capture as a DAG: independent contractions on side streams
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> opev;
+    cudaEvent_t cap_ev = nullptr;
     long long t_dev = 0;        // t_vec elements resident on the device (T1+T2 for CCSD-level methods)
     bool trace_init = false;    // stage times of context creation on stderr
     std::chrono::steady_clock::time_point t_init0;
@@ -295,6 +300,9 @@ struct ccq_b200_ctx {
     ~ccq_b200_ctx() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (lgexec) cudaGraphExecDestroy(lgexec);
+        for (auto e : opev) cudaEventDestroy(e);
+        if (cap_ev) cudaEventDestroy(cap_ev);
+        for (auto st : side) cudaStreamDestroy(st);
         split_free(split);
         if (hpin) cudaFreeHost(hpin);
         for (void *p : owned) cudaFree(p);
@@ -957,6 +965,7 @@ void instantiate(ccq_b200_ctx *c) {
                         }
                         lead.g.beta = f.beta;
                         lead.g.nseg = (int)(j - k);
+                        for (size_t q = k; q < j; ++q) lead.group_ops.push_back(lst[q]);
                         lead.group_flops = fl;
                         lead.group_size = (int)(j - k);
                         leaders.push_back({lst[j - 1], off});
@@ -1006,6 +1015,140 @@ int op_class(const ccq_b200_ctx *c, const Op &o) {
     return 3;
 }
 
+void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
+    switch (o.kind) {
+        case OP_GETT:
+            if (o.skip || o.g.M == 0 || o.g.N == 0) break;
+            if (o.zero_first) {
+                launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, st);
+                ++c->launches;
+            }
+            if (o.g.K == 0) {
+                if (!o.beta) {
+                    launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, st);
+                    ++c->launches;
+                }
+                break;
+            }
+            if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g)) {
+                c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, st);
+            } else {
+                launch_gett_f64(o.g, o.akm, o.bkm, st);
+                ++c->launches;
+            }
+            break;
+        case OP_ASM:
+            launch_assemble(o.asmargs, st);
+            ++c->launches;
+            break;
+        case OP_COPY: {
+            DevBuf &d = c->bufs.at(o.arg0);
+            DevBuf &s = c->bufs.at(o.arg1);
+            if (d.numel != s.numel) throw Error(CCQ_B200_EPLAN, "COPY size mismatch");
+            CK(cudaMemcpyAsync(d.ptr, s.ptr, sizeof(double) * d.numel, cudaMemcpyDeviceToDevice, st));
+            break;
+        }
+        case OP_ZERO: {
+            DevBuf &d = c->bufs.at(o.arg0);
+            CK(cudaMemsetAsync(d.ptr, 0, sizeof(double) * std::max(d.numel, 1LL), st));
+            break;
+        }
+        case OP_PHASE:
+            break;
+        case OP_CRDIAG:
+            launch_crdiag(c->crd, st);
+            ++c->launches;
+            break;
+        case OP_LENERGY:
+            launch_lenergy(c->bufs.at("LN").ptr, c->bufs.at("ECOR").ptr, c->bufs.at("EL").ptr, st);
+            ++c->launches;
+            break;
+        case OP_CRCC:
+            launch_crcc_sum(o.crcc, st);
+            ++c->launches;
+            break;
+    }
+}
+
+// ops[from, to) issued for stream capture as a DAG.  Every GETT waits only for
+// the GETTs it reads from, the last overwrite of its output and the earlier
+// readers of that output; beta = 1 writers of one buffer do not wait for each
+// other (their epilogues add with reductions).  Everything else (assembles,
+// copies, zeroing, split GETTs, whose slicing shares one workspace) is a
+// barrier on the capturing stream.  Independent contractions then run on side
+// streams at the same time.
+void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
+    constexpr int NSIDE = 6;
+    if (c->side.empty()) {
+        c->side.resize(NSIDE);
+        for (auto &st : c->side) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->cap_ev, cudaEventDisableTiming));
+    }
+    if (c->opev.size() < c->plan.ops.size()) {
+        size_t old = c->opev.size();
+        c->opev.resize(c->plan.ops.size(), nullptr);
+        for (size_t i = old; i < c->opev.size(); ++i) CK(cudaEventCreateWithFlags(&c->opev[i], cudaEventDisableTiming));
+    }
+    struct BufState {
+        std::vector<size_t> writers, full, readers;
+    };
+    std::map<std::string, BufState> st;
+    std::vector<size_t> pending;
+    cudaEvent_t gate = c->cap_ev;   // the last barrier (or the capture's start)
+    CK(cudaEventRecord(gate, c->stream));
+    int rr = 0;
+    auto join = [&]() {
+        for (size_t j : pending) CK(cudaStreamWaitEvent(c->stream, c->opev[j], 0));
+        pending.clear();
+        st.clear();
+    };
+    for (size_t i = from; i < to; ++i) {
+        Op &o = c->plan.ops[i];
+        if (o.kind == OP_PHASE) continue;
+        if (o.kind == OP_GETT && (o.skip || o.g.M == 0 || o.g.N == 0)) continue;
+        const bool barrier = o.kind != OP_GETT ||
+                             (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g));
+        if (barrier) {
+            join();
+            run_op(c, o, c->stream);
+            CK(cudaEventRecord(c->opev[i], c->stream));
+            gate = c->opev[i];
+            continue;
+        }
+        std::vector<size_t> deps;
+        auto add = [&](const std::vector<size_t> &v) { deps.insert(deps.end(), v.begin(), v.end()); };
+        std::vector<std::string> ins = {o.a.buf, o.b.buf};
+        for (size_t m : o.group_ops) {
+            ins.push_back(c->plan.ops[m].a.buf);
+            ins.push_back(c->plan.ops[m].b.buf);
+        }
+        for (auto &b : ins) add(st[b].writers);
+        BufState &cs = st[o.c.buf];
+        // a grouped launch carries the beta of its first member (g.beta), not its own
+        const bool overwrite = !o.g.beta || o.zero_first || o.g.K == 0;
+        add(cs.readers);
+        add(overwrite ? cs.writers : cs.full);
+        cudaStream_t sd = c->side[rr++ % NSIDE];
+        CK(cudaStreamWaitEvent(sd, gate, 0));
+        std::sort(deps.begin(), deps.end());
+        deps.erase(std::unique(deps.begin(), deps.end()), deps.end());
+        for (size_t d : deps) CK(cudaStreamWaitEvent(sd, c->opev[d], 0));
+        run_op(c, o, sd);
+        CK(cudaEventRecord(c->opev[i], sd));
+        pending.push_back(i);
+        for (auto &b : ins) st[b].readers.push_back(i);
+        if (overwrite) {
+            cs.writers.assign(1, i);
+            cs.full.assign(1, i);
+            cs.readers.clear();
+        } else {
+            cs.writers.push_back(i);
+        }
+    }
+    join();
+    CK(cudaGetLastError());
+}
+
 void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
     bool prof = c->profile != 0;
     if (prof && c->pev.size() < 2 * c->plan.ops.size()) {
@@ -1016,58 +1159,7 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
     for (size_t i = from; i < to; ++i) {
         Op &o = c->plan.ops[i];
         if (prof) CK(cudaEventRecord(c->pev[2 * i], c->stream));
-        switch (o.kind) {
-            case OP_GETT:
-                if (o.skip || o.g.M == 0 || o.g.N == 0) break;
-                if (o.zero_first) {
-                    launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, c->stream);
-                    ++c->launches;
-                }
-                if (o.g.K == 0) {
-                    if (!o.beta) {
-                        launch_zero_view(o.g.C, o.g.offC_m, o.g.offC_n, o.g.M, o.g.N, c->stream);
-                        ++c->launches;
-                    }
-                    break;
-                }
-                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g)) {
-                    c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, c->stream);
-                } else {
-                    launch_gett_f64(o.g, o.akm, o.bkm, c->stream);
-                    ++c->launches;
-                }
-                break;
-            case OP_ASM:
-                launch_assemble(o.asmargs, c->stream);
-                ++c->launches;
-                break;
-            case OP_COPY: {
-                DevBuf &d = c->bufs.at(o.arg0);
-                DevBuf &s = c->bufs.at(o.arg1);
-                if (d.numel != s.numel) throw Error(CCQ_B200_EPLAN, "COPY size mismatch");
-                CK(cudaMemcpyAsync(d.ptr, s.ptr, sizeof(double) * d.numel, cudaMemcpyDeviceToDevice, c->stream));
-                break;
-            }
-            case OP_ZERO: {
-                DevBuf &d = c->bufs.at(o.arg0);
-                CK(cudaMemsetAsync(d.ptr, 0, sizeof(double) * std::max(d.numel, 1LL), c->stream));
-                break;
-            }
-            case OP_PHASE:
-                break;
-            case OP_CRDIAG:
-                launch_crdiag(c->crd, c->stream);
-                ++c->launches;
-                break;
-            case OP_LENERGY:
-                launch_lenergy(c->bufs.at("LN").ptr, c->bufs.at("ECOR").ptr, c->bufs.at("EL").ptr, c->stream);
-                ++c->launches;
-                break;
-            case OP_CRCC:
-                launch_crcc_sum(o.crcc, c->stream);
-                ++c->launches;
-                break;
-        }
+        run_op(c, o, c->stream);
         if (prof) CK(cudaEventRecord(c->pev[2 * i + 1], c->stream));
     }
     CK(cudaGetLastError());
@@ -1106,7 +1198,7 @@ void sweep(ccq_b200_ctx *c) {
             long long l0 = c->launches;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             try {
-                run_ops(c, 0, c->cc_end);
+                run_ops_dag(c, 0, c->cc_end);
             } catch (...) {
                 cudaStreamEndCapture(c->stream, &g);
                 throw;
@@ -1486,7 +1578,7 @@ int ccq_b200_lambda_iterate(ccq_b200_ctx *c, int64_t iter, double *e_left, doubl
                 cudaGraph_t g;
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
                 try {
-                    run_ops(c, c->lambda_op, c->triples_op);
+                    run_ops_dag(c, c->lambda_op, c->triples_op);
                 } catch (...) {
                     cudaStreamEndCapture(c->stream, &g);
                     throw;
