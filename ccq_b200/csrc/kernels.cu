@@ -728,44 +728,56 @@ __device__ __forceinline__ int pick(const int (&v)[RK], int i) {
     return r;
 }
 
+// Each thread gathers EPT canonical elements, EPT * blockDim.x consecutive
+// elements per block and step: every term descriptor read from shared memory
+// serves EPT elements, and their loads are independent.
+constexpr int ASM_EPT = 2;
+
+template <int RK>
+__device__ __forceinline__ void canonical_element(const AsmArgs &a, long long lin, int (&x)[RK]) {
+    int cq[RK];
+    long long r = lin;
+#pragma unroll
+    for (int q = RK - 1; q >= 0; --q) {
+        cq[q] = 0;
+        if (q < a.nruns) {
+            cq[q] = (int)(r % a.run_count[q]);
+            r /= a.run_count[q];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < RK; ++q) {
+        if (q < a.nruns) {
+            const unsigned char *tup = a.combos + a.run_off[q] + cq[q] * a.run_len[q];
+#pragma unroll
+            for (int d = 0; d < RK; ++d) {
+                int l = d - a.run_axis0[q];
+                if (l >= 0 && l < a.run_len[q]) x[d] = tup[l];
+            }
+        }
+    }
+}
+
 template <int RK>
 __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
     constexpr int CH = 128;
     __shared__ SmTerm<RK> st[CH];
     const int nch = (a.nterms + CH - 1) / CH;
     double nacc = 0.0;
-    for (long long base = blockIdx.x * (long long)blockDim.x; base < a.total;
-         base += (long long)gridDim.x * blockDim.x) {
-        const long long lin = base + threadIdx.x;
-        const bool act = lin < a.total;
-        int x[RK];
+    const long long step = (long long)gridDim.x * blockDim.x * ASM_EPT;
+    for (long long base = (long long)blockIdx.x * blockDim.x * ASM_EPT; base < a.total; base += step) {
+        int x[ASM_EPT][RK];
+        bool act[ASM_EPT];
+        double R[ASM_EPT];
 #pragma unroll
-        for (int d = 0; d < RK; ++d) x[d] = 0;
-        if (act) {
-            // canonical element from its per-run combination indices
-            int cq[RK];
-            long long r = lin;
+        for (int e = 0; e < ASM_EPT; ++e) {
+            const long long lin = base + e * (long long)blockDim.x + threadIdx.x;
+            act[e] = lin < a.total;
+            R[e] = 0.0;
 #pragma unroll
-            for (int q = RK - 1; q >= 0; --q) {
-                cq[q] = 0;
-                if (q < a.nruns) {
-                    cq[q] = (int)(r % a.run_count[q]);
-                    r /= a.run_count[q];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < RK; ++q) {
-                if (q < a.nruns) {
-                    const unsigned char *tup = a.combos + a.run_off[q] + cq[q] * a.run_len[q];
-#pragma unroll
-                    for (int d = 0; d < RK; ++d) {
-                        int l = d - a.run_axis0[q];
-                        if (l >= 0 && l < a.run_len[q]) x[d] = tup[l];
-                    }
-                }
-            }
+            for (int d = 0; d < RK; ++d) x[e][d] = 0;
+            if (act[e]) canonical_element<RK>(a, lin, x[e]);
         }
-        double R = 0.0;
         for (int c = 0; c < nch; ++c) {
             __syncthreads();
             const int nt = min(CH, a.nterms - c * CH);
@@ -798,19 +810,32 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
                 st[t] = q;
             }
             __syncthreads();
-            if (act) {
-#pragma unroll 4
-                for (int t = 0; t < nt; ++t) {
-                    const SmTerm<RK> &q = st[t];
-                    long long off = 0;
-                    double sg = q.coef;
-                    if (q.pm == 0) {
+#pragma unroll 2
+            for (int t = 0; t < nt; ++t) {
+                const SmTerm<RK> &q = st[t];
+                const double *p = q.p;
+                if (q.pm == 0) {
+                    int tst[RK];
 #pragma unroll
-                        for (int d = 0; d < RK; ++d) off += (long long)q.tst[d] * x[d];
-                    } else {
+                    for (int d = 0; d < RK; ++d) tst[d] = q.tst[d];
+                    double v[ASM_EPT];
+#pragma unroll
+                    for (int e = 0; e < ASM_EPT; ++e) {
+                        long long off = 0;
+#pragma unroll
+                        for (int d = 0; d < RK; ++d) off += (long long)tst[d] * x[e][d];
+                        v[e] = act[e] ? __ldg(p + off) : 0.0;
+                    }
+#pragma unroll
+                    for (int e = 0; e < ASM_EPT; ++e) R[e] += q.coef * v[e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < ASM_EPT; ++e) {
+                        if (!act[e]) continue;
+                        double sg = q.coef;
                         int y[RK];
 #pragma unroll
-                        for (int j = 0; j < RK; ++j) y[j] = pick<RK>(x, q.src[j]);
+                        for (int j = 0; j < RK; ++j) y[j] = pick<RK>(x[e], q.src[j]);
                         bool zero = false;
                         // selection sort within groups: one sign flip per exchange
 #pragma unroll
@@ -828,41 +853,45 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
                                     }
                                 }
                         if (zero) continue;
+                        long long off = 0;
 #pragma unroll
                         for (int j = 0; j < RK; ++j) off += (long long)q.zs[j] * y[j];
+                        R[e] += sg * __ldg(p + off);
                     }
-                    R += sg * __ldg(q.p + off);
                 }
             }
         }
-        if (!act) continue;
-        long long toff = 0;
 #pragma unroll
-        for (int d = 0; d < RK; ++d) toff += (long long)a.tstride[d] * x[d];
-        double tnew;
-        if (a.mode != 1) {
-            double D = a.shift;
-            if (a.mode == 2) {
-                D -= *a.ecor;
-                nacc += a.nperm * R * R;
+        for (int e = 0; e < ASM_EPT; ++e) {
+            if (!act[e]) continue;
+            long long toff = 0;
+#pragma unroll
+            for (int d = 0; d < RK; ++d) toff += (long long)a.tstride[d] * x[e][d];
+            double tnew;
+            if (a.mode != 1) {
+                double D = a.shift;
+                if (a.mode == 2) {
+                    D -= *a.ecor;
+                    nacc += a.nperm * R[e] * R[e];
+                }
+#pragma unroll
+                for (int d = 0; d < RK; ++d) {
+                    if (d < RK / 2)
+                        D -= a.fdiag[a.spin[d]][x[e][d]];
+                    else
+                        D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[e][d]];
+                }
+                tnew = a.T[toff] - R[e] / D;
+            } else {
+                tnew = R[e];
             }
+            for (int pidx = 0; pidx < a.nperm; ++pidx) {
+                const signed char *P = a.perm + pidx * RK;
+                long long o = 0;
 #pragma unroll
-            for (int d = 0; d < RK; ++d) {
-                if (d < RK / 2)
-                    D -= a.fdiag[a.spin[d]][x[d]];
-                else
-                    D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[d]];
+                for (int d = 0; d < RK; ++d) o += (long long)a.tstride[d] * pick<RK>(x[e], P[d]);
+                a.T[o] = a.psign[pidx] * tnew;
             }
-            tnew = a.T[toff] - R / D;
-        } else {
-            tnew = R;
-        }
-        for (int pidx = 0; pidx < a.nperm; ++pidx) {
-            const signed char *P = a.perm + pidx * RK;
-            long long o = 0;
-#pragma unroll
-            for (int d = 0; d < RK; ++d) o += (long long)a.tstride[d] * pick<RK>(x, P[d]);
-            a.T[o] = a.psign[pidx] * tnew;
         }
     }
     if (a.mode == 2) {
@@ -872,7 +901,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
 }
 
 void launch_assemble(const AsmArgs &a, cudaStream_t s) {
-    long long blocks = (a.total + 255) / 256;
+    long long blocks = (a.total + 256 * ASM_EPT - 1) / (256 * ASM_EPT);
     if (blocks > 148 * 32) blocks = 148 * 32;
     if (blocks < 1) blocks = 1;
     switch (a.rank) {
