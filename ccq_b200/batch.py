@@ -61,7 +61,9 @@ class Instance:
         self.spec = spec
         self.ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, calc_type, s['f_a'], s['f_b'], s['v_aa'],
                                s['v_ab'], s['v_bb'], diis_space=diis_space)
-        self.ctx.use_graph(graph)
+        # one stream per instance: the instances overlap one another, so each replays a
+        # single-stream graph (mode 2) rather than its own concurrent one
+        self.ctx.use_graph(2 if graph else 0)
         self.conv = [1.0, 1.0, 1.0]
         self.e = 0.0
         self.it = 0

@@ -1198,7 +1198,10 @@ void sweep(ccq_b200_ctx *c) {
             long long l0 = c->launches;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             try {
-                run_ops_dag(c, 0, c->cc_end);
+                if (c->use_graph == 2)
+                    run_ops(c, 0, c->cc_end);
+                else
+                    run_ops_dag(c, 0, c->cc_end);
             } catch (...) {
                 cudaStreamEndCapture(c->stream, &g);
                 throw;
@@ -1578,7 +1581,10 @@ int ccq_b200_lambda_iterate(ccq_b200_ctx *c, int64_t iter, double *e_left, doubl
                 cudaGraph_t g;
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
                 try {
-                    run_ops_dag(c, c->lambda_op, c->triples_op);
+                    if (c->use_graph == 2)
+                        run_ops(c, c->lambda_op, c->triples_op);
+                    else
+                        run_ops_dag(c, c->lambda_op, c->triples_op);
                 } catch (...) {
                     cudaStreamEndCapture(c->stream, &g);
                     throw;
@@ -1703,7 +1709,13 @@ int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {
 
 int ccq_b200_use_graph(ccq_b200_ctx *c, int64_t enable) {
     if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
-    c->use_graph = enable != 0;
+    if (enable < 0 || enable > 2) return fail(Error(CCQ_B200_EINVAL, "use_graph: 0, 1 or 2"));
+    if ((int)enable != c->use_graph) {
+        if (c->gexec) cudaGraphExecDestroy(c->gexec);
+        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
+        c->gexec = c->lgexec = nullptr;
+    }
+    c->use_graph = (int)enable;
     return 0;
 }
 

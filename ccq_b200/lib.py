@@ -209,7 +209,8 @@ class Context:
         _err(self._lib.ccq_b200_set_precision(self.ptr, mode, nslices))
 
     def use_graph(self, enable=True):
-        _err(self._lib.ccq_b200_use_graph(self.ptr, int(bool(enable))))
+        """True / 1: concurrent graph, 2: single-stream graph, False / 0: eager launches."""
+        _err(self._lib.ccq_b200_use_graph(self.ptr, int(enable)))
 
     def stats(self):
         n, f, ms = I64(), C.c_double(), C.c_double()

@@ -195,8 +195,10 @@ int ccq_b200_get_l(ccq_b200_ctx *ctx, double *l_vec, int64_t n);
  * (2..7) for CCQ_B200_PREC_SPLIT. */
 int ccq_b200_set_precision(ccq_b200_ctx *ctx, int64_t mode, int64_t nslices);
 
-/* Capture one update+energy sweep in a CUDA graph and replay it (1) or run
- * the kernels one by one (0). */
+/* Capture one update+energy sweep in a CUDA graph and replay it: 1 = a graph
+ * whose independent contractions run concurrently (side streams, dependencies
+ * from the buffers each operation reads and writes), 2 = a single-stream graph
+ * (for many contexts running at once), 0 = launch the kernels one by one. */
 int ccq_b200_use_graph(ccq_b200_ctx *ctx, int64_t enable);
 
 /* Counters: kernels launched by the last iterate, algorithmic FP64 FLOPs of
