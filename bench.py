@@ -45,6 +45,7 @@ def parse():
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-converge', action='store_true')
     p.add_argument('--no-peaks', action='store_true', help='use MEASURED_PEAKS.json / fallback only')
+    p.add_argument('--no-tune', action='store_true', help='keep the shape heuristics (no autotuning sweep)')
     p.add_argument('--no-crcc', action='store_true', help='skip the CR-CC(2,3) leg (32 orbitals)')
     p.add_argument('--no-batch', action='store_true', help='skip the batched CCSD leg (64 Hamiltonians)')
     p.add_argument('--warmstart', action='store_true',
@@ -416,9 +417,16 @@ def main():
     legs = ['fp64'] + (['split'] if split_ok and args.precision != 'fp64' else [])
     clocks = Clocks(local)
     results = {}
+    tuning = {}
     it = 1
     for leg in legs:
         ctx.set_precision(lib.PREC_SPLIT if leg == 'split' else lib.PREC_FP64, args.slices)
+        if not args.no_tune:
+            # one eager sweep timing every contraction's candidates; amplitudes untouched
+            t0 = time.perf_counter()
+            before, after = ctx.autotune(3)
+            tuning[leg] = {'gett_ms_heuristic': before, 'gett_ms_tuned': after,
+                           'wall_s': time.perf_counter() - t0}
         # warm-up continues the same solve (iterations keep counting, DIIS on schedule)
         for _ in range(args.warmup):
             ctx.iterate(it)
@@ -503,7 +511,8 @@ def main():
         from ccq_b200 import config, driver
         c2 = new_ctx()
         cfg = config.Config(calc_type='CCSDT', tol=1e-10, diis_space=5, max_iter=100,
-                            gpu_precision=headline, gpu_slices=args.slices).calc_macros()
+                            gpu_precision=headline, gpu_slices=args.slices,
+                            gpu_autotune=not args.no_tune).calc_macros()
         r = driver.solve_cc(c2, cfg, out=lambda x: None)
         c2.close()
         g = golden_c2()
@@ -539,7 +548,7 @@ def main():
             'data': 'synthetic (seeded generator, no molecular integrals)',
             'config': {'workload': WORKLOAD, 'precision': headline, 'parallelism': f'replicas x{world}',
                        'l2': 'working set (T3 4x134 MB + DIIS ring) > 126 MB L2, no flush'},
-            'tflops': head['tflops'], 'legs': results,
+            'tflops': head['tflops'], 'legs': results, 'autotune': tuning or None,
             'speedup_split_vs_fp64': (results['fp64']['s_per_iter'] / results['split']['s_per_iter']
                                       if 'split' in results else None),
             'roofline': roofline,

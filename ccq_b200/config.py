@@ -10,7 +10,8 @@
 New keys of this engine are prefixed ``gpu_``: ``gpu_precision`` (fp64 |
 split), ``gpu_slices`` (int8 slices per operand), ``gpu_fp64_finish`` (|dE|
 below which the split mode hands over to FP64), ``gpu_graph`` (replay each
-sweep as one CUDA graph).
+sweep as one CUDA graph), ``gpu_autotune`` (time every contraction's tile and
+split-K candidates once before the first iteration and keep the fastest).
 """
 from __future__ import annotations
 
@@ -54,6 +55,7 @@ class Config:
     gpu_slices: int = 4
     gpu_fp64_finish: float = 1.0e-6
     gpu_graph: bool = True
+    gpu_autotune: bool = False
     # derived (process_sys_data)
     froz: int = 0
     occ_a: int = 0
@@ -158,6 +160,8 @@ def _apply(cfg, key, val):
         cfg.gpu_fp64_finish = float(val)
     elif key == 'gpu_graph':
         cfg.gpu_graph = _logical(val)
+    elif key == 'gpu_autotune':
+        cfg.gpu_autotune = _logical(val)
     else:
         cfg.extra[key] = val
 

@@ -665,7 +665,9 @@ int gett_f64_kchunk(long long M, long long N, long long K) {
 
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
     const int zsplit = a.segs ? 1 : std::max(1, (a.K + a.kchunk - 1) / a.kchunk);
-    const int fam = gett_f64_family(a.M, a.N);
+    int fam = gett_f64_family(a.M, a.N);
+    if (a.tile == 1) fam = 0;
+    else if (a.tile == 2 && std::min(a.M, a.N) <= 32) fam = a.M <= a.N ? 1 : 2;
     if (fam) {
         gett_f64_prepare();
         const int shrt = std::min(a.M, a.N), lng = std::max(a.M, a.N);

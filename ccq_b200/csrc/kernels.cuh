@@ -45,6 +45,7 @@ struct GettArgs {
     int vec_a, vec_b, vec_c;
     const GettSeg *segs;  // grouped launch: nseg terms (A, B, tables, K, alpha above unused)
     int nseg;
+    int tile;       // 0: tile family by shape (gett_f64_family); 1: 64 x 64 tiles; 2: skinny tiles
 };
 
 constexpr int MAXG = 4;  // antisymmetric axis groups per source view

@@ -107,6 +107,7 @@ struct Op {
     bool skip = false;         // member of a grouped GETT run by a later op
     double group_flops = 0.0;  // FLOPs of a grouped launch (leader only)
     int group_size = 0;
+    int split_choice = -1;     // split precision for this op: -1 by shape (split_eligible), 0 no, 1 yes (autotuned)
     std::vector<size_t> group_ops;   // every op of a grouped launch (leader only; members are skipped)
     std::vector<int> hcm, hcn; // output offset tables (grouping key)
     AsmArgs asmargs{};
@@ -1009,8 +1010,14 @@ void instantiate(ccq_b200_ctx *c) {
     CK(cudaStreamSynchronize(c->stream));
 }
 
+// the op runs on the split-precision kernel in this context's current mode
+bool use_split(const ccq_b200_ctx *c, const Op &o) {
+    if (c->precision != CCQ_B200_PREC_SPLIT || !o.split) return false;
+    return o.split_choice >= 0 ? o.split_choice == 1 : split_eligible(o.g);
+}
+
 int op_class(const ccq_b200_ctx *c, const Op &o) {
-    if (o.kind == OP_GETT) return (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g)) ? 1 : 0;
+    if (o.kind == OP_GETT) return use_split(c, o) ? 1 : 0;
     if (o.kind == OP_ASM) return 2;
     return 3;
 }
@@ -1030,7 +1037,7 @@ void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
                 }
                 break;
             }
-            if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g)) {
+            if (use_split(c, o)) {
                 c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, st);
             } else {
                 launch_gett_f64(o.g, o.akm, o.bkm, st);
@@ -1107,7 +1114,7 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         if (o.kind == OP_PHASE) continue;
         if (o.kind == OP_GETT && (o.skip || o.g.M == 0 || o.g.N == 0)) continue;
         const bool barrier = o.kind != OP_GETT ||
-                             (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g));
+                             use_split(c, o);
         if (barrier) {
             join();
             run_op(c, o, c->stream);
@@ -1224,7 +1231,7 @@ long long count_sweep_launches(ccq_b200_ctx *c) {
         if (o.kind == OP_GETT && o.g.M && o.g.N && !o.skip) {
             if (o.zero_first || o.g.K == 0) ++n;
             if (o.g.K)
-                n += (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_eligible(o.g))
+                n += use_split(c, o)
                          ? split_launch_count(o.g, c->nslices) : 1;
         } else if (o.kind == OP_ASM) {
             ++n;
@@ -1669,6 +1676,157 @@ int ccq_b200_get_l(ccq_b200_ctx *c, double *l_vec, int64_t n) {
         CK(cudaSetDevice(c->device));
         CK(cudaMemcpyAsync(l_vec, c->lvec, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+// ---- autotuner ------------------------------------------------------------------
+// One eager sweep in which every contraction is timed in each candidate
+// configuration (tile family, split-K chunk, and in split mode int8 slices or
+// DMMA), writing into scratch so that the sweep's own data stay intact; the op
+// then runs once for real in the fastest configuration.  The amplitudes are
+// restored afterwards, so tuning does not count as an iteration.
+
+static bool split_capable(const GettArgs &g) {
+    long long tiles = ((g.M + 127LL) / 128) * ((g.N + 127LL) / 128);
+    return g.M >= 64 && g.N >= 64 && g.K >= 256 && tiles >= 64;
+}
+
+struct TuneCfg {
+    int tile, kchunk, split;
+};
+
+static float time_cfg(ccq_b200_ctx *c, Op &o, const TuneCfg &t, double *scratch, int reps) {
+    GettArgs g = o.g;
+    g.C = scratch;
+    g.tile = t.tile;
+    g.kchunk = t.kchunk;
+    const bool zf = !g.segs && g.beta == 0 && (g.K + t.kchunk - 1) / t.kchunk > 1;
+    auto run = [&]() {
+        if (t.split) {
+            split_gett(c->split, g, o.akm, o.bkm, c->nslices, c->stream);
+        } else {
+            if (zf) launch_zero_view(g.C, g.offC_m, g.offC_n, g.M, g.N, c->stream);
+            launch_gett_f64(g, o.akm, o.bkm, c->stream);
+        }
+    };
+    run();
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < reps; ++r) run();
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    CK(cudaGetLastError());
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    return ms / reps;
+}
+
+int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double *ms_tuned) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        if (reps < 1) reps = 3;
+        CK(cudaSetDevice(c->device));
+        CK(cudaStreamSynchronize(c->stream));
+        // amplitude state to restore: t_vec and the amplitude blocks outside it
+        std::vector<std::pair<double *, long long>> keep;
+        keep.push_back({c->tvec, c->t_dev});
+        for (auto &b : c->plan.bufs)
+            if (b.kind == "amp") {
+                const DevBuf &d = c->bufs.at(b.name);
+                if (d.ptr && (d.ptr < c->tvec || d.ptr >= c->tvec + c->t_dev)) keep.push_back({d.ptr, d.numel});
+            }
+        long long nkeep = 0, nscr = 1;
+        for (auto &k : keep) nkeep += k.second;
+        for (size_t i = 0; i < c->cc_end; ++i) {
+            const Op &o = c->plan.ops[i];
+            if (o.kind == OP_GETT) nscr = std::max(nscr, c->bufs.at(o.c.buf).numel);
+        }
+        double *backup = nullptr, *scratch = nullptr;
+        CK(cudaMalloc(&backup, sizeof(double) * std::max(nkeep, 1LL)));
+        CK(cudaMalloc(&scratch, sizeof(double) * nscr));
+        auto release = [&]() {
+            cudaFree(backup);
+            cudaFree(scratch);
+        };
+        double t0 = 0.0, t1 = 0.0;
+        try {
+            long long off = 0;
+            for (auto &k : keep) {
+                CK(cudaMemcpyAsync(backup + off, k.first, sizeof(double) * k.second, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+                off += k.second;
+            }
+            for (size_t i = 0; i < c->cc_end; ++i) {
+                Op &o = c->plan.ops[i];
+                if (o.kind != OP_GETT || o.skip || o.g.M == 0 || o.g.N == 0 || o.g.K == 0) {
+                    run_op(c, o, c->stream);
+                    continue;
+                }
+                const long long M = o.g.M, N = o.g.N, K = o.g.K;
+                std::vector<TuneCfg> cand;
+                const TuneCfg cur{o.g.tile, o.g.kchunk, use_split(c, o) ? 1 : 0};
+                cand.push_back(cur);
+                std::vector<int> tiles = {1};
+                if (std::min(M, N) <= 32) tiles.push_back(2);
+                for (int tl : tiles) {
+                    std::vector<long long> ch;
+                    if (o.g.segs) {
+                        ch.push_back(o.g.kchunk);
+                    } else {
+                        const long long c0 = o.g.kchunk;
+                        for (long long x : {c0, K, 2 * c0, c0 / 2, c0 / 4})
+                            ch.push_back(std::max(16LL, std::min(K + 15 - (K + 15) % 16, (x + 15) / 16 * 16)));
+                    }
+                    for (long long x : ch) {
+                        TuneCfg t{tl, (int)x, 0};
+                        bool dup = false;
+                        for (auto &q : cand) dup = dup || (q.tile == t.tile && q.kchunk == t.kchunk && q.split == 0);
+                        if (!dup) cand.push_back(t);
+                    }
+                }
+                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_capable(o.g) && !cur.split)
+                    cand.push_back(TuneCfg{0, o.g.kchunk, 1});
+                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && cur.split)
+                    cand.push_back(TuneCfg{0, o.g.kchunk, 0});
+                float best = 1e30f;
+                TuneCfg pick = cur;
+                for (size_t q = 0; q < cand.size(); ++q) {
+                    const float ms = time_cfg(c, o, cand[q], scratch, (int)reps);
+                    if (q == 0) t0 += ms;
+                    if (ms < best) {
+                        best = ms;
+                        pick = cand[q];
+                    }
+                }
+                t1 += best;
+                o.g.tile = pick.tile;
+                o.g.kchunk = pick.kchunk;
+                o.zero_first = !o.g.segs && o.beta == 0 && (o.g.K + pick.kchunk - 1) / pick.kchunk > 1;
+                if (c->precision == CCQ_B200_PREC_SPLIT && o.split) o.split_choice = pick.split;
+                run_op(c, o, c->stream);
+            }
+            off = 0;
+            for (auto &k : keep) {
+                CK(cudaMemcpyAsync(k.first, backup + off, sizeof(double) * k.second, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+                off += k.second;
+            }
+            CK(cudaStreamSynchronize(c->stream));
+        } catch (...) {
+            cudaStreamSynchronize(c->stream);
+            release();
+            throw;
+        }
+        release();
+        if (c->gexec) cudaGraphExecDestroy(c->gexec);
+        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
+        c->gexec = c->lgexec = nullptr;
+        if (ms_default) *ms_default = t0;
+        if (ms_tuned) *ms_tuned = t1;
         return 0;
     } catch (const Error &e) {
         return fail(e);

@@ -49,6 +49,8 @@ def solve_cc(ctx, cfg, out=print, precision=None):
     split = prec == 'split'
     ctx.set_precision(lib.PREC_SPLIT if split else lib.PREC_FP64, cfg.gpu_slices)
     ctx.use_graph(cfg.gpu_graph)
+    if cfg.gpu_autotune:
+        ctx.autotune()
     conv = [1.0, 1.0, 1.0]
     en_cor = 0.0
     failed = False

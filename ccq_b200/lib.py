@@ -54,6 +54,7 @@ SIGNATURES = {
     'ccq_b200_crcc23': (C.c_int, [C.c_void_p, DP]),
     'ccq_b200_get_l': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_set_precision': (C.c_int, [C.c_void_p, I64, I64]),
+    'ccq_b200_autotune': (C.c_int, [C.c_void_p, I64, DP, DP]),
     'ccq_b200_use_graph': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), DP, DP]),
     'ccq_b200_timing': (C.c_int, [C.c_void_p, DP, DP]),
@@ -204,6 +205,12 @@ class Context:
         out = np.empty(self.vec_size)
         _err(self._lib.ccq_b200_get_l(self.ptr, _p(out), out.size))
         return out
+
+    def autotune(self, reps=3):
+        """Times every contraction's candidate configurations once; returns (ms before, ms after)."""
+        a, b = C.c_double(), C.c_double()
+        _err(self._lib.ccq_b200_autotune(self.ptr, reps, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def set_precision(self, mode, nslices=4):
         _err(self._lib.ccq_b200_set_precision(self.ptr, mode, nslices))

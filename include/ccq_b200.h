@@ -144,6 +144,15 @@ int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
 int ccq_b200_iterate_async(ccq_b200_ctx *ctx, int64_t iter);
 int ccq_b200_iterate_wait(ccq_b200_ctx *ctx, double *e_cor, double *residuum, int64_t *did_diis);
 
+/* Autotuner (no counterpart in the reference): one eager sweep that times every
+ * contraction in each candidate configuration (64 x 64 or skinny tiles, split-K
+ * chunk, and in split mode int8 slices or DMMA) on scratch output, keeps the
+ * fastest per contraction for the later sweeps and restores the amplitudes, so
+ * tuning does not count as an iteration.  reps timed runs per candidate;
+ * *ms_default / *ms_tuned = summed per-contraction times before / after.
+ * Re-run after ccq_b200_set_precision to tune the other mode. */
+int ccq_b200_autotune(ccq_b200_ctx *ctx, int64_t reps, double *ms_default, double *ms_tuned);
+
 /* ---- learned warm start ---------------------------------------------------------
  * A per-amplitude multilayer perceptron (no counterpart in the reference, which
  * starts every solve from T = 0): y = w3 . tanh(W2 tanh(W1 x + b1) + b2) + b3 with
