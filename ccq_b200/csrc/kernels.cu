@@ -639,6 +639,121 @@ cudaError_t gett_f64_prepare() {
     return err;
 }
 
+// ---------------------------------------------------------------------------
+// Small-K GETT on the FP64 FMA pipe: for K of a few dozen the contraction is
+// bound by writing C (16-268 MB intermediates at 40 orbitals), not by the
+// products, and B200's FP64 FMA rate equals its DMMA rate.  One thread owns one
+// index f of the output's contiguous side ("F side": n when c_nfast, else m)
+// and BS indices of the other side, so every store of a warp covers 32
+// consecutive outputs; the F operand streams straight into registers, the S
+// operand is staged per K chunk in shared memory (scaled by alpha) and read by
+// broadcast.  Grouped launches loop over their segments.
+// ---------------------------------------------------------------------------
+constexpr int QT = 256, QKC = 16;
+
+template <int BS, bool GROUPED>
+__global__ void __launch_bounds__(QT, 2) gett_f64_smallk_kernel(GettArgs g, int fside, int skm) {
+    __shared__ __align__(16) double Ss[QKC][BS];
+    __shared__ int soffc[BS];
+    const int tid = threadIdx.x;
+    const int Fsz = fside ? g.N : g.M, Ssz = fside ? g.M : g.N;
+    const int f = blockIdx.x * QT + tid;
+    const int s0 = blockIdx.y * BS;
+    const bool fin = f < Fsz;
+    const int *offcs = fside ? g.offC_m : g.offC_n;
+    if (tid < BS) soffc[tid] = s0 + tid < Ssz ? __ldg(offcs + s0 + tid) : 0;
+    double acc[BS];
+#pragma unroll
+    for (int q = 0; q < BS; ++q) acc[q] = 0.0;
+    const int nseg = GROUPED ? g.nseg : 1;
+    for (int sg = 0; sg < nseg; ++sg) {
+        const double *A = g.A, *B = g.B;
+        const int *oam = g.offA_m, *oak = g.offA_k, *obn = g.offB_n, *obk = g.offB_k;
+        int K = g.K;
+        double alpha = g.alpha;
+        if (GROUPED) {
+            const GettSeg &q = g.segs[sg];
+            A = q.A;
+            B = q.B;
+            oam = q.offA_m;
+            oak = q.offA_k;
+            obn = q.offB_n;
+            obk = q.offB_k;
+            K = q.K;
+            alpha = q.alpha;
+        }
+        const double *F = fside ? B : A, *S = fside ? A : B;
+        const int *ofi = fside ? obn : oam, *ofk = fside ? obk : oak;
+        const int *osi = fside ? oam : obn, *osk = fside ? oak : obk;
+        const long long fb = fin ? (long long)__ldg(ofi + f) : 0;
+        for (int k0 = 0; k0 < K; k0 += QKC) {
+            const int kc = min(QKC, K - k0);
+            double fv[QKC];
+#pragma unroll
+            for (int k = 0; k < QKC; ++k) fv[k] = (fin && k < kc) ? __ldg(F + fb + __ldg(ofk + k0 + k)) : 0.0;
+            __syncthreads();  // the previous chunk's reads of Ss (and soffc) are done
+            for (int i = tid; i < QKC * BS; i += QT) {
+                const int k = skm ? i % QKC : i / BS;
+                const int q = skm ? i / QKC : i % BS;
+                double v = 0.0;
+                if (k < kc && s0 + q < Ssz) v = alpha * __ldg(S + (long long)__ldg(osi + s0 + q) + __ldg(osk + k0 + k));
+                Ss[k][q] = v;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < QKC; ++k) {
+                if (k < kc) {
+                    const double a = fv[k];
+#pragma unroll
+                    for (int q = 0; q < BS; q += 2) {
+                        const double2 b = *reinterpret_cast<const double2 *>(&Ss[k][q]);
+                        acc[q] += a * b.x;
+                        acc[q + 1] += a * b.y;
+                    }
+                }
+            }
+        }
+    }
+    if (!fin) return;
+    double *cf = g.C + __ldg((fside ? g.offC_n : g.offC_m) + f);
+    // beta = 1 updates add with reductions (concurrent writers of one intermediate)
+#pragma unroll
+    for (int q = 0; q < BS; ++q) {
+        if (s0 + q < Ssz) {
+            if (g.beta)
+                atomicAdd(cf + soffc[q], acc[q]);
+            else
+                cf[soffc[q]] = acc[q];
+        }
+    }
+}
+
+template <int BS>
+void launch_smallk_bs(const GettArgs &a, int fside, int skm, dim3 grid, cudaStream_t s) {
+    if (a.segs)
+        gett_f64_smallk_kernel<BS, true><<<grid, QT, 0, s>>>(a, fside, skm);
+    else
+        gett_f64_smallk_kernel<BS, false><<<grid, QT, 0, s>>>(a, fside, skm);
+}
+
+// false when the shape does not fit the launch (the caller takes the DMMA path)
+bool launch_smallk(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
+    const int fside = a.c_nfast ? 1 : 0;
+    const long long Fsz = fside ? a.N : a.M, Ssz = fside ? a.M : a.N;
+    const int bs = Ssz <= 8 ? 8 : Ssz <= 16 ? 16 : 32;
+    const long long gy = (Ssz + bs - 1) / bs, gx = (Fsz + QT - 1) / QT;
+    if (gy > 65535 || gx > 0x7fffffffLL) return false;
+    const int skm = fside ? a_kmajor : b_kmajor;
+    dim3 grid((unsigned)gx, (unsigned)gy, 1);
+    if (bs == 8)
+        launch_smallk_bs<8>(a, fside, skm, grid, s);
+    else if (bs == 16)
+        launch_smallk_bs<16>(a, fside, skm, grid, s);
+    else
+        launch_smallk_bs<32>(a, fside, skm, grid, s);
+    return true;
+}
+
 int gett_f64_family(long long M, long long N) {
     if (M <= 32 && M <= N) return 1;
     if (N <= 32 && N < M) return 2;
@@ -664,6 +779,7 @@ int gett_f64_kchunk(long long M, long long N, long long K) {
 }
 
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
+    if (a.tile == 3 && launch_smallk(a, a_kmajor, b_kmajor, s)) return;
     const int zsplit = a.segs ? 1 : std::max(1, (a.K + a.kchunk - 1) / a.kchunk);
     int fam = gett_f64_family(a.M, a.N);
     if (a.tile == 1) fam = 0;

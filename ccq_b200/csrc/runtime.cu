@@ -1686,8 +1686,8 @@ int ccq_b200_get_l(ccq_b200_ctx *c, double *l_vec, int64_t n) {
 
 // ---- autotuner ------------------------------------------------------------------
 // One eager sweep in which every contraction is timed in each candidate
-// configuration (tile family, split-K chunk, and in split mode int8 slices or
-// DMMA), writing into scratch so that the sweep's own data stay intact; the op
+// configuration (64 x 64 / skinny DMMA tiles or the small-K FMA kernel,
+// split-K chunk, and in split mode int8 slices or DMMA), writing into scratch so that the sweep's own data stay intact; the op
 // then runs once for real in the fastest configuration.  The amplitudes are
 // restored afterwards, so tuning does not count as an iteration.
 
@@ -1788,6 +1788,8 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
                         if (!dup) cand.push_back(t);
                     }
                 }
+                // small-K FMA kernel: whole K per launch
+                if (K <= 128) cand.push_back(TuneCfg{3, o.g.segs ? o.g.kchunk : (int)((K + 15) / 16 * 16), 0});
                 if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_capable(o.g) && !cur.split)
                     cand.push_back(TuneCfg{0, o.g.kchunk, 1});
                 if (c->precision == CCQ_B200_PREC_SPLIT && o.split && cur.split)
@@ -1833,6 +1835,23 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
     } catch (const std::exception &e) {
         return fail(Error(CCQ_B200_EINVAL, e.what()));
     }
+}
+
+int ccq_b200_force_tile(ccq_b200_ctx *c, int64_t tile) {
+    if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
+    if (tile < 0 || tile > 3) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..3"));
+    for (auto &o : c->plan.ops) {
+        if (o.kind != OP_GETT || o.g.K == 0) continue;
+        o.g.tile = (int)tile;
+        if (o.g.segs) continue;
+        // the small-K kernel takes the whole K range in one launch; the others the shape's split-K
+        o.g.kchunk = tile == 3 ? (o.g.K + 15) / 16 * 16 : gett_f64_kchunk(o.g.M, o.g.N, o.g.K);
+        o.zero_first = (o.g.K + o.g.kchunk - 1) / o.g.kchunk > 1 && o.beta == 0;
+    }
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
+    c->gexec = c->lgexec = nullptr;
+    return 0;
 }
 
 int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {

@@ -55,6 +55,7 @@ SIGNATURES = {
     'ccq_b200_get_l': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_set_precision': (C.c_int, [C.c_void_p, I64, I64]),
     'ccq_b200_autotune': (C.c_int, [C.c_void_p, I64, DP, DP]),
+    'ccq_b200_force_tile': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_use_graph': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), DP, DP]),
     'ccq_b200_timing': (C.c_int, [C.c_void_p, DP, DP]),
@@ -211,6 +212,10 @@ class Context:
         a, b = C.c_double(), C.c_double()
         _err(self._lib.ccq_b200_autotune(self.ptr, reps, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def force_tile(self, tile):
+        """Every contraction on one kernel family (0 shape default, 1 64x64, 2 skinny, 3 small-K)."""
+        _err(self._lib.ccq_b200_force_tile(self.ptr, tile))
 
     def set_precision(self, mode, nslices=4):
         _err(self._lib.ccq_b200_set_precision(self.ptr, mode, nslices))

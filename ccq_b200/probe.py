@@ -2,7 +2,7 @@
 
     python -m ccq_b200.probe egemm K1 K2 K3 [repeats]
     python -m ccq_b200.probe egemm_split K1 K2 K3 [slices]
-    python -m ccq_b200.probe sweep fp64|split OUTFILE [warm-up iterations]
+    python -m ccq_b200.probe sweep fp64|split OUTFILE [warm-up iterations] [0|1|2|3|tune]
     python -m ccq_b200.probe warmstart CCSDT|CCSDTQ NORB NEL [COUNT TRAIN EPOCHS]
 
 Runs ccq_b200_egemm (the FP64 GETT kernel) on random column-major operands;
@@ -49,12 +49,17 @@ def main(argv):
         prec = argv[1] if len(argv) > 1 else 'fp64'
         out = argv[2] if len(argv) > 2 else 'ops_profile.txt'
         warm = int(argv[3]) if len(argv) > 3 else 3
+        family = argv[4] if len(argv) > 4 else '0'   # kernel family to force (0..3) or 'tune'
         s = synth.system(synth.C2)
         d = s['dims']
         # a one-vector DIIS ring keeps the device footprint small for profiler captures
         ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CCSDT', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
                           s['v_bb'], diis_space=1)
         ctx.set_precision(lib.PREC_SPLIT if prec == 'split' else lib.PREC_FP64, 4)
+        if family == 'tune':
+            print('autotune (ms before, after):', ctx.autotune(3))
+        elif family != '0':
+            ctx.force_tile(int(family))
         for it in range(1, warm + 1):
             ctx.iterate(it)
         if os.path.exists(out):

@@ -145,13 +145,19 @@ int ccq_b200_iterate_async(ccq_b200_ctx *ctx, int64_t iter);
 int ccq_b200_iterate_wait(ccq_b200_ctx *ctx, double *e_cor, double *residuum, int64_t *did_diis);
 
 /* Autotuner (no counterpart in the reference): one eager sweep that times every
- * contraction in each candidate configuration (64 x 64 or skinny tiles, split-K
- * chunk, and in split mode int8 slices or DMMA) on scratch output, keeps the
+ * contraction in each candidate configuration (64 x 64 DMMA tiles, skinny DMMA
+ * tiles, the small-K FMA kernel; split-K chunk; in split mode int8 slices or
+ * DMMA) on scratch output, keeps the
  * fastest per contraction for the later sweeps and restores the amplitudes, so
  * tuning does not count as an iteration.  reps timed runs per candidate;
  * *ms_default / *ms_tuned = summed per-contraction times before / after.
  * Re-run after ccq_b200_set_precision to tune the other mode. */
 int ccq_b200_autotune(ccq_b200_ctx *ctx, int64_t reps, double *ms_default, double *ms_tuned);
+/* Pins every contraction to one GETT kernel family: 0 = by shape, 1 = 64 x 64
+ * DMMA tiles, 2 = skinny DMMA tiles (where one side is <= 32), 3 = small-K
+ * FMA kernel.  A family that does not fit a shape falls back to the shape's
+ * default.  For tests and experiments; ccq_b200_autotune picks per contraction. */
+int ccq_b200_force_tile(ccq_b200_ctx *ctx, int64_t tile);
 
 /* ---- learned warm start ---------------------------------------------------------
  * A per-amplitude multilayer perceptron (no counterpart in the reference, which

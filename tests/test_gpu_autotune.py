@@ -70,3 +70,39 @@ def test_tuned_solve_matches_untuned(prec):
         ctx.close()
     assert abs(res[True].e_cor - res[False].e_cor) < 1e-10
     assert abs(res[True].iterations - res[False].iterations) <= 1
+
+
+@pytest.mark.parametrize('tile', [1, 2, 3])
+@pytest.mark.parametrize('method,n,oa,ob', [('CCSD', 7, 3, 2), ('CCSDT', 7, 3, 2)])
+def test_forced_kernel_family_matches_oracle(tile, method, n, oa, ob, plan_text):
+    """Every contraction on one GETT family (64 x 64 DMMA, skinny DMMA, small-K FMA)."""
+    s = random_system(n, oa, ob, seed=21)
+    ctx = make_ctx(s, method, shift=0.05)
+    ctx.force_tile(tile)
+    bc = BlockCC(plan_text(method, False), s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], s['dims'], method,
+                 shift=0.05)
+    t, _ = random_t(s['dims'], seed=5, scale=0.03, nmax=3 if method == 'CCSDT' else 2)
+    ctx.set_t(t)
+    tc = t.copy()
+    for _ in range(2):
+        ctx.update()
+        bc.update(tc)
+    np.testing.assert_allclose(ctx.get_t(), tc, atol=1e-12, rtol=0)
+    ctx.close()
+
+
+def test_small_k_kernel_on_large_views():
+    """20 orbitals: several 256-wide F tiles and 32-wide S tiles per contraction, grouped launches."""
+    s = synth.system(synth.SynthSpec(20, 8, 40, 0.05, 3))
+    d = s['dims']
+    t, _ = random_t(d, seed=6, scale=0.02, nmax=3)
+    out = {}
+    for tile in (0, 3):
+        ctx = make_ctx(s, 'CCSDT')
+        ctx.force_tile(tile)
+        ctx.set_t(t)
+        for _ in range(2):
+            ctx.update()
+        out[tile] = ctx.get_t()
+        ctx.close()
+    np.testing.assert_allclose(out[3], out[0], atol=1e-12, rtol=0)
