@@ -11,7 +11,10 @@ New keys of this engine are prefixed ``gpu_``: ``gpu_precision`` (fp64 |
 split), ``gpu_slices`` (int8 slices per operand), ``gpu_fp64_finish`` (|dE|
 below which the split mode hands over to FP64), ``gpu_graph`` (replay each
 sweep as one CUDA graph), ``gpu_autotune`` (time every contraction's tile and
-split-K candidates once before the first iteration and keep the fastest).
+split-K candidates once before the first iteration and keep the fastest),
+``gpu_checkpoint_every`` (write the checkpoint every N iterations).  The
+reference's ``fcidump``, ``restart`` and ``output_bin`` keys are served:
+``restart`` resumes t_vec, T4 and the DIIS ring from ``output_bin``.
 """
 from __future__ import annotations
 
@@ -46,6 +49,9 @@ class Config:
     calc_type: str = ''
     onebody: str = 'onebody.inp'
     twobody: str = 'twobody.inp'
+    fcidump: str = ''
+    bin_file: str = ''
+    gpu_checkpoint_every: int = 0
     keep_bin: bool = True
     num_threads: int = 1
     restart: bool = False
@@ -71,6 +77,12 @@ class Config:
         self.occ_b = self.occ_a - _ftrunc_div(self.mult - 1, 2)
         self.orbs = (self.nel + self.nvirt) // 2
         return self
+
+    def bin_path(self):
+        """Checkpoint file: output_bin, else tvec_<label>.bin (tvec.bin without a label)."""
+        if self.bin_file:
+            return self.bin_file
+        return f'tvec_{self.label}.bin' if self.label else 'tvec.bin'
 
     def calc_macros(self):
         ct = self.calc_type
@@ -146,8 +158,14 @@ def _apply(cfg, key, val):
         cfg.onebody = val
     elif key == 'twobody':
         cfg.twobody = val
+    elif key == 'fcidump':
+        cfg.fcidump = val
     elif key == 'keep_bin':
         cfg.keep_bin = _logical(val)
+    elif key == 'output_bin':
+        cfg.bin_file = val
+    elif key == 'gpu_checkpoint_every':
+        cfg.gpu_checkpoint_every = int(val)
     elif key == 'num_threads':
         cfg.num_threads = int(val)
     elif key == 'gpu_precision':
@@ -164,6 +182,16 @@ def _apply(cfg, key, val):
         cfg.gpu_autotune = _logical(val)
     else:
         cfg.extra[key] = val
+
+
+def apply_fcidump(cfg, path):
+    """FCIDUMP override (``src/parser.f90:168-169``, ``get_fcidump`` ``:260-313``):
+    nel = NELEC, nvirt = 2 NORB - NELEC, then the derived sizes again."""
+    from . import lib
+    norb, nelec = lib.fcidump_header(path)
+    cfg.nel = nelec
+    cfg.nvirt = 2 * norb - nelec
+    return cfg.process()
 
 
 def format_config(cfg):

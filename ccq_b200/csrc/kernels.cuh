@@ -16,6 +16,9 @@
 
 namespace ccqb {
 
+// message returned by ccq_b200_last_error() on this thread
+void set_last_error(const char *msg);
+
 constexpr int MAXR = 8;        // max tensor rank (T4 blocks)
 constexpr int MAX_TERMS = 65536; // max views gathered by one assemble
 

@@ -45,6 +45,12 @@ int fail(const Error &e) {
     return e.code;
 }
 
+}  // namespace
+
+void ccqb::set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
+namespace {
+
 // ---------------------------------------------------------------------------
 // plan text
 // ---------------------------------------------------------------------------
@@ -1419,6 +1425,227 @@ int ccq_b200_block(ccq_b200_ctx *c, const char *name, double *host, int64_t n, i
                            to_device ? (const void *)host : (const void *)it->second.ptr, sizeof(double) * n,
                            to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+// ---- checkpoint / restart -------------------------------------------------------
+// File: "CCQB200C" | int64 version, froz, oa, ob, va, vb, rhf, ds, t_dev, vec_size,
+// nblocks, with_ring, iteration | double state[8] | char calc_type[32] | t_vec
+// (t_dev doubles) | per amplitude block outside t_vec: char name[8], int64 numel,
+// doubles | ring ((ds+1) vec_size doubles) when with_ring | "CKPTEND!" int64 bytes.
+// Copies go through one pinned staging buffer in 64 MiB pieces.
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'C', 'C', 'Q', 'B', '2', '0', '0', 'C'};
+constexpr char kCkptEnd[8] = {'C', 'K', 'P', 'T', 'E', 'N', 'D', '!'};
+constexpr long long kCkptVersion = 1;
+constexpr size_t kStage = 64ull << 20;
+
+struct CkptHead {
+    long long version, froz, oa, ob, va, vb, rhf, ds, t_dev, vec_size, nblocks, with_ring, iteration;
+    double state[8];
+    char calc_type[32];
+};
+
+std::vector<std::pair<std::string, const DevBuf *>> outside_blocks(const ccq_b200_ctx *c) {
+    std::vector<std::pair<std::string, const DevBuf *>> out;
+    for (auto &b : c->plan.bufs)
+        if (b.kind == "amp") {
+            const DevBuf &d = c->bufs.at(b.name);
+            if (d.ptr && (d.ptr < c->tvec || d.ptr >= c->tvec + c->t_dev)) out.push_back({b.name, &d});
+        }
+    return out;
+}
+
+struct Pinned {
+    void *p = nullptr;
+    Pinned() { CK(cudaMallocHost(&p, kStage)); }
+    ~Pinned() { cudaFreeHost(p); }
+};
+
+void write_all(FILE *f, const void *p, size_t n, long long &total) {
+    if (n && fwrite(p, 1, n, f) != n) throw Error(CCQ_B200_EINVAL, "checkpoint: write failed");
+    total += (long long)n;
+}
+
+void read_all(FILE *f, void *p, size_t n) {
+    if (n && fread(p, 1, n, f) != n) throw Error(CCQ_B200_EINVAL, "checkpoint: file truncated");
+}
+
+void dev_to_file(ccq_b200_ctx *c, FILE *f, const double *src, long long n, Pinned &st, long long &total) {
+    const long long per = (long long)(kStage / sizeof(double));
+    for (long long o = 0; o < n; o += per) {
+        const long long k = std::min(per, n - o);
+        CK(cudaMemcpyAsync(st.p, src + o, sizeof(double) * k, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        write_all(f, st.p, sizeof(double) * k, total);
+    }
+}
+
+void file_to_dev(ccq_b200_ctx *c, FILE *f, double *dst, long long n, Pinned &st) {
+    const long long per = (long long)(kStage / sizeof(double));
+    for (long long o = 0; o < n; o += per) {
+        const long long k = std::min(per, n - o);
+        read_all(f, st.p, sizeof(double) * k);
+        CK(cudaMemcpyAsync(dst + o, st.p, sizeof(double) * k, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+}
+
+CkptHead read_head(FILE *f) {
+    char magic[8];
+    read_all(f, magic, 8);
+    if (memcmp(magic, kCkptMagic, 8) != 0) throw Error(CCQ_B200_EINVAL, "checkpoint: not a checkpoint file");
+    CkptHead h;
+    read_all(f, &h, sizeof(h));
+    if (h.version != kCkptVersion) throw Error(CCQ_B200_EINVAL, "checkpoint: unknown version");
+    h.calc_type[31] = '\0';
+    return h;
+}
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() {
+        if (f) fclose(f);
+    }
+};
+
+}  // namespace
+
+int ccq_b200_checkpoint_save(ccq_b200_ctx *c, const char *path, int64_t with_ring, int64_t iteration,
+                             const double *state) {
+    try {
+        if (!c || !path) throw Error(CCQ_B200_EINVAL, "checkpoint_save: null argument");
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "checkpoint_save: an iteration is pending");
+        CK(cudaSetDevice(c->device));
+        CK(cudaStreamSynchronize(c->stream));
+        auto blocks = outside_blocks(c);
+        CkptHead h{};
+        h.version = kCkptVersion;
+        h.froz = c->froz;
+        h.oa = c->oa;
+        h.ob = c->ob;
+        h.va = c->va;
+        h.vb = c->vb;
+        h.rhf = c->rhf;
+        h.ds = c->ds;
+        h.t_dev = c->t_dev;
+        h.vec_size = c->vec_size;
+        h.nblocks = (long long)blocks.size();
+        h.with_ring = with_ring ? 1 : 0;
+        h.iteration = iteration;
+        for (int k = 0; k < 8; ++k) h.state[k] = state ? state[k] : 0.0;
+        snprintf(h.calc_type, sizeof(h.calc_type), "%s", c->calc_type.c_str());
+        // write next to the target and rename at the end: a crash never leaves a torn checkpoint
+        const std::string tmp = std::string(path) + ".part";
+        FileCloser fc{fopen(tmp.c_str(), "wb")};
+        if (!fc.f) throw Error(CCQ_B200_EINVAL, std::string("checkpoint_save: cannot open ") + tmp);
+        Pinned st;
+        long long total = 0;
+        write_all(fc.f, kCkptMagic, 8, total);
+        write_all(fc.f, &h, sizeof(h), total);
+        dev_to_file(c, fc.f, c->tvec, c->t_dev, st, total);
+        for (auto &b : blocks) {
+            char nm[8] = {0};
+            snprintf(nm, sizeof(nm), "%s", b.first.c_str());
+            long long n = b.second->numel;
+            write_all(fc.f, nm, 8, total);
+            write_all(fc.f, &n, sizeof(n), total);
+            dev_to_file(c, fc.f, b.second->ptr, n, st, total);
+        }
+        if (with_ring) dev_to_file(c, fc.f, c->ring, (long long)(c->ds + 1) * c->vec_size, st, total);
+        write_all(fc.f, kCkptEnd, 8, total);
+        total += (long long)sizeof(total);
+        write_all(fc.f, &total, sizeof(total), total);
+        if (fclose(fc.f) != 0) {
+            fc.f = nullptr;
+            throw Error(CCQ_B200_EINVAL, "checkpoint_save: close failed");
+        }
+        fc.f = nullptr;
+        if (rename(tmp.c_str(), path) != 0) throw Error(CCQ_B200_EINVAL, "checkpoint_save: rename failed");
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_checkpoint_info(const char *path, int64_t *dims, int64_t *iteration, int64_t *with_ring,
+                             double *state, char *calc_type, int64_t len) {
+    try {
+        if (!path) throw Error(CCQ_B200_EINVAL, "checkpoint_info: null path");
+        FileCloser fc{fopen(path, "rb")};
+        if (!fc.f) throw Error(CCQ_B200_EINVAL, std::string("Restart file not found: ") + path);
+        CkptHead h = read_head(fc.f);
+        if (dims) {
+            const long long d[9] = {h.froz, h.oa, h.ob, h.va, h.vb, h.rhf, h.ds, h.t_dev, h.vec_size};
+            for (int k = 0; k < 9; ++k) dims[k] = d[k];
+        }
+        if (iteration) *iteration = h.iteration;
+        if (with_ring) *with_ring = h.with_ring;
+        if (state)
+            for (int k = 0; k < 8; ++k) state[k] = h.state[k];
+        if (calc_type && len > 0) snprintf(calc_type, (size_t)len, "%s", h.calc_type);
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_checkpoint_load(ccq_b200_ctx *c, const char *path, int64_t *iteration, double *state,
+                             int64_t *with_ring) {
+    try {
+        if (!c || !path) throw Error(CCQ_B200_EINVAL, "checkpoint_load: null argument");
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "checkpoint_load: an iteration is pending");
+        CK(cudaSetDevice(c->device));
+        FileCloser fc{fopen(path, "rb")};
+        if (!fc.f) throw Error(CCQ_B200_EINVAL, std::string("Restart file not found: ") + path);
+        CkptHead h = read_head(fc.f);
+        auto blocks = outside_blocks(c);
+        if (std::string(h.calc_type) != c->calc_type || h.froz != c->froz || h.oa != c->oa || h.ob != c->ob ||
+            h.va != c->va || h.vb != c->vb || h.rhf != c->rhf || h.t_dev != c->t_dev || h.vec_size != c->vec_size ||
+            h.nblocks != (long long)blocks.size())
+            throw Error(CCQ_B200_EINVAL, "checkpoint_load: the file belongs to another system or method");
+        if (h.with_ring && h.ds != c->ds) throw Error(CCQ_B200_EINVAL, "checkpoint_load: diis_space differs");
+        // the size trailer first: a truncated file is refused before any device state changes
+        long long expect = 8 + (long long)sizeof(CkptHead) + 8 * h.t_dev + 16;   // magic, head, t_vec, trailer
+        for (auto &b : blocks) expect += 16 + 8 * b.second->numel;
+        if (h.with_ring) expect += 8 * (h.ds + 1) * h.vec_size;
+        if (fseek(fc.f, 0, SEEK_END) != 0 || ftell(fc.f) != expect)
+            throw Error(CCQ_B200_EINVAL, "checkpoint_load: file size does not match its header");
+        if (fseek(fc.f, expect - 16, SEEK_SET) != 0) throw Error(CCQ_B200_EINVAL, "checkpoint_load: seek failed");
+        char endm[8];
+        long long total = 0;
+        read_all(fc.f, endm, 8);
+        read_all(fc.f, &total, 8);
+        if (memcmp(endm, kCkptEnd, 8) != 0 || total != expect) throw Error(CCQ_B200_EINVAL, "checkpoint_load: bad trailer");
+        if (fseek(fc.f, 8 + (long)sizeof(CkptHead), SEEK_SET) != 0)
+            throw Error(CCQ_B200_EINVAL, "checkpoint_load: seek failed");
+        Pinned st;
+        file_to_dev(c, fc.f, c->tvec, c->t_dev, st);
+        for (auto &b : blocks) {
+            char nm[8];
+            long long n = 0;
+            read_all(fc.f, nm, 8);
+            read_all(fc.f, &n, 8);
+            nm[7] = '\0';
+            if (b.first != nm || n != b.second->numel) throw Error(CCQ_B200_EINVAL, "checkpoint_load: block mismatch");
+            file_to_dev(c, fc.f, b.second->ptr, n, st);
+        }
+        if (h.with_ring) file_to_dev(c, fc.f, c->ring, (long long)(h.ds + 1) * h.vec_size, st);
+        if (iteration) *iteration = h.iteration;
+        if (with_ring) *with_ring = h.with_ring;
+        if (state)
+            for (int k = 0; k < 8; ++k) state[k] = h.state[k];
         return 0;
     } catch (const Error &e) {
         return fail(e);

@@ -55,11 +55,27 @@ def solve_cc(ctx, cfg, out=print, precision=None):
     en_cor = 0.0
     failed = False
     hist = []
+    it0 = 0
+    fp64_iters = 0
+    if cfg.restart:
+        # continue from the checkpoint (src/solve_cc.f90:56-60 prints the restart energy; its
+        # T1-T3 restart starts from zero, here the saved amplitudes and DIIS ring are resumed)
+        path = cfg.bin_path()
+        if not os.path.exists(path):
+            raise ValueError('CONFIGURATION ERROR: Restart file not found')
+        it_saved, state, with_ring = ctx.load_checkpoint(path)
+        out(f"  {'Restart correlation energy':>27}  {ctx.energy():16.10f}\n")
+        if with_ring:
+            # the ring is resumed too: iteration numbering, DIIS schedule and convergence history go on
+            it0 = it_saved
+            en_cor, conv, fp64_iters = state[0], list(state[1:4]), int(state[4])
+            if split and not state[5]:
+                split = False
+                ctx.set_precision(lib.PREC_FP64, cfg.gpu_slices)
     prev = time.time()
     print_iter_head(out)
-    it = 0
-    fp64_iters = 0
-    for it in range(1, cfg.max_iter + 1):
+    it = it0
+    for it in range(it0 + 1, cfg.max_iter + 1):
         e_new, res, did = ctx.iterate(it)
         st = ctx.stats()
         diff = en_cor - e_new
@@ -82,6 +98,8 @@ def solve_cc(ctx, cfg, out=print, precision=None):
             split = False
             ctx.set_precision(lib.PREC_FP64, cfg.gpu_slices)
             out('      FP64 finish')
+        if cfg.gpu_checkpoint_every and it % cfg.gpu_checkpoint_every == 0:
+            ctx.save_checkpoint(cfg.bin_path(), it, solver_state(en_cor, conv, fp64_iters, split))
         if not split and fp64_iters >= 3 and all(abs(c) < cfg.tol for c in conv):
             break
         if math.isnan(e_new):
@@ -91,7 +109,13 @@ def solve_cc(ctx, cfg, out=print, precision=None):
         if it == cfg.max_iter:
             out(f'FAILED TO CONVERGE IN {cfg.max_iter} ITERATIONS. KEEPING LAST T VECTOR.')
             failed = True
-    return Result(e_cor=en_cor, iterations=it, failed=failed, history=hist)
+    return Result(e_cor=en_cor, iterations=it, failed=failed, history=hist,
+                  state=solver_state(en_cor, conv, fp64_iters, split))
+
+
+def solver_state(en_cor, conv, fp64_iters, split):
+    """The host half of a checkpoint: energy, last three dE, FP64 iterations, split flag."""
+    return [en_cor, conv[0], conv[1], conv[2], float(fp64_iters), float(split)]
 
 
 def solve_lcc(ctx, cfg, e_cor, out=print):
@@ -142,8 +166,11 @@ def print_cct3(out, e_ref, e_cor, e23):
 def load_system(cfg, base_dir='.'):
     def path(p):
         return p if os.path.isabs(p) else os.path.join(base_dir, p)
-    e1 = I.read_onebody(path(cfg.onebody), cfg.orbs)
-    e2, enuc = I.read_twobody(path(cfg.twobody), cfg.orbs)
+    if cfg.fcidump:
+        e1, e2, enuc = I.read_fcidump(path(cfg.fcidump), cfg.orbs)
+    else:
+        e1 = I.read_onebody(path(cfg.onebody), cfg.orbs)
+        e2, enuc = I.read_twobody(path(cfg.twobody), cfg.orbs)
     fa, fb = I.fock(e1, e2, cfg.occ_a, cfg.occ_b)
     vaa, vab, vbb = I.spin_blocks(e2, cfg.froz)
     eref = I.hf_energy(e1, e2, cfg.occ_a, cfg.occ_b) + enuc
@@ -151,7 +178,13 @@ def load_system(cfg, base_dir='.'):
 
 
 def run(input_path, out=print, base_dir='.'):
-    cfg = cfgmod.parse(input_path).calc_macros()
+    cfg = cfgmod.parse(input_path)
+    if cfg.fcidump:
+        fp = cfg.fcidump if os.path.isabs(cfg.fcidump) else os.path.join(base_dir, cfg.fcidump)
+        if not os.path.exists(fp):
+            raise ValueError('CONFIGURATION ERROR: FCIDUMP file not found')
+        cfgmod.apply_fcidump(cfg, fp)
+    cfg.calc_macros()
     sysd = load_system(cfg, base_dir)
     out('Calculation parameters: ' + cfgmod.format_config(cfg))
     out(f"  Reference energy {sysd['e_ref']:.12f}")
@@ -160,8 +193,14 @@ def run(input_path, out=print, base_dir='.'):
     ctx = lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, cfg.calc_type, sysd['f_a'], sysd['f_b'],
                       sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
                       diis_space=cfg.diis_space)
+    cfg.bin_file = cfg.bin_path()
+    if not os.path.isabs(cfg.bin_file):
+        cfg.bin_file = os.path.join(base_dir, cfg.bin_file)
     try:
         r = solve_cc(ctx, cfg, out)
+        if cfg.keep_bin:
+            # final amplitudes and ring: restart= continues an unconverged run exactly
+            ctx.save_checkpoint(cfg.bin_path(), r.iterations, r.state)
         if cfg.calc_type == 'CR-CC(2,3)':
             # hbar2 + solve_lcc + crcc23 (src/calc_driver.f90:55-73)
             r.left = solve_lcc(ctx, cfg, r.e_cor, out)

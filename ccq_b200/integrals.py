@@ -3,6 +3,8 @@
 Mirrors the reference's input side so that a ccq input deck runs unchanged:
   * ``read_onebody``   <- ``load_e1int``  (``src/integrals.f90:11-43``)
   * ``read_twobody``   <- ``load_e2int``  (``src/integrals.f90:45-91``)
+  * ``read_fcidump``   <- ``load_fcidump`` (``src/integrals.f90:93-210``), through
+    the library's native reader (``ccq_b200_fcidump_read``)
   * ``spin_blocks``    <- ``load_ints``   (``src/integrals.f90:212-297``)
   * ``fock``           <- ``gen_fock_operator`` (``src/integrals.f90:300-364``)
   * ``hf_energy``      <- ``calc_hf_energy`` (``src/energy.f90:49-101``)
@@ -70,6 +72,47 @@ def read_twobody(path, orbs):
     i, a, j, b = idx[:, 0] - 1, idx[:, 1] - 1, idx[:, 2] - 1, idx[:, 3] - 1
     e2[i, j, a, b] = vals
     return e2, en_repul
+
+
+def read_fcidump(path, orbs):
+    """(e1int, e2int, E_nuc) from the unique integrals of a FCIDUMP file.
+
+    Orbitals are renumbered by ascending orbital energy and every (ia|jb) is
+    expanded to its eight permutations, as ``load_fcidump`` does.
+    """
+    from . import lib
+    return lib.fcidump_read(path, orbs)
+
+
+def write_fcidump(path, e1, e2, en_repul=0.0, nelec=0, eps=None, order=None, thresh=0.0):
+    """FCIDUMP with the unique integrals (i >= a, j >= b, (ia) >= (jb)) of e1int/e2int.
+
+    ``order`` relabels orbital p as ``order[p] + 1`` in the file (the reader
+    undoes it through the orbital-energy records ``eps``).
+    """
+    n = e1.shape[0]
+    lab = (np.arange(n) if order is None else np.asarray(order)) + 1
+    lines = [f" &FCI NORB={n:3d},NELEC={nelec:3d},MS2=0,", "  ORBSYM=" + ",".join("1" * n) + ",", "  ISYM=1,",
+             " &END"]
+    for i in range(n):
+        for a in range(i + 1):
+            for j in range(n):
+                for b in range(j + 1):
+                    if i * (i + 1) // 2 + a < j * (j + 1) // 2 + b:
+                        continue
+                    v = e2[i, j, a, b]
+                    if abs(v) > thresh:
+                        lines.append(f"{v: .16E} {lab[i]:4d} {lab[a]:4d} {lab[j]:4d} {lab[b]:4d}")
+    for i in range(n):
+        for a in range(i + 1):
+            if abs(e1[i, a]) > thresh:
+                lines.append(f"{e1[i, a]: .16E} {lab[i]:4d} {lab[a]:4d}    0    0")
+    if eps is not None:
+        for i in range(n):
+            lines.append(f"{eps[i]: .16E} {lab[i]:4d}    0    0    0")
+    lines.append(f"{en_repul: .16E}    0    0    0    0")
+    with open(path, 'w') as fh:
+        fh.write("\n".join(lines) + "\n")
 
 
 def write_onebody(path, e1):

@@ -63,6 +63,13 @@ SIGNATURES = {
     'ccq_b200_profile_get': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
     'ccq_b200_free': (C.c_int, [C.c_void_p]),
     'ccq_b200_last_error': (C.c_int, [C.c_char_p, I64]),
+    'ccq_b200_checkpoint_save': (C.c_int, [C.c_void_p, C.c_char_p, I64, I64, DP]),
+    'ccq_b200_checkpoint_load': (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(I64), DP, C.POINTER(I64)]),
+    'ccq_b200_checkpoint_info': (C.c_int, [C.c_char_p, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), DP,
+                                           C.c_char_p, I64]),
+    'ccq_b200_fcidump_header': (C.c_int, [C.c_char_p, C.POINTER(I64), C.POINTER(I64)]),
+    'ccq_b200_fcidump_read': (C.c_int, [C.c_char_p, I64, DP, DP, DP]),
+    'ccq_b200_fcidump_read_device': (C.c_int, [C.c_char_p, I64, DP, C.c_void_p, DP, C.c_void_p]),
 }
 
 
@@ -90,6 +97,47 @@ def _err(code):
 
 def _p(a):
     return a.ctypes.data_as(DP)
+
+
+def fcidump_header(path):
+    """(NORB, NELEC) of a FCIDUMP header (-1 for a key that is absent)."""
+    lib = load()
+    n, e = I64(), I64()
+    _err(lib.ccq_b200_fcidump_header(os.fsencode(path), C.byref(n), C.byref(e)))
+    return n.value, e.value
+
+
+def fcidump_read(path, norb):
+    """e1int[i, a], e2int[i, j, a, b] = <ij|ab> (index meaning of the reference's arrays), E_nuc."""
+    lib = load()
+    e1 = np.zeros((norb, norb), order='F')
+    e2 = np.zeros((norb, norb, norb, norb), order='F')
+    en = C.c_double()
+    _err(lib.ccq_b200_fcidump_read(os.fsencode(path), norb, _p(e1), _p(e2), C.byref(en)))
+    return np.ascontiguousarray(e1), np.ascontiguousarray(e2), en.value
+
+
+def fcidump_read_device(path, norb, e2_dev_ptr, stream=0):
+    """As fcidump_read, with e2int (Fortran order, norb^4 doubles) expanded into device memory."""
+    lib = load()
+    e1 = np.zeros((norb, norb), order='F')
+    en = C.c_double()
+    _err(lib.ccq_b200_fcidump_read_device(os.fsencode(path), norb, _p(e1), C.c_void_p(e2_dev_ptr), C.byref(en),
+                                          C.c_void_p(stream)))
+    return np.ascontiguousarray(e1), en.value
+
+
+def checkpoint_info(path):
+    """Header of a checkpoint: dict(calc_type, dims, iteration, with_ring, state)."""
+    lib = load()
+    dims = (I64 * 9)()
+    it, ring = I64(), I64()
+    st = np.zeros(8)
+    buf = C.create_string_buffer(32)
+    _err(lib.ccq_b200_checkpoint_info(os.fsencode(path), dims, C.byref(it), C.byref(ring), _p(st), buf, 32))
+    names = ('froz', 'oa', 'ob', 'va', 'vb', 'rhf', 'diis_space', 't_dev', 'vec_size')
+    return dict(calc_type=buf.value.decode(), dims=dict(zip(names, list(dims))), iteration=it.value,
+                with_ring=bool(ring.value), state=st)
 
 
 def egemm(k1, k2, k3, A, B):
@@ -216,6 +264,20 @@ class Context:
     def force_tile(self, tile):
         """Every contraction on one kernel family (0 shape default, 1 64x64, 2 skinny, 3 small-K)."""
         _err(self._lib.ccq_b200_force_tile(self.ptr, tile))
+
+    def save_checkpoint(self, path, iteration=0, state=None, with_ring=True):
+        """Resident t_vec, T4 blocks and (with_ring) the DIIS ring to ``path``."""
+        st = np.zeros(8)
+        if state is not None:
+            st[:len(state)] = state
+        _err(self._lib.ccq_b200_checkpoint_save(self.ptr, os.fsencode(path), int(with_ring), iteration, _p(st)))
+
+    def load_checkpoint(self, path):
+        """Restores a checkpoint; returns (iteration, state[8], with_ring)."""
+        it, ring = I64(), I64()
+        st = np.zeros(8)
+        _err(self._lib.ccq_b200_checkpoint_load(self.ptr, os.fsencode(path), C.byref(it), _p(st), C.byref(ring)))
+        return it.value, st, bool(ring.value)
 
     def set_precision(self, mode, nslices=4):
         _err(self._lib.ccq_b200_set_precision(self.ptr, mode, nslices))

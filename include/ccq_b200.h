@@ -159,6 +159,39 @@ int ccq_b200_autotune(ccq_b200_ctx *ctx, int64_t reps, double *ms_default, doubl
  * default.  For tests and experiments; ccq_b200_autotune picks per contraction. */
 int ccq_b200_force_tile(ccq_b200_ctx *ctx, int64_t tile);
 
+/* ---- checkpoint / restart ------------------------------------------------
+ * The reference's restart (src/solve_cc.f90:56-60, src/utils/cc_utils.f90:89-168)
+ * keeps only the T4 files and restarts T1-T3 from zero.  Here a checkpoint
+ * holds the resident t_vec, the amplitude blocks kept outside it (T4) and,
+ * with with_ring, the DIIS ring, so that a solve continued from it follows
+ * the uninterrupted trajectory.  iteration and state[8] are the caller's
+ * solver state (iteration number, energy, convergence history), stored
+ * as given.  checkpoint_load refuses a file of another system, method or
+ * diis_space, and a truncated file, before touching device state.
+ * checkpoint_info reads the header: dims = froz, oa, ob, va, vb, rhf,
+ * diis_space, t_dev, vec_size. */
+int ccq_b200_checkpoint_save(ccq_b200_ctx *ctx, const char *path, int64_t with_ring, int64_t iteration,
+                             const double *state);
+int ccq_b200_checkpoint_load(ccq_b200_ctx *ctx, const char *path, int64_t *iteration, double *state,
+                             int64_t *with_ring);
+int ccq_b200_checkpoint_info(const char *path, int64_t *dims, int64_t *iteration, int64_t *with_ring,
+                             double *state, char *calc_type, int64_t len);
+
+/* ---- FCIDUMP integrals ---------------------------------------------------
+ * Replaces get_fcidump (src/parser.f90:260-313) and load_fcidump
+ * (src/integrals.f90:93-210).  fcidump_header: NORB and NELEC of the header
+ * (-1 when absent; the reference then sets nel = NELEC, nvirt = 2 NORB - NELEC).
+ * fcidump_read: e1int(norb,norb) and e2int(norb,norb,norb,norb), Fortran order,
+ * e2int(i,j,a,b) = <ij|ab> = (ia|jb), from the unique integrals of the file
+ * (8-fold permutational expansion, orbitals renumbered by ascending orbital
+ * energy, later records overwrite earlier ones), *enuc = nuclear repulsion.
+ * fcidump_read_device: the same with e2int in device memory, expanded on the
+ * GPU (e1int stays a host array). */
+int ccq_b200_fcidump_header(const char *path, int64_t *norb, int64_t *nelec);
+int ccq_b200_fcidump_read(const char *path, int64_t norb, double *e1, double *e2, double *enuc);
+int ccq_b200_fcidump_read_device(const char *path, int64_t norb, double *e1, double *e2_dev, double *enuc,
+                                 void *stream);
+
 /* ---- learned warm start ---------------------------------------------------------
  * A per-amplitude multilayer perceptron (no counterpart in the reference, which
  * starts every solve from T = 0): y = w3 . tanh(W2 tanh(W1 x + b1) + b2) + b3 with
