@@ -103,8 +103,9 @@ __device__ __forceinline__ void load_tile(double *S, const double *base, const i
     }
 }
 
-// K loop of one contraction term over [kbeg, kend): 2-stage cp.async pipeline.
-template <bool AK, bool BKM>
+// K loop of one contraction term over [kbeg, kend): NST-stage cp.async pipeline
+// (As and Bs hold NST tiles each; one commit group per K tile, empty past the end).
+template <bool AK, bool BKM, int NST>
 __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As, double *Bs, const double *A,
                                               const double *B,
                                               const int *offA_m, const int *offA_k, const int *offB_n,
@@ -132,22 +133,25 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As
         offb[0] = n < N ? __ldg(offB_n + n) : 0;
     }
     const int ntiles = kend > kbeg ? (kend - kbeg + BKT - 1) / BKT : 0;
-    if (ntiles > 0) {
-        load_tile<AK>(As, A, offa, offA_k, m0, M, kbeg, kend, tid, va);
-        load_tile<BKM>(Bs, B, offb, offB_k, n0, N, kbeg, kend, tid, vb);
+#pragma unroll
+    for (int q = 0; q < NST - 1; ++q) {
+        if (q < ntiles) {
+            load_tile<AK>(As + q * TILE, A, offa, offA_k, m0, M, kbeg + q * BKT, kend, tid, va);
+            load_tile<BKM>(Bs + q * TILE, B, offb, offB_k, n0, N, kbeg + q * BKT, kend, tid, vb);
+        }
         cp_async_commit();
     }
     for (int t = 0; t < ntiles; ++t) {
-        const int st = t & 1;
-        if (t + 1 < ntiles) {
-            int k0 = kbeg + (t + 1) * BKT;
-            load_tile<AK>(As + (st ^ 1) * TILE, A, offa, offA_k, m0, M, k0, kend, tid, va);
-            load_tile<BKM>(Bs + (st ^ 1) * TILE, B, offb, offB_k, n0, N, k0, kend, tid, vb);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+        const int st = t % NST;
+        // refill the stage computed in the previous step (released by its trailing barrier)
+        const int tn = t + NST - 1;
+        if (tn < ntiles) {
+            const int sn = tn % NST;
+            load_tile<AK>(As + sn * TILE, A, offa, offA_k, m0, M, kbeg + tn * BKT, kend, tid, va);
+            load_tile<BKM>(Bs + sn * TILE, B, offb, offB_k, n0, N, kbeg + tn * BKT, kend, tid, vb);
         }
+        cp_async_commit();
+        cp_async_wait<NST - 1>();   // tile t has landed
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < BKT; kk += 4) {
@@ -168,11 +172,11 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As
     }
 }
 
-template <bool AK, bool BKM, bool GROUPED>
+template <bool AK, bool BKM, bool GROUPED, int NST>
 __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
-    __shared__ __align__(16) double smem[4 * TILE];
+    extern __shared__ __align__(16) double smem[];
     double *As = smem;
-    double *Bs = smem + 2 * TILE;
+    double *Bs = smem + NST * TILE;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
@@ -201,20 +205,20 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
 #pragma unroll
                         for (int q = 0; q < 4; ++q) acc[i][j][q] *= r;
             }
-            gett_mainloop<AK, BKM>(acc, As, Bs, sg.A, sg.B, sg.offA_m, sg.offA_k, sg.offB_n, sg.offB_k, g.M, g.N, m0,
+            gett_mainloop<AK, BKM, NST>(acc, As, Bs, sg.A, sg.B, sg.offA_m, sg.offA_k, sg.offB_n, sg.offB_k, g.M, g.N, m0,
                                    n0, 0, sg.K, tid, wm, wn, gid, tig, g.vec_a != 0, g.vec_b != 0);
             alpha = sg.alpha;
         }
     } else {
         const int kbeg = blockIdx.z * g.kchunk;
         const int kend = min(g.K, kbeg + g.kchunk);
-        gett_mainloop<AK, BKM>(acc, As, Bs, g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k, g.M, g.N, m0, n0, kbeg,
+        gett_mainloop<AK, BKM, NST>(acc, As, Bs, g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k, g.M, g.N, m0, n0, kbeg,
                                kend, tid, wm, wn, gid, tig, g.vec_a != 0, g.vec_b != 0);
     }
 
     // epilogue: stage the tile in shared memory, then write along the output's
     // contiguous mode (g.c_nfast) so that stores and the beta read coalesce
-    static_assert(BM * (BN + 1) <= 4 * TILE, "C tile must fit in the operand buffers");
+    static_assert(BM * (BN + 1) <= 4 * TILE, "C tile must fit in the operand buffers of two stages");
     double (*Cs)[BN + 1] = reinterpret_cast<double (*)[BN + 1]>(smem);
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
@@ -289,16 +293,28 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
     }
 }
 
-template <bool G>
+template <bool G, int NST>
 void launch_gett_v(const GettArgs &a, int a_kmajor, int b_kmajor, dim3 grid, cudaStream_t s) {
+    constexpr size_t sm = sizeof(double) * 2 * NST * TILE;
     if (a_kmajor && b_kmajor)
-        gett_f64_kernel<true, true, G><<<grid, 128, 0, s>>>(a);
+        gett_f64_kernel<true, true, G, NST><<<grid, 128, sm, s>>>(a);
     else if (a_kmajor)
-        gett_f64_kernel<true, false, G><<<grid, 128, 0, s>>>(a);
+        gett_f64_kernel<true, false, G, NST><<<grid, 128, sm, s>>>(a);
     else if (b_kmajor)
-        gett_f64_kernel<false, true, G><<<grid, 128, 0, s>>>(a);
+        gett_f64_kernel<false, true, G, NST><<<grid, 128, sm, s>>>(a);
     else
-        gett_f64_kernel<false, false, G><<<grid, 128, 0, s>>>(a);
+        gett_f64_kernel<false, false, G, NST><<<grid, 128, sm, s>>>(a);
+}
+
+template <bool G, int NST>
+cudaError_t gett_attr() {
+    constexpr int sm = (int)(sizeof(double) * 2 * NST * TILE);
+    constexpr auto at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e = cudaFuncSetAttribute(gett_f64_kernel<true, true, G, NST>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_kernel<true, false, G, NST>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_kernel<false, true, G, NST>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_kernel<false, false, G, NST>, at, sm);
+    return e;
 }
 
 // ---------------------------------------------------------------------------
@@ -635,6 +651,8 @@ cudaError_t gett_f64_prepare() {
         if (err == cudaSuccess) err = skinny_attr<16, true>();
         if (err == cudaSuccess) err = skinny_attr<32, false>();
         if (err == cudaSuccess) err = skinny_attr<32, true>();
+        if (err == cudaSuccess) err = gett_attr<false, 3>();
+        if (err == cudaSuccess) err = gett_attr<true, 3>();
     });
     return err;
 }
@@ -782,7 +800,7 @@ void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t
     if (a.tile == 3 && launch_smallk(a, a_kmajor, b_kmajor, s)) return;
     const int zsplit = a.segs ? 1 : std::max(1, (a.K + a.kchunk - 1) / a.kchunk);
     int fam = gett_f64_family(a.M, a.N);
-    if (a.tile == 1) fam = 0;
+    if (a.tile == 1 || a.tile == 4) fam = 0;
     else if (a.tile == 2 && std::min(a.M, a.N) <= 32) fam = a.M <= a.N ? 1 : 2;
     if (fam) {
         gett_f64_prepare();
@@ -798,10 +816,14 @@ void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t
         return;
     }
     dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, zsplit);
-    if (a.segs)
-        launch_gett_v<true>(a, a_kmajor, b_kmajor, grid, s);
-    else
-        launch_gett_v<false>(a, a_kmajor, b_kmajor, grid, s);
+    if (a.tile == 4) {
+        gett_f64_prepare();
+        a.segs ? launch_gett_v<true, 3>(a, a_kmajor, b_kmajor, grid, s)
+               : launch_gett_v<false, 3>(a, a_kmajor, b_kmajor, grid, s);
+    } else {
+        a.segs ? launch_gett_v<true, 2>(a, a_kmajor, b_kmajor, grid, s)
+               : launch_gett_v<false, 2>(a, a_kmajor, b_kmajor, grid, s);
+    }
 }
 
 __global__ void zero_view_kernel(double *C, const int *offm, const int *offn, int M, int N) {

@@ -49,7 +49,8 @@ struct GettArgs {
     const GettSeg *segs;  // grouped launch: nseg terms (A, B, tables, K, alpha above unused)
     int nseg;
     int tile;       // 0: tile family by shape (gett_f64_family); 1: 64 x 64 tiles; 2: skinny tiles;
-                    // 3: small-K FMA kernel (whole K per launch, kchunk ignored)
+                    // 3: small-K FMA kernel (whole K per launch, kchunk ignored);
+                    // 4: 64 x 64 tiles with a 3-stage operand pipeline
 };
 
 constexpr int MAXG = 4;  // antisymmetric axis groups per source view

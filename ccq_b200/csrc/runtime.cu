@@ -2066,7 +2066,7 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
 
 int ccq_b200_force_tile(ccq_b200_ctx *c, int64_t tile) {
     if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
-    if (tile < 0 || tile > 3) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..3"));
+    if (tile < 0 || tile > 4) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..4"));
     for (auto &o : c->plan.ops) {
         if (o.kind != OP_GETT || o.g.K == 0) continue;
         o.g.tile = (int)tile;
