@@ -218,8 +218,13 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
 
     // epilogue: stage the tile in shared memory, then write along the output's
     // contiguous mode (g.c_nfast) so that stores and the beta read coalesce
-    static_assert(BM * (BN + 1) <= 4 * TILE, "C tile must fit in the operand buffers of two stages");
+    static_assert(BM * (BN + 1) * 2 + BM + BN <= 8 * TILE, "C tile and output tables must fit in two stages");
     double (*Cs)[BN + 1] = reinterpret_cast<double (*)[BN + 1]>(smem);
+    // the tile's output offsets, staged once (-1: outside C)
+    int *ocm = reinterpret_cast<int *>(smem + BM * (BN + 1));
+    int *ocn = ocm + BM;
+    if (tid < BM) ocm[tid] = m0 + tid < g.M ? __ldg(g.offC_m + m0 + tid) : -1;
+    else if (tid < BM + BN) ocn[tid - BM] = n0 + tid - BM < g.N ? __ldg(g.offC_n + n0 + tid - BM) : -1;
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -246,10 +251,8 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
                 int slow = slow0 + 4 * (p0 + u);
                 int ml = g.c_nfast ? slow : fast;
                 int nl = g.c_nfast ? fast : slow;
-                int m = m0 + ml, n = n0 + nl;
-                bool in = m < g.M && n < g.N;
-                cp[u] = in ? reinterpret_cast<double2 *>(g.C + (long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + n))
-                           : nullptr;
+                const int om = ocm[ml], on = ocn[nl];
+                cp[u] = (om >= 0 && on >= 0) ? reinterpret_cast<double2 *>(g.C + (long long)om + on) : nullptr;
                 cv[u] = g.c_nfast ? make_double2(Cs[ml][nl], Cs[ml][nl + 1]) : make_double2(Cs[ml][nl], Cs[ml + 1][nl]);
             }
             double2 old[4];
@@ -273,9 +276,8 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
             int slow = slow0 + 2 * (p0 + u);
             int ml = g.c_nfast ? slow : fast;
             int nl = g.c_nfast ? fast : slow;
-            int m = m0 + ml, n = n0 + nl;
-            bool in = m < g.M && n < g.N;
-            cp[u] = in ? g.C + (long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + n) : nullptr;
+            const int om = ocm[ml], on = ocn[nl];
+            cp[u] = (om >= 0 && on >= 0) ? g.C + (long long)om + on : nullptr;
             cv[u] = Cs[ml][nl];
         }
         if (atomic) {
