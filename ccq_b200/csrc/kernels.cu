@@ -875,10 +875,10 @@ __device__ __forceinline__ int pick(const int (&v)[RK], int i) {
 // serves EPT elements, and their loads are independent.
 constexpr int ASM_EPT = 2;
 
-template <int RK>
-__device__ __forceinline__ void canonical_element(const AsmArgs &a, long long lin, int (&x)[RK]) {
+template <int RK, typename Off>
+__device__ __forceinline__ void canonical_element(const AsmArgs &a, Off lin, int (&x)[RK]) {
     int cq[RK];
-    long long r = lin;
+    Off r = lin;
 #pragma unroll
     for (int q = RK - 1; q >= 0; --q) {
         cq[q] = 0;
@@ -900,8 +900,9 @@ __device__ __forceinline__ void canonical_element(const AsmArgs &a, long long li
     }
 }
 
-template <int RK>
-__global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
+// Off: index type of every offset (int when AsmArgs::off32 says they all fit)
+template <int RK, typename Off>
+__global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
     constexpr int CH = 128;
     __shared__ SmTerm<RK> st[CH];
     const int nch = (a.nterms + CH - 1) / CH;
@@ -918,7 +919,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
             R[e] = 0.0;
 #pragma unroll
             for (int d = 0; d < RK; ++d) x[e][d] = 0;
-            if (act[e]) canonical_element<RK>(a, lin, x[e]);
+            if (act[e]) canonical_element<RK, Off>(a, (Off)lin, x[e]);
         }
         for (int c = 0; c < nch; ++c) {
             __syncthreads();
@@ -952,25 +953,29 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
                 st[t] = q;
             }
             __syncthreads();
-#pragma unroll 2
-            for (int t = 0; t < nt; ++t) {
+            // plain views first (a branch-free loop, so the loads of several terms are in flight
+            // together), then the views read sorted with sign
+            const int np = min(max(a.nplain - c * CH, 0), nt);
+#pragma unroll 4
+            for (int t = 0; t < np; ++t) {
                 const SmTerm<RK> &q = st[t];
                 const double *p = q.p;
-                if (q.pm == 0) {
-                    int tst[RK];
+                double v[ASM_EPT];
 #pragma unroll
-                    for (int d = 0; d < RK; ++d) tst[d] = q.tst[d];
-                    double v[ASM_EPT];
+                for (int e = 0; e < ASM_EPT; ++e) {
+                    Off off = 0;
 #pragma unroll
-                    for (int e = 0; e < ASM_EPT; ++e) {
-                        long long off = 0;
+                    for (int d = 0; d < RK; ++d) off += (Off)q.tst[d] * x[e][d];
+                    v[e] = act[e] ? __ldg(p + off) : 0.0;
+                }
 #pragma unroll
-                        for (int d = 0; d < RK; ++d) off += (long long)tst[d] * x[e][d];
-                        v[e] = act[e] ? __ldg(p + off) : 0.0;
-                    }
-#pragma unroll
-                    for (int e = 0; e < ASM_EPT; ++e) R[e] += q.coef * v[e];
-                } else {
+                for (int e = 0; e < ASM_EPT; ++e) R[e] += q.coef * v[e];
+            }
+#pragma unroll 2
+            for (int t = np; t < nt; ++t) {
+                const SmTerm<RK> &q = st[t];
+                const double *p = q.p;
+                {
 #pragma unroll
                     for (int e = 0; e < ASM_EPT; ++e) {
                         if (!act[e]) continue;
@@ -995,9 +1000,9 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
                                     }
                                 }
                         if (zero) continue;
-                        long long off = 0;
+                        Off off = 0;
 #pragma unroll
-                        for (int j = 0; j < RK; ++j) off += (long long)q.zs[j] * y[j];
+                        for (int j = 0; j < RK; ++j) off += (Off)q.zs[j] * y[j];
                         R[e] += sg * __ldg(p + off);
                     }
                 }
@@ -1006,9 +1011,9 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
 #pragma unroll
         for (int e = 0; e < ASM_EPT; ++e) {
             if (!act[e]) continue;
-            long long toff = 0;
+            Off toff = 0;
 #pragma unroll
-            for (int d = 0; d < RK; ++d) toff += (long long)a.tstride[d] * x[e][d];
+            for (int d = 0; d < RK; ++d) toff += (Off)a.tstride[d] * x[e][d];
             double tnew;
             if (a.mode != 1) {
                 double D = a.shift;
@@ -1029,9 +1034,9 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
             }
             for (int pidx = 0; pidx < a.nperm; ++pidx) {
                 const signed char *P = a.perm + pidx * RK;
-                long long o = 0;
+                Off o = 0;
 #pragma unroll
-                for (int d = 0; d < RK; ++d) o += (long long)a.tstride[d] * pick<RK>(x[e], P[d]);
+                for (int d = 0; d < RK; ++d) o += (Off)a.tstride[d] * pick<RK>(x[e], P[d]);
                 a.T[o] = a.psign[pidx] * tnew;
             }
         }
@@ -1046,11 +1051,21 @@ void launch_assemble(const AsmArgs &a, cudaStream_t s) {
     long long blocks = (a.total + 256 * ASM_EPT - 1) / (256 * ASM_EPT);
     if (blocks > 148 * 32) blocks = 148 * 32;
     if (blocks < 1) blocks = 1;
+    if (a.off32) {
+        switch (a.rank) {
+            case 2: assemble_kernel<2, int><<<(int)blocks, 256, 0, s>>>(a); break;
+            case 4: assemble_kernel<4, int><<<(int)blocks, 256, 0, s>>>(a); break;
+            case 6: assemble_kernel<6, int><<<(int)blocks, 256, 0, s>>>(a); break;
+            case 8: assemble_kernel<8, int><<<(int)blocks, 256, 0, s>>>(a); break;
+            default: break;
+        }
+        return;
+    }
     switch (a.rank) {
-        case 2: assemble_kernel<2><<<(int)blocks, 256, 0, s>>>(a); break;
-        case 4: assemble_kernel<4><<<(int)blocks, 256, 0, s>>>(a); break;
-        case 6: assemble_kernel<6><<<(int)blocks, 256, 0, s>>>(a); break;
-        case 8: assemble_kernel<8><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 2: assemble_kernel<2, long long><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 4: assemble_kernel<4, long long><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 6: assemble_kernel<6, long long><<<(int)blocks, 256, 0, s>>>(a); break;
+        case 8: assemble_kernel<8, long long><<<(int)blocks, 256, 0, s>>>(a); break;
         default: break;
     }
 }

@@ -95,6 +95,8 @@ struct AsmArgs {
     int nruns;
     int run_axis0[MAXR], run_len[MAXR], run_count[MAXR], run_off[MAXR];
     const unsigned char *combos;
+    int off32;                // every offset (terms, T, canonical index) fits in 32 bits
+    int nplain;               // terms [0, nplain) read plain views (no sorted groups); the rest sorted
 };
 
 // FP64 GETT.  Tile family by output shape: 0 = 64 x 64 tiles; 1 = skinny rows

@@ -805,9 +805,12 @@ void instantiate(ccq_b200_ctx *c) {
             for (int k = 0; k < level; ++k) target.push_back("i" + std::to_string(k));
             for (int k = 0; k < level; ++k) target.push_back("a" + std::to_string(k));
             PendA pa{i, hterms.size(), hperm.size()};
+            // 32-bit offsets when the block, every source buffer and the element count fit
+            bool off32 = T.numel < (1LL << 31);
             for (auto &t : o.terms) {
                 Resolved V = resolve(c, t.second);
                 const DevBuf &src = c->bufs.at(t.second.buf);
+                off32 = off32 && src.numel < (1LL << 31);
                 AsmTerm at{};
                 at.p = V.base;
                 at.coef = t.first;
@@ -832,6 +835,18 @@ void instantiate(ccq_b200_ctx *c) {
             }
             a.nterms = (int)o.terms.size();
             if (a.nterms > MAX_TERMS) throw Error(CCQ_B200_EPLAN, "too many assemble terms");
+            a.off32 = off32 ? 1 : 0;
+            {
+                // plain views (no antisymmetric group of two or more axes) ahead of the sorted ones
+                auto plain = [](const AsmTerm &x) {
+                    for (int g = 0; g < x.ng; ++g)
+                        if (x.glen[g] > 1) return false;
+                    return true;
+                };
+                auto first = hterms.begin() + (long)pa.t0;
+                auto mid = std::stable_partition(first, hterms.end(), plain);
+                a.nplain = (int)(mid - first);
+            }
             // orbit permutations: within same-spin runs of each half
             std::vector<std::vector<int>> runs;
             for (int half = 0; half < 2; ++half) {
