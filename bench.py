@@ -440,6 +440,7 @@ def main():
         st = ctx.stats()
         tot = allmax(sum(ms), world)
         results[leg] = {'s_per_iter': job_seconds_per_iter(sum(ms), world, args.steps), 'ms_total': tot,
+                        'ms_each': [round(x, 3) for x in ms],
                         'tflops': st['flops'] * world * args.steps / (tot * 1e-3) / 1e12,
                         'launches_per_iter': st['launches'], 'flops_per_iter': st['flops']}
     head = results[headline]

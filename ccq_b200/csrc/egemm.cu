@@ -104,7 +104,8 @@ int egemm_impl(long long k1, long long k2, long long k3, const double *A, const 
 ccqb::SplitWorkspace g_split;
 
 // Split-precision egemm (same layout as egemm_impl), nslices int8 slices.
-int egemm_split_impl(long long k1, long long k2, long long k3, const double *A, const double *B, double *C, int S) {
+int egemm_split_impl(long long k1, long long k2, long long k3, const double *A, const double *B, double *C, int S,
+                     int persistent) {
     if (k1 <= 0 || k2 <= 0 || k3 <= 0 || !A || !B || !C || S < 2 || S > 4) return CCQ_B200_EINVAL;
     if (k1 > INT32_MAX || k2 > INT32_MAX || k3 > INT32_MAX || k1 * k3 > INT32_MAX || k2 * k3 > INT32_MAX ||
         k1 * k2 > INT32_MAX)
@@ -161,7 +162,7 @@ int egemm_split_impl(long long k1, long long k2, long long k3, const double *A, 
     try {
         long long kp = (k3 + 63) / 64 * 64;
         ccqb::split_reserve(g_split, ccqb::SplitSizes{k1 * kp, k2 * kp, std::max(k1, k2)}, S);
-        ccqb::split_gett(g_split, g, 1, 1, S, s);
+        ccqb::split_gett(g_split, g, 1, 1, S, s, persistent);
     } catch (const std::exception &) {
         return CCQ_B200_ECUDA;
     }
@@ -178,7 +179,12 @@ extern "C" {
 
 int ccq_b200_egemm_split(int64_t k1, int64_t k2, int64_t k3, const double *A, const double *B, double *C,
                          int64_t nslices) {
-    return egemm_split_impl(k1, k2, k3, A, B, C, (int)nslices);
+    return egemm_split_impl(k1, k2, k3, A, B, C, (int)nslices, 0);
+}
+
+int ccq_b200_egemm_split_kernel(int64_t k1, int64_t k2, int64_t k3, const double *A, const double *B, double *C,
+                                int64_t nslices, int64_t persistent) {
+    return egemm_split_impl(k1, k2, k3, A, B, C, (int)nslices, persistent ? 1 : 0);
 }
 
 

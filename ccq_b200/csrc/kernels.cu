@@ -1261,4 +1261,38 @@ void launch_diis_extrap(const double *ring, long long stride, int ds, long long 
     diis_extrap_kernel<<<(int)blocks, 256, 0, s>>>(ring, stride, ds, n, coef, t);
 }
 
+// With lazy module loading a kernel's code is loaded at its first launch; a
+// first launch in the middle of a solve (the first DIIS step) was measured to
+// stall for ~0.7 s after other libraries had loaded theirs.  Touching every
+// function of the iteration here loads them when the context is created.
+cudaError_t preload_kernels(int ds) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaSuccess;
+    auto touch = [&](const void *f) {
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, f);
+    };
+    switch (ds) {
+#define CASE(D) \
+    case D: touch((const void *)gram_kernel<D>); break;
+        CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10) CASE(11) CASE(12)
+#undef CASE
+        default: break;
+    }
+    touch((const void *)zero_view_kernel);
+    touch((const void *)f2c4_kernel);
+    touch((const void *)fill_kernel);
+    touch((const void *)sqdiff_kernel);
+    touch((const void *)diis_solve_kernel);
+    touch((const void *)diis_extrap_kernel);
+    touch((const void *)assemble_kernel<2, int>);
+    touch((const void *)assemble_kernel<4, int>);
+    touch((const void *)assemble_kernel<6, int>);
+    touch((const void *)assemble_kernel<8, int>);
+    touch((const void *)assemble_kernel<2, long long>);
+    touch((const void *)assemble_kernel<4, long long>);
+    touch((const void *)assemble_kernel<6, long long>);
+    touch((const void *)assemble_kernel<8, long long>);
+    return e;
+}
+
 }  // namespace ccqb

@@ -108,6 +108,9 @@ int gett_f64_kchunk(long long M, long long N, long long K);
 // Sets the shared-memory limits of the skinny kernels; call once before the
 // first launch (outside stream capture).
 cudaError_t gett_f64_prepare();
+// Loads the code of the iteration's kernels now (lazy module loading would
+// load each at its first launch, possibly in the middle of a solve).
+cudaError_t preload_kernels(int diis_space);
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s);
 void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N, cudaStream_t s);
 void launch_assemble(const AsmArgs &a, cudaStream_t s);

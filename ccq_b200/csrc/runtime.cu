@@ -113,7 +113,7 @@ struct Op {
     bool skip = false;         // member of a grouped GETT run by a later op
     double group_flops = 0.0;  // FLOPs of a grouped launch (leader only)
     int group_size = 0;
-    int split_choice = -1;     // split precision for this op: -1 by shape (split_eligible), 0 no, 1 yes (autotuned)
+    int split_choice = -1;     // -1 by shape (split_eligible); autotuned: 0 DMMA, 1 per-tile split kernel, 2 persistent
     std::vector<size_t> group_ops;   // every op of a grouped launch (leader only; members are skipped)
     std::vector<int> hcm, hcn; // output offset tables (grouping key)
     AsmArgs asmargs{};
@@ -1034,8 +1034,11 @@ void instantiate(ccq_b200_ctx *c) {
 // the op runs on the split-precision kernel in this context's current mode
 bool use_split(const ccq_b200_ctx *c, const Op &o) {
     if (c->precision != CCQ_B200_PREC_SPLIT || !o.split) return false;
-    return o.split_choice >= 0 ? o.split_choice == 1 : split_eligible(o.g);
+    return o.split_choice >= 0 ? o.split_choice >= 1 : split_eligible(o.g);
 }
+
+// persistent split kernel (one CTA per SM, overlapped epilogue) unless tuned to the per-tile one
+int split_persistent(const Op &o) { return o.split_choice == 1 ? 0 : 1; }
 
 int op_class(const ccq_b200_ctx *c, const Op &o) {
     if (o.kind == OP_GETT) return use_split(c, o) ? 1 : 0;
@@ -1059,7 +1062,7 @@ void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
                 break;
             }
             if (use_split(c, o)) {
-                c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, st);
+                c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, st, split_persistent(o));
             } else {
                 launch_gett_f64(o.g, o.akm, o.bkm, st);
                 ++c->launches;
@@ -1298,6 +1301,7 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         c = new ccq_b200_ctx();
         CK(cudaGetDevice(&c->device));
         CK(gett_f64_prepare());
+        CK(preload_kernels((int)diis_space));
         c->calc_type = ct;
         c->rhf = rhf != 0;
         c->shift = shift;
@@ -1950,7 +1954,7 @@ static float time_cfg(ccq_b200_ctx *c, Op &o, const TuneCfg &t, double *scratch,
     const bool zf = !g.segs && g.beta == 0 && (g.K + t.kchunk - 1) / t.kchunk > 1;
     auto run = [&]() {
         if (t.split) {
-            split_gett(c->split, g, o.akm, o.bkm, c->nslices, c->stream);
+            split_gett(c->split, g, o.akm, o.bkm, c->nslices, c->stream, t.split == 2);
         } else {
             if (zf) launch_zero_view(g.C, g.offC_m, g.offC_n, g.M, g.N, c->stream);
             launch_gett_f64(g, o.akm, o.bkm, c->stream);
@@ -1995,6 +1999,15 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
             cudaFree(scratch);
         };
         double t0 = 0.0, t1 = 0.0;
+        // every candidate's time, one line each, when CCQ_B200_TUNE_DUMP names a file
+        const char *dpath = getenv("CCQ_B200_TUNE_DUMP");
+        FILE *dump = dpath ? fopen(dpath, "a") : nullptr;
+        struct DumpCloser {
+            FILE *&f;
+            ~DumpCloser() {
+                if (f) fclose(f);
+            }
+        } dump_closer{dump};
         try {
             long long off = 0;
             for (auto &k : keep) {
@@ -2010,7 +2023,7 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
                 }
                 const long long M = o.g.M, N = o.g.N, K = o.g.K;
                 std::vector<TuneCfg> cand;
-                const TuneCfg cur{o.g.tile, o.g.kchunk, use_split(c, o) ? 1 : 0};
+                const TuneCfg cur{o.g.tile, o.g.kchunk, use_split(c, o) ? (split_persistent(o) ? 2 : 1) : 0};
                 cand.push_back(cur);
                 std::vector<int> tiles = {1};
                 if (std::min(M, N) <= 32) tiles.push_back(2);
@@ -2032,14 +2045,17 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
                 }
                 // small-K FMA kernel: whole K per launch
                 if (K <= 128) cand.push_back(TuneCfg{3, o.g.segs ? o.g.kchunk : (int)((K + 15) / 16 * 16), 0});
-                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && split_capable(o.g) && !cur.split)
-                    cand.push_back(TuneCfg{0, o.g.kchunk, 1});
-                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && cur.split)
-                    cand.push_back(TuneCfg{0, o.g.kchunk, 0});
+                // split precision: DMMA, the per-tile and the persistent int8 kernel
+                if (c->precision == CCQ_B200_PREC_SPLIT && o.split && (split_capable(o.g) || cur.split))
+                    for (int v : {0, 1, 2})
+                        if (v != cur.split) cand.push_back(TuneCfg{0, o.g.kchunk, v});
                 float best = 1e30f;
                 TuneCfg pick = cur;
                 for (size_t q = 0; q < cand.size(); ++q) {
                     const float ms = time_cfg(c, o, cand[q], scratch, (int)reps);
+                    if (dump)
+                        fprintf(dump, "%zu %s %lld %lld %lld tile=%d kchunk=%d split=%d %.6f\n", i, o.tag.c_str(), M, N,
+                                K, cand[q].tile, cand[q].kchunk, cand[q].split, ms);
                     if (q == 0) t0 += ms;
                     if (ms < best) {
                         best = ms;

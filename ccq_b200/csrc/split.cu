@@ -424,6 +424,242 @@ __global__ void __launch_bounds__(128, 2)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+// barrier among the four epilogue warps only (ids 0 and 1 are left to __syncthreads)
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+
+// Persistent variant: one CTA per SM walks the output tiles.  Warp 0 lane 0
+// issues the TMA loads of a STAGES-deep ring, warp 1 lane 0 issues the MMAs of
+// a tile into one of two TMEM accumulator sets, and warps 2-5 drain the other
+// set (level recombination, scaling, scattered beta write) while the next tile
+// is multiplied: the epilogue of tile t overlaps the MMAs of tile t + 1.
+// Barriers: full/empty per ring stage; accf[b] (MMA -> epilogue, committed by
+// tcgen05) and acce[b] (epilogue -> MMA, 128 arrivals) per accumulator set.
+// Every wait is bounded; a timeout sets a shared abort flag that every role
+// checks before its next wait, and the host reads the error word.
+template <int S, int NT, int STAGES>
+struct Persist {
+    static constexpr int A_BYTES = TM * BKB, B_BYTES = NT * BKB;
+    static constexpr int STAGE = S * (A_BYTES + B_BYTES);
+    static constexpr int BUFC = S * NT;   // TMEM columns of one accumulator set (levels 2..S+1)
+    static constexpr int CW = 32;         // output columns per epilogue pass
+    static constexpr int CS_BYTES = TM * (CW + 1) * 8;
+    static constexpr int TAB_BYTES = TM * 4 + NT * 4 + TM * 8 + NT * 8;
+    static constexpr int BAR_BYTES = (2 * STAGES + 5) * 8 + 16;
+    static constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE + CS_BYTES + TAB_BYTES + BAR_BYTES;
+    static_assert(2 * BUFC <= 512, "two accumulator sets must fit in TMEM");
+    static_assert(STAGE % 1024 == 0 && A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "swizzle atom alignment");
+    static_assert((TM * 4 + NT * 4) % 8 == 0 && CS_BYTES % 8 == 0, "table alignment");
+};
+
+template <int S, int NT, int STAGES>
+__global__ void __launch_bounds__(192, 1)
+    split_gett_persistent(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, SplitArgs p) {
+    using P = Persist<S, NT, STAGES>;
+    constexpr int CW = P::CW;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    double (*Cs)[CW + 1] = reinterpret_cast<double (*)[CW + 1]>(smem + STAGES * P::STAGE);
+    int *eas = reinterpret_cast<int *>(smem + STAGES * P::STAGE + P::CS_BYTES);
+    int *ebs = eas + TM;
+    long long *oms = reinterpret_cast<long long *>(ebs + NT);   // output row offsets (-1: outside)
+    long long *ons = oms + TM;                                   // output column offsets
+    uint64_t *full = reinterpret_cast<uint64_t *>(ons + NT);
+    uint64_t *empty = full + STAGES;
+    uint64_t *accf = empty + STAGES;
+    uint64_t *acce = accf + 2;
+    uint64_t *fin = acce + 2;   // the MMA issuer's last commit: all its MMAs have completed
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(fin + 1);
+    __shared__ volatile int abort_flag;
+    __shared__ volatile int epi_stop;   // written by epilogue thread 0 only, read by all four warps after a barrier
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = (p.M + TM - 1) / TM, nt = (p.N + NT - 1) / NT;
+    const int ntiles = mt * nt;
+    const int ktiles = p.Kp / BKB;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 128);
+        }
+        mbar_init(fin, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer: the k-tiles of every tile of this CTA, through the ring
+            long long kc = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x) {
+                const int m0 = (tile % mt) * TM, n0 = (tile / mt) * NT;
+                for (int kt = 0; kt < ktiles; ++kt, ++kc) {
+                    const int s = (int)(kc % STAGES);
+                    if (kc >= STAGES && !mbar_wait(&empty[s], (unsigned)(((kc / STAGES) - 1) & 1))) abort_flag = 1;
+                    if (abort_flag) break;
+                    unsigned char *st = smem + s * P::STAGE;
+                    mbar_expect_tx(&full[s], P::STAGE);
+                    tma_load_3d(st, &ta, &full[s], kt * BKB, m0, 0);
+                    tma_load_3d(st + S * P::A_BYTES, &tb, &full[s], kt * BKB, n0, 0);
+                }
+            }
+            // every issued copy lands before the CTA can exit
+            for (long long q = kc > STAGES ? kc - STAGES : 0; q < kc; ++q)
+                if (!mbar_wait(&full[q % STAGES], (unsigned)((q / STAGES) & 1))) abort_flag = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer: S32 <- S8 x S8, K-major A and B, M = 128, N = NT
+            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                                   ((uint32_t)(TM >> 4) << 24);
+            long long kc = 0;
+            int tl = 0;
+            for (int tile = blockIdx.x; tile < ntiles && !abort_flag; tile += gridDim.x, ++tl) {
+                const int b = tl & 1, u = tl >> 1;
+                // the epilogue has drained this accumulator set (its previous use)
+                if (u > 0 && !mbar_wait(&acce[b], (unsigned)((u - 1) & 1))) {
+                    abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n");
+                const uint32_t tacc = tmem + (uint32_t)(b * P::BUFC);
+                bool ok = true;
+                for (int kt = 0; kt < ktiles; ++kt, ++kc) {
+                    const int s = (int)(kc % STAGES);
+                    if (abort_flag || !mbar_wait(&full[s], (unsigned)((kc / STAGES) & 1))) {
+                        abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n");
+                    unsigned char *st = smem + s * P::STAGE;
+#pragma unroll
+                    for (int kk = 0; kk < BKB / 32; ++kk) {
+#pragma unroll
+                        for (int i = 0; i < S; ++i) {
+                            const uint64_t da = smem_desc_sw64(st + i * P::A_BYTES) + (uint64_t)(kk * 32 >> 4);
+#pragma unroll
+                            for (int j = 0; j < S - i; ++j) {
+                                const uint64_t db =
+                                    smem_desc_sw64(st + S * P::A_BYTES + j * P::B_BYTES) + (uint64_t)(kk * 32 >> 4);
+                                // the first product of each level at the tile's first K step initialises it
+                                const uint32_t acc = (kt > 0 || kk > 0 || i > 0) ? 1u : 0u;
+                                umma_i8(tacc + (uint32_t)((i + j) * NT), da, db, idesc, acc);
+                            }
+                        }
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                umma_commit(&accf[b]);
+            }
+            // TMEM is released below only after every MMA this thread issued has completed
+            umma_commit(fin);
+            if (!mbar_wait(fin, 0)) abort_flag = 1;
+        }
+    } else {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31
+        const int q = warp & 3, row = q * 32 + lane, et = threadIdx.x - 64;
+        int tl = 0;
+        // the four warps leave the tile loop together: the stop decision is taken by one thread
+        // and published through a barrier, never read from abort_flag by each thread on its own
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tl) {
+            const int b = tl & 1, u = tl >> 1;
+            if (et == 0) {
+                const bool ok = !abort_flag && mbar_wait(&accf[b], (unsigned)(u & 1));
+                if (!ok) abort_flag = 1;
+                epi_stop = ok ? 0 : 1;
+            }
+            epi_sync();
+            if (epi_stop) break;
+            // the phase has completed (thread 0 saw it): this returns at once and orders this thread's reads
+            mbar_wait(&accf[b], (unsigned)(u & 1));
+            asm volatile("tcgen05.fence::after_thread_sync;\n");
+            const int m0 = (tile % mt) * TM, n0 = (tile / mt) * NT;
+            for (int t = et; t < TM; t += 128) {
+                const bool in = m0 + t < p.M;
+                eas[t] = in ? p.ea[m0 + t] : 0;
+                oms[t] = in ? (long long)p.offC_m[m0 + t] : -1;
+            }
+            for (int t = et; t < NT; t += 128) {
+                const bool in = n0 + t < p.N;
+                ebs[t] = in ? p.eb[n0 + t] : 0;
+                ons[t] = in ? (long long)p.offC_n[n0 + t] : -1;
+            }
+            const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * P::BUFC);
+#pragma unroll 1
+            for (int cb = 0; cb < NT; cb += CW) {
+                double val[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c) val[c] = 0.0;
+#pragma unroll
+                for (int lev = S - 1; lev >= 0; --lev) {
+                    int v[32];
+                    tmem_ld32<NT>(tacc + (uint32_t)(lev * NT + cb), v);
+                    const double w = ldexp(1.0, -7 * lev);
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) val[c] += (double)v[c] * w;
+                }
+                if (cb + CW >= NT) {
+                    // this thread's reads of the set are complete: release it to the MMA warp
+                    asm volatile("tcgen05.fence::before_thread_sync;\n");
+                    mbar_arrive(&acce[b]);
+                }
+                epi_sync();   // the previous pass's write-out has finished reading Cs (and the tables are in)
+#pragma unroll
+                for (int c = 0; c < 32; ++c) Cs[row][c] = val[c];
+                epi_sync();
+#pragma unroll 1
+                for (int p0 = 0; p0 < TM * CW / 128; p0 += 16) {
+                    double *cp[16];
+                    double cv[16];
+#pragma unroll
+                    for (int uu = 0; uu < 16; ++uu) {
+                        const int idx = (p0 + uu) * 128 + et;
+                        int ml, nl;
+                        if (p.c_nfast) {
+                            nl = idx % CW;
+                            ml = idx / CW;
+                        } else {
+                            ml = idx % TM;
+                            nl = idx / TM;
+                        }
+                        const long long om = oms[ml], on = ons[cb + nl];
+                        cp[uu] = (om >= 0 && on >= 0) ? p.C + om + on : nullptr;
+                        cv[uu] = p.alpha * ldexp(Cs[ml][nl], eas[ml] + ebs[cb + nl] - 12);
+                    }
+                    double old[16];
+#pragma unroll
+                    for (int uu = 0; uu < 16; ++uu) old[uu] = (cp[uu] && p.beta) ? *cp[uu] : 0.0;
+#pragma unroll
+                    for (int uu = 0; uu < 16; ++uu)
+                        if (cp[uu]) *cp[uu] = old[uu] + cv[uu];
+                }
+            }
+            epi_sync();   // tables and Cs are free for the next tile
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n");
+    __syncthreads();
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
+    if (threadIdx.x == 0 && abort_flag) atomicExch(p.err, 1);
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -460,6 +696,20 @@ CUtensorMap make_map(signed char *base, long long rows, long long Kp, int S, int
 }
 
 template <int S, int NT, int STAGES>
+void launch_split_persistent(const CUtensorMap &ta, const CUtensorMap &tb, const SplitArgs &a, cudaStream_t s) {
+    const int tiles = ((a.M + TM - 1) / TM) * ((a.N + NT - 1) / NT);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms < 1) sms = 148;
+    }
+    const int grid = std::min(tiles, sms);
+    split_gett_persistent<S, NT, STAGES><<<grid, 192, Persist<S, NT, STAGES>::SMEM, s>>>(ta, tb, a);
+}
+
+template <int S, int NT, int STAGES>
 void launch_split(const CUtensorMap &ta, const CUtensorMap &tb, const SplitArgs &a, cudaStream_t s) {
     constexpr int STAGE = S * (TM * BKB + NT * BKB);
     size_t smem = (size_t)STAGES * STAGE + 1024 + 256;
@@ -476,6 +726,13 @@ void set_smem_attr() {
     if (cudaFuncSetAttribute(split_gett_kernel<S, NT, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         throw std::runtime_error("cannot enable large shared memory for the split kernel");
+}
+
+template <int S, int NT, int STAGES>
+void set_persist_attr() {
+    if (cudaFuncSetAttribute(split_gett_persistent<S, NT, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Persist<S, NT, STAGES>::SMEM) != cudaSuccess)
+        throw std::runtime_error("cannot enable large shared memory for the persistent split kernel");
 }
 
 }  // namespace
@@ -498,6 +755,9 @@ void split_reserve(SplitWorkspace &w, SplitSizes sz, int nslices) {
     set_smem_attr<2, 128, 3>();
     set_smem_attr<3, 64, 2>();
     set_smem_attr<4, 64, 2>();
+    set_persist_attr<2, 128, 4>();
+    set_persist_attr<3, 64, 3>();
+    set_persist_attr<4, 64, 3>();
     w.cap_a = ca;
     w.cap_b = cb;
     w.cap_mn = sz.mn;
@@ -544,7 +804,8 @@ void slice_operand(const double *base, const int *offr, const int *offk, int R, 
     }
 }
 
-int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor, int S, cudaStream_t s) {
+int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor, int S, cudaStream_t s,
+               int persistent) {
     if (S < 2 || S > 4) throw std::runtime_error("split GETT supports 2..4 slices");
     long long Kp = ((long long)g.K + BKB - 1) / BKB * BKB;
     long long Mr = g.M, Nr = g.N;
@@ -555,6 +816,14 @@ int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor,
     CUtensorMap ta = make_map(w.a, Mr, Kp, S, TM);
     CUtensorMap tb = make_map(w.b, Nr, Kp, S, tile_n(S));
     SplitArgs a{g.C, g.offC_m, g.offC_n, w.ea, w.eb, g.M, g.N, g.K, (int)Kp, g.alpha, g.beta, g.c_nfast, w.err};
+    if (persistent) {
+        switch (S) {
+            case 2: launch_split_persistent<2, 128, 4>(ta, tb, a, s); break;
+            case 3: launch_split_persistent<3, 64, 3>(ta, tb, a, s); break;
+            case 4: launch_split_persistent<4, 64, 3>(ta, tb, a, s); break;
+        }
+        return 3;
+    }
     switch (S) {
         case 2: launch_split<2, 128, 3>(ta, tb, a, s); break;
         case 3: launch_split<3, 64, 2>(ta, tb, a, s); break;

@@ -28,7 +28,10 @@ struct SplitWorkspace {
 void split_reserve(SplitWorkspace &w, SplitSizes s, int nslices);
 void split_free(SplitWorkspace &w);
 // Runs one GETT in split precision; returns the number of kernels launched.
-int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor, int nslices, cudaStream_t s);
+// persistent: one CTA per SM over all output tiles, epilogue overlapped with
+// the next tile's MMAs (else one CTA per output tile).
+int split_gett(SplitWorkspace &w, const GettArgs &g, int a_kmajor, int b_kmajor, int nslices, cudaStream_t s,
+               int persistent = 0);
 int split_launch_count(const GettArgs &g, int nslices);
 // Large enough for the tensor-core split path (else FP64 DMMA).
 bool split_eligible(const GettArgs &g);

@@ -36,6 +36,7 @@ class Dims(C.Structure):
 SIGNATURES = {
     'ccq_b200_egemm': (C.c_int, [I64, I64, I64, DP, DP, DP]),
     'ccq_b200_egemm_split': (C.c_int, [I64, I64, I64, DP, DP, DP, I64]),
+    'ccq_b200_egemm_split_kernel': (C.c_int, [I64, I64, I64, DP, DP, DP, I64, I64]),
     'ccq_b200_egemm1': (C.c_int, [I64, I64, DP, DP, DP]),
     'ccq_b200_egemm2': (C.c_int, [I64, I64, DP, DP, DP]),
     'ccq_b200_init': (C.c_int, [C.POINTER(Dims), C.c_char_p, DP, DP, DP, DP, DP, I64, C.c_double, I64,
@@ -150,13 +151,16 @@ def egemm(k1, k2, k3, A, B):
     return Cm
 
 
-def egemm_split(k1, k2, k3, A, B, nslices=4):
-    """egemm with int8 Ozaki slices on the tcgen05 tensor pipe."""
+def egemm_split(k1, k2, k3, A, B, nslices=4, persistent=None):
+    """egemm with int8 Ozaki slices on the tcgen05 tensor pipe (persistent: pick the kernel)."""
     lib = load()
     A = np.asfortranarray(A, dtype=np.float64).reshape((k3, k1), order='F')
     B = np.asfortranarray(B, dtype=np.float64).reshape((k3, k2), order='F')
     Cm = np.zeros((k2, k1), order='F')
-    _err(lib.ccq_b200_egemm_split(k1, k2, k3, _p(A), _p(B), _p(Cm), nslices))
+    if persistent is None:
+        _err(lib.ccq_b200_egemm_split(k1, k2, k3, _p(A), _p(B), _p(Cm), nslices))
+    else:
+        _err(lib.ccq_b200_egemm_split_kernel(k1, k2, k3, _p(A), _p(B), _p(Cm), nslices, int(persistent)))
     return Cm
 
 

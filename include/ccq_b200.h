@@ -71,6 +71,10 @@ int ccq_b200_egemm2(int64_t k2, int64_t k3, const double *A, const double *B, do
  * about nslices * 2^(-7 nslices - 5) * k3 * max|A col| * max|B col|. */
 int ccq_b200_egemm_split(int64_t k1, int64_t k2, int64_t k3,
                          const double *A, const double *B, double *C, int64_t nslices);
+/* The same with the kernel chosen: persistent = 0 one CTA per output tile,
+ * 1 one CTA per SM walking the tiles with the epilogue overlapped. */
+int ccq_b200_egemm_split_kernel(int64_t k1, int64_t k2, int64_t k3, const double *A, const double *B, double *C,
+                                int64_t nslices, int64_t persistent);
 
 /* Fortran link-level drop-ins with gfortran's names and by-reference
  * arguments (ILP64 integers): link libccq_b200 in place of dgemm.o. */
