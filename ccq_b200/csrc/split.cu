@@ -226,6 +226,13 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                  : "memory");
 }
 
+// x * 2^n, correctly rounded: a multiply by the power of two built from its exponent bits
+// when 2^n is a normal double, else the library ldexp
+__device__ __forceinline__ double scale2(double x, int n) {
+    if (n >= -1022 && n <= 1023) return x * __longlong_as_double((long long)(n + 1023) << 52);
+    return ldexp(x, n);
+}
+
 template <int NT>
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
     asm volatile(
@@ -407,7 +414,7 @@ __global__ void __launch_bounds__(128, 2)
                     }
                     long long om = oms[ml], on = ons[cb + nl];
                     cp[u] = (om >= 0 && on >= 0) ? p.C + om + on : nullptr;
-                    cv[u] = p.alpha * ldexp(Cs[ml][nl], eas[ml] + ebs[cb + nl] - 12);
+                    cv[u] = p.alpha * scale2(Cs[ml][nl], eas[ml] + ebs[cb + nl] - 12);
                 }
                 double old[16];
 #pragma unroll
@@ -427,16 +434,23 @@ __global__ void __launch_bounds__(128, 2)
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
-// barrier among the four epilogue warps only (ids 0 and 1 are left to __syncthreads)
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+// named barriers of the persistent kernel's epilogue warps (barrier 0 is __syncthreads):
+// 1 and 2 for the two halves (128 threads each), 3 for all eight warps
+__device__ __forceinline__ void epi_sync_half(int h) {
+    if (h == 0)
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+    else
+        asm volatile("bar.sync 2, 128;\n" ::: "memory");
+}
+__device__ __forceinline__ void epi_sync_all() { asm volatile("bar.sync 3, 256;\n" ::: "memory"); }
 
 // Persistent variant: one CTA per SM walks the output tiles.  Warp 0 lane 0
 // issues the TMA loads of a STAGES-deep ring, warp 1 lane 0 issues the MMAs of
-// a tile into one of two TMEM accumulator sets, and warps 2-5 drain the other
+// a tile into one of two TMEM accumulator sets, and warps 2-9 drain the other
 // set (level recombination, scaling, scattered beta write) while the next tile
 // is multiplied: the epilogue of tile t overlaps the MMAs of tile t + 1.
 // Barriers: full/empty per ring stage; accf[b] (MMA -> epilogue, committed by
-// tcgen05) and acce[b] (epilogue -> MMA, 128 arrivals) per accumulator set.
+// tcgen05) and acce[b] (epilogue -> MMA, 256 arrivals) per accumulator set.
 // Every wait is bounded; a timeout sets a shared abort flag that every role
 // checks before its next wait, and the host reads the error word.
 template <int S, int NT, int STAGES>
@@ -445,7 +459,7 @@ struct Persist {
     static constexpr int STAGE = S * (A_BYTES + B_BYTES);
     static constexpr int BUFC = S * NT;   // TMEM columns of one accumulator set (levels 2..S+1)
     static constexpr int CW = 32;         // output columns per epilogue pass
-    static constexpr int CS_BYTES = TM * (CW + 1) * 8;
+    static constexpr int CS_BYTES = 2 * TM * (CW + 1) * 8;   // one staging tile per epilogue half
     static constexpr int TAB_BYTES = TM * 4 + NT * 4 + TM * 8 + NT * 8;
     static constexpr int BAR_BYTES = (2 * STAGES + 5) * 8 + 16;
     static constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE + CS_BYTES + TAB_BYTES + BAR_BYTES;
@@ -455,7 +469,7 @@ struct Persist {
 };
 
 template <int S, int NT, int STAGES>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(320, 1)
     split_gett_persistent(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, SplitArgs p) {
     using P = Persist<S, NT, STAGES>;
     constexpr int CW = P::CW;
@@ -473,7 +487,7 @@ __global__ void __launch_bounds__(192, 1)
     uint64_t *fin = acce + 2;   // the MMA issuer's last commit: all its MMAs have completed
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(fin + 1);
     __shared__ volatile int abort_flag;
-    __shared__ volatile int epi_stop;   // written by epilogue thread 0 only, read by all four warps after a barrier
+    __shared__ volatile int epi_stop;   // written by epilogue thread 0 only, read by all eight warps after a barrier
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (p.M + TM - 1) / TM, nt = (p.N + NT - 1) / NT;
@@ -488,7 +502,7 @@ __global__ void __launch_bounds__(192, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&accf[b], 1);
-            mbar_init(&acce[b], 128);
+            mbar_init(&acce[b], 256);
         }
         mbar_init(fin, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -573,10 +587,12 @@ __global__ void __launch_bounds__(192, 1)
             if (!mbar_wait(fin, 0)) abort_flag = 1;
         }
     } else {
-        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31
-        const int q = warp & 3, row = q * 32 + lane, et = threadIdx.x - 64;
+        // epilogue: warps 2-9.  Warp w reads TMEM lanes 32 (w % 4) .. + 31 (its quadrant); the two
+        // warps of a quadrant split the tile's 32-column chunks (half h takes chunks h, h + 2, ...)
+        const int q = warp & 3, row = q * 32 + lane, et = threadIdx.x - 64, h = et >> 7, eh = et & 127;
+        double (*Ch)[CW + 1] = Cs + h * TM;
         int tl = 0;
-        // the four warps leave the tile loop together: the stop decision is taken by one thread
+        // the eight warps leave the tile loop together: the stop decision is taken by one thread
         // and published through a barrier, never read from abort_flag by each thread on its own
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tl) {
             const int b = tl & 1, u = tl >> 1;
@@ -585,25 +601,26 @@ __global__ void __launch_bounds__(192, 1)
                 if (!ok) abort_flag = 1;
                 epi_stop = ok ? 0 : 1;
             }
-            epi_sync();
+            epi_sync_all();
             if (epi_stop) break;
             // the phase has completed (thread 0 saw it): this returns at once and orders this thread's reads
             mbar_wait(&accf[b], (unsigned)(u & 1));
             asm volatile("tcgen05.fence::after_thread_sync;\n");
             const int m0 = (tile % mt) * TM, n0 = (tile / mt) * NT;
-            for (int t = et; t < TM; t += 128) {
+            for (int t = et; t < TM; t += 256) {
                 const bool in = m0 + t < p.M;
                 eas[t] = in ? p.ea[m0 + t] : 0;
                 oms[t] = in ? (long long)p.offC_m[m0 + t] : -1;
             }
-            for (int t = et; t < NT; t += 128) {
+            for (int t = et; t < NT; t += 256) {
                 const bool in = n0 + t < p.N;
                 ebs[t] = in ? p.eb[n0 + t] : 0;
                 ons[t] = in ? (long long)p.offC_n[n0 + t] : -1;
             }
+            epi_sync_all();   // tables in
             const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * P::BUFC);
 #pragma unroll 1
-            for (int cb = 0; cb < NT; cb += CW) {
+            for (int cb = h * CW; cb < NT; cb += 2 * CW) {
                 double val[32];
 #pragma unroll
                 for (int c = 0; c < 32; ++c) val[c] = 0.0;
@@ -615,22 +632,22 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
                     for (int c = 0; c < 32; ++c) val[c] += (double)v[c] * w;
                 }
-                if (cb + CW >= NT) {
+                if (cb + 2 * CW >= NT) {
                     // this thread's reads of the set are complete: release it to the MMA warp
                     asm volatile("tcgen05.fence::before_thread_sync;\n");
                     mbar_arrive(&acce[b]);
                 }
-                epi_sync();   // the previous pass's write-out has finished reading Cs (and the tables are in)
+                epi_sync_half(h);   // this half's previous write-out has finished reading Ch
 #pragma unroll
-                for (int c = 0; c < 32; ++c) Cs[row][c] = val[c];
-                epi_sync();
+                for (int c = 0; c < 32; ++c) Ch[row][c] = val[c];
+                epi_sync_half(h);
 #pragma unroll 1
-                for (int p0 = 0; p0 < TM * CW / 128; p0 += 16) {
-                    double *cp[16];
-                    double cv[16];
+                for (int p0 = 0; p0 < TM * CW / 128; p0 += 8) {
+                    double *cp[8];
+                    double cv[8];
 #pragma unroll
-                    for (int uu = 0; uu < 16; ++uu) {
-                        const int idx = (p0 + uu) * 128 + et;
+                    for (int uu = 0; uu < 8; ++uu) {
+                        const int idx = (p0 + uu) * 128 + eh;
                         int ml, nl;
                         if (p.c_nfast) {
                             nl = idx % CW;
@@ -641,17 +658,17 @@ __global__ void __launch_bounds__(192, 1)
                         }
                         const long long om = oms[ml], on = ons[cb + nl];
                         cp[uu] = (om >= 0 && on >= 0) ? p.C + om + on : nullptr;
-                        cv[uu] = p.alpha * ldexp(Cs[ml][nl], eas[ml] + ebs[cb + nl] - 12);
+                        cv[uu] = p.alpha * scale2(Ch[ml][nl], eas[ml] + ebs[cb + nl] - 12);
                     }
-                    double old[16];
+                    double old[8];
 #pragma unroll
-                    for (int uu = 0; uu < 16; ++uu) old[uu] = (cp[uu] && p.beta) ? *cp[uu] : 0.0;
+                    for (int uu = 0; uu < 8; ++uu) old[uu] = (cp[uu] && p.beta) ? *cp[uu] : 0.0;
 #pragma unroll
-                    for (int uu = 0; uu < 16; ++uu)
+                    for (int uu = 0; uu < 8; ++uu)
                         if (cp[uu]) *cp[uu] = old[uu] + cv[uu];
                 }
             }
-            epi_sync();   // tables and Cs are free for the next tile
+            epi_sync_all();   // tables and staging tiles are free for the next tile
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n");
@@ -706,7 +723,7 @@ void launch_split_persistent(const CUtensorMap &ta, const CUtensorMap &tb, const
         if (sms < 1) sms = 148;
     }
     const int grid = std::min(tiles, sms);
-    split_gett_persistent<S, NT, STAGES><<<grid, 192, Persist<S, NT, STAGES>::SMEM, s>>>(ta, tb, a);
+    split_gett_persistent<S, NT, STAGES><<<grid, 320, Persist<S, NT, STAGES>::SMEM, s>>>(ta, tb, a);
 }
 
 template <int S, int NT, int STAGES>
