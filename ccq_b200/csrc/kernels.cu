@@ -444,9 +444,9 @@ __device__ __forceinline__ void skinny_load(double *st, const SkTerm &p, const S
     }
 }
 
-// K loop of one term over [kbeg, kend): SST-stage ring, one barrier per slab
+// K loop of one term over [kbeg, kend): ST-stage ring, one barrier per slab
 // (the slab loaded at step t overwrites the stage computed at step t - 1).
-template <int BMS, bool AK, bool BKM>
+template <int BMS, bool AK, bool BKM, int ST>
 __device__ __forceinline__ void skinny_mainloop(double (&acc)[BMS / 16][4][4], double *sm, SkTabs &t,
                                                 const SkTerm &p, int M, int N, int m0, int n0, int kbeg, int kend,
                                                 int tid, int wn, int gid, int tig, bool vb) {
@@ -471,18 +471,18 @@ __device__ __forceinline__ void skinny_mainloop(double (&acc)[BMS / 16][4][4], d
     __syncthreads();
     const int nt = kend > kbeg ? (kend - kbeg + SBK - 1) / SBK : 0;
 #pragma unroll
-    for (int s = 0; s < SST - 1; ++s) {
+    for (int s = 0; s < ST - 1; ++s) {
         if (s < nt) skinny_load<BMS, AK, BKM>(sm + s * T::STAGE, p, t, M, N, m0, n0, kbeg + s * SBK, kend, tid, vb);
         cp_async_commit();
     }
     for (int it = 0; it < nt; ++it) {
-        cp_async_wait<SST - 2>();
+        cp_async_wait<ST - 2>();
         __syncthreads();
-        const int tn = it + SST - 1;
+        const int tn = it + ST - 1;
         if (tn < nt)
-            skinny_load<BMS, AK, BKM>(sm + (tn % SST) * T::STAGE, p, t, M, N, m0, n0, kbeg + tn * SBK, kend, tid, vb);
+            skinny_load<BMS, AK, BKM>(sm + (tn % ST) * T::STAGE, p, t, M, N, m0, n0, kbeg + tn * SBK, kend, tid, vb);
         cp_async_commit();
-        const double *As = sm + (it % SST) * T::STAGE, *Bs = As + T::ATILE;
+        const double *As = sm + (it % ST) * T::STAGE, *Bs = As + T::ATILE;
 #pragma unroll
         for (int kk = 0; kk < SBK; kk += 4) {
             double a[BMS / 16][2], b[4];
@@ -503,7 +503,7 @@ __device__ __forceinline__ void skinny_mainloop(double (&acc)[BMS / 16][4][4], d
     __syncthreads();
 }
 
-template <int BMS, bool AK, bool BKM, bool GROUPED>
+template <int BMS, bool AK, bool BKM, bool GROUPED, int ST>
 __global__ void __launch_bounds__(128) gett_f64_skinny_kernel(GettArgs g) {
     using T = Skinny<BMS>;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(128) gett_f64_skinny_kernel(GettArgs g) {
             }
             const SkTerm p = sw ? SkTerm{sg.B, sg.A, sg.offB_n, sg.offB_k, sg.offA_m, sg.offA_k}
                                 : SkTerm{sg.A, sg.B, sg.offA_m, sg.offA_k, sg.offB_n, sg.offB_k};
-            skinny_mainloop<BMS, AK, BKM>(acc, sm, t, p, M, N, m0, n0, 0, sg.K, tid, wn, gid, tig, vb);
+            skinny_mainloop<BMS, AK, BKM, ST>(acc, sm, t, p, M, N, m0, n0, 0, sg.K, tid, wn, gid, tig, vb);
             alpha = sg.alpha;
         }
     } else {
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(128) gett_f64_skinny_kernel(GettArgs g) {
                             : SkTerm{g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k};
         const int kbeg = blockIdx.z * g.kchunk;
         const int kend = min(g.K, kbeg + g.kchunk);
-        skinny_mainloop<BMS, AK, BKM>(acc, sm, t, p, M, N, m0, n0, kbeg, kend, tid, wn, gid, tig, vb);
+        skinny_mainloop<BMS, AK, BKM, ST>(acc, sm, t, p, M, N, m0, n0, kbeg, kend, tid, wn, gid, tig, vb);
     }
 
     // epilogue: stage the tile, then write along the output's contiguous mode
@@ -614,34 +614,35 @@ __global__ void __launch_bounds__(128) gett_f64_skinny_kernel(GettArgs g) {
     }
 }
 
-template <int BMS, bool G>
+template <int BMS, bool G, int ST>
 void launch_skinny_v(const GettArgs &a, int ak, int bk, dim3 grid, cudaStream_t s) {
-    // ring stages: every K slab of a slice when they fit below SST (all loaded
+    // ring stages: every K slab of a slice when they fit below ST (all loaded
     // in the prologue), else the full ring; grouped launches take the full ring
-    int stages = SST;
+    int stages = ST;
     if (!G) {
         const int nt = (std::min(a.K, a.kchunk) + SBK - 1) / SBK;
-        if (nt < SST) stages = std::max(nt, Skinny<BMS>::CS_STAGES);
+        if (nt < ST) stages = std::max(nt, Skinny<BMS>::CS_STAGES);
     }
+    stages = std::max(stages, Skinny<BMS>::CS_STAGES);
     const int sm = Skinny<BMS>::smem(stages);
     if (ak && bk)
-        gett_f64_skinny_kernel<BMS, true, true, G><<<grid, 128, sm, s>>>(a);
+        gett_f64_skinny_kernel<BMS, true, true, G, ST><<<grid, 128, sm, s>>>(a);
     else if (ak)
-        gett_f64_skinny_kernel<BMS, true, false, G><<<grid, 128, sm, s>>>(a);
+        gett_f64_skinny_kernel<BMS, true, false, G, ST><<<grid, 128, sm, s>>>(a);
     else if (bk)
-        gett_f64_skinny_kernel<BMS, false, true, G><<<grid, 128, sm, s>>>(a);
+        gett_f64_skinny_kernel<BMS, false, true, G, ST><<<grid, 128, sm, s>>>(a);
     else
-        gett_f64_skinny_kernel<BMS, false, false, G><<<grid, 128, sm, s>>>(a);
+        gett_f64_skinny_kernel<BMS, false, false, G, ST><<<grid, 128, sm, s>>>(a);
 }
 
-template <int BMS, bool G>
+template <int BMS, bool G, int ST>
 cudaError_t skinny_attr() {
-    constexpr int sm = Skinny<BMS>::SMEM;
+    const int sm = Skinny<BMS>::smem(std::max(ST, Skinny<BMS>::CS_STAGES));
     constexpr auto at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, true, true, G>, at, sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, true, false, G>, at, sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, false, true, G>, at, sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, false, false, G>, at, sm);
+    cudaError_t e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, true, true, G, ST>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, true, false, G, ST>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, false, true, G, ST>, at, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_skinny_kernel<BMS, false, false, G, ST>, at, sm);
     return e;
 }
 
@@ -649,10 +650,14 @@ cudaError_t gett_f64_prepare() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
-        err = skinny_attr<16, false>();
-        if (err == cudaSuccess) err = skinny_attr<16, true>();
-        if (err == cudaSuccess) err = skinny_attr<32, false>();
-        if (err == cudaSuccess) err = skinny_attr<32, true>();
+        err = skinny_attr<16, false, SST>();
+        if (err == cudaSuccess) err = skinny_attr<16, true, SST>();
+        if (err == cudaSuccess) err = skinny_attr<32, false, SST>();
+        if (err == cudaSuccess) err = skinny_attr<32, true, SST>();
+        if (err == cudaSuccess) err = skinny_attr<16, false, 2>();
+        if (err == cudaSuccess) err = skinny_attr<16, true, 2>();
+        if (err == cudaSuccess) err = skinny_attr<32, false, 2>();
+        if (err == cudaSuccess) err = skinny_attr<32, true, 2>();
         if (err == cudaSuccess) err = gett_attr<false, 3>();
         if (err == cudaSuccess) err = gett_attr<true, 3>();
     });
@@ -803,17 +808,26 @@ void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t
     const int zsplit = a.segs ? 1 : std::max(1, (a.K + a.kchunk - 1) / a.kchunk);
     int fam = gett_f64_family(a.M, a.N);
     if (a.tile == 1 || a.tile == 4) fam = 0;
-    else if (a.tile == 2 && std::min(a.M, a.N) <= 32) fam = a.M <= a.N ? 1 : 2;
+    else if ((a.tile == 2 || a.tile == 5) && std::min(a.M, a.N) <= 32) fam = a.M <= a.N ? 1 : 2;
     if (fam) {
         gett_f64_prepare();
         const int shrt = std::min(a.M, a.N), lng = std::max(a.M, a.N);
         const int ak = fam == 2 ? b_kmajor : a_kmajor, bk = fam == 2 ? a_kmajor : b_kmajor;
+        const bool two = a.tile == 5;   // 2-stage ring: half the shared memory, more CTAs per SM
         if (shrt <= 16) {
             dim3 grid((lng + SBN - 1) / SBN, (shrt + 15) / 16, zsplit);
-            a.segs ? launch_skinny_v<16, true>(a, ak, bk, grid, s) : launch_skinny_v<16, false>(a, ak, bk, grid, s);
+            if (two)
+                a.segs ? launch_skinny_v<16, true, 2>(a, ak, bk, grid, s) : launch_skinny_v<16, false, 2>(a, ak, bk, grid, s);
+            else
+                a.segs ? launch_skinny_v<16, true, SST>(a, ak, bk, grid, s)
+                       : launch_skinny_v<16, false, SST>(a, ak, bk, grid, s);
         } else {
             dim3 grid((lng + SBN - 1) / SBN, (shrt + 31) / 32, zsplit);
-            a.segs ? launch_skinny_v<32, true>(a, ak, bk, grid, s) : launch_skinny_v<32, false>(a, ak, bk, grid, s);
+            if (two)
+                a.segs ? launch_skinny_v<32, true, 2>(a, ak, bk, grid, s) : launch_skinny_v<32, false, 2>(a, ak, bk, grid, s);
+            else
+                a.segs ? launch_skinny_v<32, true, SST>(a, ak, bk, grid, s)
+                       : launch_skinny_v<32, false, SST>(a, ak, bk, grid, s);
         }
         return;
     }

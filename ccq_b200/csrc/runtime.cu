@@ -2026,7 +2026,10 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
                 const TuneCfg cur{o.g.tile, o.g.kchunk, use_split(c, o) ? (split_persistent(o) ? 2 : 1) : 0};
                 cand.push_back(cur);
                 std::vector<int> tiles = {1};
-                if (std::min(M, N) <= 32) tiles.push_back(2);
+                if (std::min(M, N) <= 32) {
+                    tiles.push_back(2);
+                    tiles.push_back(5);
+                }
                 for (int tl : tiles) {
                     std::vector<long long> ch;
                     if (o.g.segs) {
@@ -2097,7 +2100,7 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
 
 int ccq_b200_force_tile(ccq_b200_ctx *c, int64_t tile) {
     if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
-    if (tile < 0 || tile > 4) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..4"));
+    if (tile < 0 || tile > 5) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..5"));
     for (auto &o : c->plan.ops) {
         if (o.kind != OP_GETT || o.g.K == 0) continue;
         o.g.tile = (int)tile;

@@ -159,7 +159,8 @@ int ccq_b200_iterate_wait(ccq_b200_ctx *ctx, double *e_cor, double *residuum, in
 int ccq_b200_autotune(ccq_b200_ctx *ctx, int64_t reps, double *ms_default, double *ms_tuned);
 /* Pins every contraction to one GETT kernel family: 0 = by shape, 1 = 64 x 64
  * DMMA tiles, 2 = skinny DMMA tiles (where one side is <= 32), 3 = small-K
- * FMA kernel, 4 = 64 x 64 DMMA tiles with a 3-stage operand pipeline.  A family that does not fit a shape falls back to the shape's
+ * FMA kernel, 4 = 64 x 64 DMMA tiles with a 3-stage operand pipeline, 5 = skinny
+ * DMMA tiles with a 2-stage ring.  A family that does not fit a shape falls back to the shape's
  * default.  For tests and experiments; ccq_b200_autotune picks per contraction. */
 int ccq_b200_force_tile(ccq_b200_ctx *ctx, int64_t tile);
 

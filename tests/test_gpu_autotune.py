@@ -72,7 +72,7 @@ def test_tuned_solve_matches_untuned(prec):
     assert abs(res[True].iterations - res[False].iterations) <= 1
 
 
-@pytest.mark.parametrize('tile', [1, 2, 3, 4])
+@pytest.mark.parametrize('tile', [1, 2, 3, 4, 5])
 @pytest.mark.parametrize('method,n,oa,ob', [('CCSD', 7, 3, 2), ('CCSDT', 7, 3, 2)])
 def test_forced_kernel_family_matches_oracle(tile, method, n, oa, ob, plan_text):
     """Every contraction on one GETT family (64 x 64 DMMA, skinny DMMA, small-K FMA)."""
