@@ -1,7 +1,7 @@
 """Single-kernel probes for profiling (one GETT launch of a fixed shape).
 
     python -m ccq_b200.probe egemm K1 K2 K3 [repeats]
-    python -m ccq_b200.probe egemm_split K1 K2 K3 [slices]
+    python -m ccq_b200.probe egemm_split K1 K2 K3 [slices] [tile|persistent]
     python -m ccq_b200.probe sweep fp64|split OUTFILE [warm-up iterations] [0|1|2|3|tune]
     python -m ccq_b200.probe warmstart CCSDT|CCSDTQ NORB NEL [COUNT TRAIN EPOCHS]
 
@@ -34,14 +34,18 @@ def main(argv):
     elif kind == 'egemm_split':
         k1, k2, k3 = (int(x) for x in argv[1:4])
         S = int(argv[4]) if len(argv) > 4 else 4
+        persistent = (argv[5] == 'persistent') if len(argv) > 5 else None
         rng = np.random.default_rng(0)
         A = np.asfortranarray(rng.normal(size=(k3, k1)))
         B = np.asfortranarray(rng.normal(size=(k3, k2)))
-        C = lib.egemm_split(k1, k2, k3, A, B, S)
+        for _ in range(3 if persistent is not None else 1):
+            C = lib.egemm_split(k1, k2, k3, A, B, S, persistent=persistent)
         ref = B[:, :64].T @ A[:, :64]
         err = float(np.abs(C[:64, :64] - ref).max())
-        print(f'egemm_split {k1}x{k2}x{k3} S={S}: max err {err:.2e}')
-        assert err < 1e-5
+        # the split bound: 2^(-7S+2) k3 max|A| max|B|
+        bound = 2.0 ** (-7 * S + 2) * k3 * np.abs(A[:, :64]).max() * np.abs(B[:, :64]).max()
+        print(f'egemm_split {k1}x{k2}x{k3} S={S}: max err {err:.2e} (bound {bound:.2e})')
+        assert err <= bound
     elif kind == 'sweep':
         # per-operation device times of one CCSDT sweep on the 40-orbital workload
         import os
