@@ -62,11 +62,15 @@ class Config:
     gpu_fp64_finish: float = 1.0e-6
     gpu_graph: bool = True
     gpu_autotune: bool = False
+    act_occ: int = -1
+    act_unocc: int = -1
     # derived (process_sys_data)
     froz: int = 0
     occ_a: int = 0
     occ_b: int = 0
     orbs: int = 0
+    act_occ_b: int = 0
+    act_unocc_a: int = 0
     lvl_t: bool = False
     lvl_q: bool = False
     extra: dict = field(default_factory=dict)
@@ -76,6 +80,9 @@ class Config:
         self.occ_a = self.nel // 2
         self.occ_b = self.occ_a - _ftrunc_div(self.mult - 1, 2)
         self.orbs = (self.nel + self.nvirt) // 2
+        # active space (process_sys_data, src/parser.f90:495-499)
+        self.act_occ_b = max(self.occ_b - self.act_occ, self.froz)
+        self.act_unocc_a = min(self.occ_a + self.act_unocc, self.orbs)
         return self
 
     def bin_path(self):
@@ -92,12 +99,17 @@ class Config:
             self.lvl_t, self.lvl_q = True, False
         elif ct == 'CCSDTQ':
             self.lvl_t, self.lvl_q = True, True
+        elif ct == 'CCSDt':
+            # src/parser.f90:380-388: active-space triples with act_ind_t = 1
+            if self.act_occ == -1 and self.act_unocc == -1:
+                raise ValueError('CONFIGURATION ERROR: Active space methods require an active space')
+            self.lvl_t, self.lvl_q = True, False
         elif ct == 'CR-CC(2,3)':
             # src/parser.f90:368-377: CCSD, then hbar, left CCSD and the MM(2,3) correction
             self.lvl_t, self.lvl_q = False, False
         else:
             raise ValueError(f'calc_type {ct!r} is not served by this engine '
-                             '(CCSD, CCSDT, CCSDTQ, CR-CC(2,3) are; the others stay on the CPU program)')
+                             '(CCSD, CCSDT, CCSDTQ, CCSDt, CR-CC(2,3) are; the others stay on the CPU program)')
         return self
 
 
@@ -180,6 +192,10 @@ def _apply(cfg, key, val):
         cfg.gpu_graph = _logical(val)
     elif key == 'gpu_autotune':
         cfg.gpu_autotune = _logical(val)
+    elif key == 'act_occ':
+        cfg.act_occ = int(val)
+    elif key == 'act_unocc':
+        cfg.act_unocc = int(val)
     else:
         cfg.extra[key] = val
 

@@ -1043,6 +1043,17 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
                         D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[e][d]];
                 }
                 tnew = a.T[toff] - R[e] / D;
+                if (a.act) {
+                    bool occ = false, vir = false;
+#pragma unroll
+                    for (int d = 0; d < RK; ++d) {
+                        if (d < RK / 2)
+                            occ = occ || x[e][d] >= a.act_occ_lo;
+                        else
+                            vir = vir || x[e][d] < a.act_vir_hi[a.spin[d]];
+                    }
+                    if (!(occ && vir)) tnew = 0.0;
+                }
             } else {
                 tnew = R[e];
             }

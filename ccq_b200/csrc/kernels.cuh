@@ -98,6 +98,11 @@ struct AsmArgs {
     const unsigned char *combos;
     int off32;                // every offset (terms, T, canonical index) fits in 32 bits
     int nplain;               // terms [0, nplain) read plain views (no sorted groups); the rest sorted
+    // active-space triples (mode 0 only): an element is kept when at least one occupied index is
+    // >= act_occ_lo and at least one virtual index is < act_vir_hi[spin]; the others are set to zero
+    int act;
+    int act_occ_lo;
+    int act_vir_hi[2];
 };
 
 // FP64 GETT.  Tile family by output shape: 0 = 64 x 64 tiles; 1 = skinny rows

@@ -2098,6 +2098,35 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
     }
 }
 
+int ccq_b200_set_active(ccq_b200_ctx *c, int64_t act_occ_b, int64_t act_unocc_a) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        if (c->calc_type != "CCSDT") throw Error(CCQ_B200_EINVAL, "set_active: a CCSDT context is required");
+        const long long occ_a = c->froz + c->oa, occ_b = c->froz + c->ob, orbs = occ_a + c->va;
+        if (act_occ_b < c->froz || act_occ_b > occ_b || act_unocc_a < occ_a || act_unocc_a > orbs)
+            throw Error(CCQ_B200_EINVAL, "set_active: froz <= act_occ_b <= occ_b and occ_a <= act_unocc_a <= orbs");
+        for (auto &o : c->plan.ops) {
+            if (o.kind != OP_ASM || o.block[1] != '3' || o.asmargs.mode != 0) continue;
+            AsmArgs &a = o.asmargs;
+            // spatial orbitals above act_occ_b (occupied) and up to act_unocc_a (virtual) are active,
+            // for both spins; indices here count from froz (occupied) and from occ (virtual)
+            a.act = 1;
+            a.act_occ_lo = (int)(act_occ_b - c->froz);
+            a.act_vir_hi[0] = (int)(act_unocc_a - occ_a);
+            a.act_vir_hi[1] = (int)(act_unocc_a - occ_b);
+        }
+        // kernel arguments are recorded in the captured graphs
+        if (c->gexec) cudaGraphExecDestroy(c->gexec);
+        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
+        c->gexec = c->lgexec = nullptr;
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
 int ccq_b200_force_tile(ccq_b200_ctx *c, int64_t tile) {
     if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
     if (tile < 0 || tile > 5) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..5"));

@@ -190,9 +190,13 @@ def run(input_path, out=print, base_dir='.'):
     out(f"  Reference energy {sysd['e_ref']:.12f}")
     out('Coupled cluster')
     out('---------------')
-    ctx = lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, cfg.calc_type, sysd['f_a'], sysd['f_b'],
+    # CCSDt runs the CCSDT plan with the triples held to the active space
+    ctype = 'CCSDT' if cfg.calc_type == 'CCSDt' else cfg.calc_type
+    ctx = lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, ctype, sysd['f_a'], sysd['f_b'],
                       sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
                       diis_space=cfg.diis_space)
+    if cfg.calc_type == 'CCSDt':
+        ctx.set_active(cfg.act_occ_b, cfg.act_unocc_a)
     cfg.bin_file = cfg.bin_path()
     if not os.path.isabs(cfg.bin_file):
         cfg.bin_file = os.path.join(base_dir, cfg.bin_file)

@@ -57,6 +57,7 @@ SIGNATURES = {
     'ccq_b200_set_precision': (C.c_int, [C.c_void_p, I64, I64]),
     'ccq_b200_autotune': (C.c_int, [C.c_void_p, I64, DP, DP]),
     'ccq_b200_force_tile': (C.c_int, [C.c_void_p, I64]),
+    'ccq_b200_set_active': (C.c_int, [C.c_void_p, I64, I64]),
     'ccq_b200_use_graph': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), DP, DP]),
     'ccq_b200_timing': (C.c_int, [C.c_void_p, DP, DP]),
@@ -264,6 +265,10 @@ class Context:
         a, b = C.c_double(), C.c_double()
         _err(self._lib.ccq_b200_autotune(self.ptr, reps, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def set_active(self, act_occ_b, act_unocc_a):
+        """CCSDt: triples with >= 1 active occupied and >= 1 active virtual index (ccq's boundaries)."""
+        _err(self._lib.ccq_b200_set_active(self.ptr, act_occ_b, act_unocc_a))
 
     def force_tile(self, tile):
         """Every contraction on one kernel family (0 shape default, 1 64x64, 2 skinny, 3 small-K, 4 64x64 3-stage,

@@ -157,6 +157,15 @@ int ccq_b200_iterate_wait(ccq_b200_ctx *ctx, double *e_cor, double *residuum, in
  * *ms_default / *ms_tuned = summed per-contraction times before / after.
  * Re-run after ccq_b200_set_precision to tune the other mode. */
 int ccq_b200_autotune(ccq_b200_ctx *ctx, int64_t reps, double *ms_default, double *ms_tuned);
+/* Active-space CCSDt (calc_type=CCSDt, src/parser.f90:380-388 with
+ * act_ind_t = 1): on a CCSDT context, keeps only the triples with at least
+ * one active occupied and at least one active virtual index and holds the
+ * others at zero.  Active: spatial orbitals act_occ_b < p <= occ (occupied)
+ * and occ < p <= act_unocc_a (virtual), both spins, with ccq's
+ * act_occ_b = max(occ_b - act_occ, froz), act_unocc_a = min(occ_a + act_unocc,
+ * orbs) (src/parser.f90:495-499; 1-based). */
+int ccq_b200_set_active(ccq_b200_ctx *ctx, int64_t act_occ_b, int64_t act_unocc_a);
+
 /* Pins every contraction to one GETT kernel family: 0 = by shape, 1 = 64 x 64
  * DMMA tiles, 2 = skinny DMMA tiles (where one side is <= 32), 3 = small-K
  * FMA kernel, 4 = 64 x 64 DMMA tiles with a 3-stage operand pipeline, 5 = skinny

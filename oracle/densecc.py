@@ -15,8 +15,31 @@ from oracle.spinorb import SpinOrbitalSystem
 METHOD = {'CCSD': (2,), 'CCSDT': (2, 3), 'CCSDTQ': (2, 3, 4)}
 
 
+def active_mask(name, shape, dims, active):
+    """CCSDt triples kept: >= 1 active occupied and >= 1 active virtual index.
+
+    ``active = (act_occ_b, act_unocc_a)``: ccq's boundaries (``src/parser.f90:495-499``,
+    ``src/update_cc.F90:412-440``): occupied spatial orbitals above act_occ_b and
+    virtual ones up to act_unocc_a are active, for both spins.
+    """
+    m1, m2 = active
+    nb = 'ABCD'.index(name[2])
+    spins = [0] * (3 - nb) + [1] * nb
+    occ_any = np.zeros(shape, dtype=bool)
+    vir_any = np.zeros(shape, dtype=bool)
+    for d in range(3):
+        idx = np.arange(shape[d]).reshape([-1 if e == d else 1 for e in range(6)])
+        occ_any |= np.broadcast_to(idx >= m1 - dims.froz, shape)
+    for d in range(3):
+        occ = dims.occ_a if spins[d] == 0 else dims.occ_b
+        idx = np.arange(shape[3 + d]).reshape([-1 if e == 3 + d else 1 for e in range(6)])
+        vir_any |= np.broadcast_to(idx < m2 - occ, shape)
+    return occ_any & vir_any
+
+
 class DenseCC:
-    def __init__(self, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, method, shift=0.0, rhf=False):
+    def __init__(self, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, method, shift=0.0, rhf=False, active=None):
+        self.active = active   # CCSDt: (act_occ_b, act_unocc_a), triples outside the active space held at zero
         self.dims = dims
         self.method = method
         self.tranks = METHOD[method]
@@ -56,6 +79,8 @@ class DenseCC:
                 Rb = self.so.to_blocks({level: R}, [name])[name]
                 D = S.denominator(name, blocks[name].shape, fda, fdb, self.dims, self.shift)
                 new = S.jacobi_block(name, blocks[name], Rb, D)
+                if self.active is not None and level == 3:
+                    new = np.where(active_mask(name, new.shape, self.dims, self.active), new, 0.0)
             if name in self.t4:
                 self.t4[name] = new
             else:
