@@ -37,7 +37,7 @@ WORKLOAD = 'CCSDT, 40 spatial orbitals, nel=16, nvir=64, L=80, sigma=0.025, seed
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument('--gpus', type=int, default=1)
-    p.add_argument('--steps', type=int, default=12)
+    p.add_argument('--steps', type=int, default=40)
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     p.add_argument('--precision', default='auto', choices=['auto', 'split', 'fp64'])
@@ -92,6 +92,7 @@ def job_seconds_per_iter(ms_total_rank, world, steps):
 
 
 class Clocks:
+    """nvidia-smi samples every 50 ms; the summary keeps the samples taken inside the timed window."""
     FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
               'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
@@ -100,16 +101,27 @@ class Clocks:
         self.local = local
         self.proc = None
         self.path = os.path.join(ROOT, 'gpurun_out', f'clocks_rank{local}.csv')
+        self.stamps = []   # (host time, line count) when the timed window opens and closes
 
     def start(self):
+        """Starts sampling (before the warm-up, so that the sampler runs when the timed window opens)."""
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, 'w')
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.local), f'--query-gpu={self.FIELDS}',
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', '50'],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+
+    def mark(self):
+        """Opens or closes the timed window: the number of samples written so far."""
+        try:
+            self.fh.flush()
+            with open(self.path) as fh:
+                self.stamps.append(sum(1 for _ in fh))
+        except Exception:
+            self.stamps.append(None)
 
     def stop(self):
         if not self.proc:
@@ -122,7 +134,13 @@ class Clocks:
         self.fh.close()
         sm, smax, reasons = [], [], set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for line in open(self.path):
+        lines = open(self.path).readlines()
+        window = 'timed region'
+        if len(self.stamps) == 2 and None not in self.stamps and self.stamps[1] > self.stamps[0]:
+            lines = lines[self.stamps[0]:self.stamps[1]]
+        else:
+            window = 'warm-up and timed region'
+        for line in lines:
             f = [x.strip() for x in line.split(',')]
             if len(f) < 9:
                 continue
@@ -137,7 +155,7 @@ class Clocks:
         if not sm:
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no samples']}
         return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': max(smax), 'reasons': sorted(reasons),
-                'samples': len(sm)}
+                'samples': len(sm), 'window': window}
 
 
 def measure_peaks():
@@ -427,14 +445,17 @@ def main():
             before, after = ctx.autotune(3)
             tuning[leg] = {'gett_ms_heuristic': before, 'gett_ms_tuned': after,
                            'wall_s': time.perf_counter() - t0}
+        if leg == headline:
+            clocks.start()
         # warm-up continues the same solve (iterations keep counting, DIIS on schedule)
         for _ in range(args.warmup):
             ctx.iterate(it)
             it += 1
         if leg == headline:
-            clocks.start()
+            clocks.mark()
         ms, es = time_leg(ctx, it, args.steps, world)
         if leg == headline:
+            clocks.mark()
             clk = clocks.stop()
         it += args.steps
         st = ctx.stats()
