@@ -7,11 +7,13 @@ network predicts the remaining correction per amplitude,
     t2_init = mp2 * (1 + r),   r = net(features)
 
 where the features are symmetric under the antisymmetry of the amplitude
-(gap D, the occupied and virtual orbital-energy sums, log |mp2|, log |v|, and
-the family parameter lambda), so t2_init keeps the antisymmetry of mp2 and
-vanishes where mp2 does.  T1 starts at zero and T3 / T4 are built by the first
-sweep from the predicted T2.  The exact CC iteration to the same tol decides
-the result: the warm start only changes where the iteration starts.
+(gap D, the occupied and virtual orbital-energy sums, log |mp2|, log |v|, the
+family parameter lambda, and, from the nearest solved member of the family
+(the anchor), its converged ratio t/mp2 - 1 at the same element and the lambda
+distance to it), so t2_init keeps the antisymmetry of mp2 and vanishes where
+mp2 does.  T1 and T3 start from the anchor's converged values (zero without an
+anchor); T4 is built by the first sweep.  The exact CC iteration to the same
+tol decides the result: the warm start only changes where the iteration starts.
 
 Training and inference run in this library's kernels (``ccq_b200_mlp_*``,
 ``csrc/mlp.cu``): forward, backward (mean-squared loss) and Adam, FP32.
@@ -27,7 +29,7 @@ import numpy as np
 from . import integrals as I
 from . import lib, synth
 
-NFEAT = 6
+NFEAT = 8
 C4_SEED = 4000
 C4_COUNT = 200
 C4_TRAIN = 150
@@ -65,11 +67,13 @@ def _check(code):
         raise lib.CCQB200Error(code, 'warm-start network kernel failed')
 
 
-def block_features(fdiag_o, fdiag_v, v_block, lam):
+def block_features(fdiag_o, fdiag_v, v_block, lam, anchor_ratio=None, dlam=0.0):
     """Features and MP2 amplitudes of one stored T2 block.
 
     fdiag_o = (occ energies of the two occupied axes), fdiag_v likewise;
-    v_block[i, j, a, b] = <ij||ab> in the block's spin pattern.
+    v_block[i, j, a, b] = <ij||ab> in the block's spin pattern; anchor_ratio =
+    the anchor's converged t/mp2 - 1 on this block (zero without an anchor),
+    dlam = lambda - the anchor's lambda.
     Returns (X [N, NFEAT], mp2 [N]) over every stored element, and the block shape.
     """
     eo1, eo2 = fdiag_o
@@ -80,14 +84,34 @@ def block_features(fdiag_o, fdiag_v, v_block, lam):
     mp2 = -v_block / gap
     shape = v_block.shape
     tiny = 1e-300
+    ar = np.zeros(shape) if anchor_ratio is None else np.asarray(anchor_ratio).reshape(shape)
     X = np.stack([gap, np.broadcast_to(eo, shape), np.broadcast_to(ev, shape),
                   np.log(np.abs(mp2) + tiny), np.log(np.abs(v_block) + tiny),
-                  np.full(shape, lam)], axis=-1).reshape(-1, NFEAT)
+                  np.full(shape, lam), ar, np.full(shape, dlam)], axis=-1).reshape(-1, NFEAT)
     return X, mp2.reshape(-1), shape
 
 
-def system_blocks(s, lam):
-    """(name, X, mp2, shape) for T2A, T2B, T2C of a system from ``synth.system``."""
+def ratios(mp2, t, cut=1e-6):
+    """t / mp2 - 1 where |mp2| exceeds cut * max |mp2| (else 0), clipped to [-2, 2]."""
+    r = np.zeros_like(mp2)
+    m = np.abs(mp2) > cut * np.abs(mp2).max()
+    r[m] = np.clip((t[m] - mp2[m]) / mp2[m], -2.0, 2.0)
+    return r
+
+
+def anchor_of(spec, t):
+    """(lambda, {block: converged t/mp2 - 1}) of a solved family member (t: its t_vec)."""
+    s = synth.system(spec)
+    lay = tlayout(s)
+    out = {}
+    for name, X, mp2, shape in system_blocks(s, spec.lam):
+        out[name] = ratios(mp2, np.asarray(lay.view(t, name)).reshape(-1)).reshape(shape)
+    return spec.lam, out
+
+
+def system_blocks(s, lam, anchor=None):
+    """(name, X, mp2, shape) for T2A, T2B, T2C of a system from ``synth.system``;
+    anchor = ``anchor_of`` of the nearest solved family member, or None."""
     d = s['dims']
     fr = d.froz
     fa = np.diag(s['f_a'])[fr:]
@@ -99,7 +123,9 @@ def system_blocks(s, lam):
             ('T2A', (fa[:oa], fa[:oa], fa[oa:], fa[oa:], vaa[:oa, :oa, oa:, oa:])),
             ('T2B', (fa[:oa], fb[:ob], fa[oa:], fb[ob:], vab[:oa, :ob, oa:, ob:])),
             ('T2C', (fb[:ob], fb[:ob], fb[ob:], fb[ob:], vbb[:ob, :ob, ob:, ob:]))):
-        X, mp2, shape = block_features((eoa, eob), (eva, evb), np.asarray(v), lam)
+        ar = None if anchor is None else anchor[1][name]
+        dl = 0.0 if anchor is None else lam - anchor[0]
+        X, mp2, shape = block_features((eoa, eob), (eva, evb), np.asarray(v), lam, ar, dl)
         out.append((name, X, mp2, shape))
     return out
 
@@ -132,15 +158,15 @@ class WarmStart:
     # -- data -------------------------------------------------------------------
     @staticmethod
     def samples(specs_and_t2, cut=1e-6):
-        """Training samples from (spec, {block: converged T2 array}) pairs.
+        """Training samples from (spec, {block: converged T2 array}, anchor) triples.
 
         Target r = (t - mp2) / mp2 on elements whose |mp2| exceeds cut * max|mp2|,
         clipped to [-2, 2].
         """
         xs, ys = [], []
-        for spec, t2 in specs_and_t2:
+        for spec, t2, anchor in specs_and_t2:
             s = synth.system(spec)
-            for name, X, mp2, shape in system_blocks(s, spec.lam):
+            for name, X, mp2, shape in system_blocks(s, spec.lam, anchor):
                 t = np.asarray(t2[name]).reshape(-1)
                 m = np.abs(mp2) > cut * np.abs(mp2).max()
                 r = np.clip((t[m] - mp2[m]) / mp2[m], -2.0, 2.0)
@@ -196,10 +222,11 @@ class WarmStart:
                                            torch.cuda.current_stream().cuda_stream))
         return Y.cpu().numpy().astype(np.float64) * self.ysd
 
-    def initial_t(self, s, lam, layout):
-        """A full t_vec (reference layout) with T2 = mp2 (1 + r), everything else zero."""
-        t = np.zeros(layout.t_size)
-        for name, X, mp2, shape in system_blocks(s, lam):
+    def initial_t(self, s, lam, layout, anchor=None, t_anchor=None):
+        """A full t_vec (reference layout): T2 = mp2 (1 + r); T1 and T3 from the anchor's
+        converged t_vec ``t_anchor`` when given, else zero."""
+        t = np.zeros(layout.t_size) if t_anchor is None else np.array(t_anchor, dtype=np.float64)
+        for name, X, mp2, shape in system_blocks(s, lam, anchor):
             r = np.clip(self.predict_ratio(X), -2.0, 2.0)
             layout.view(t, name)[...] = (mp2 * (1.0 + r)).reshape(shape)
         return t
@@ -237,11 +264,18 @@ def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1
     t0 = time.perf_counter()
     plain, _ = batch.solve_batch(specs, tol=tol, calc_type=method, keep_t=True)
     t1 = time.perf_counter()
+    anchors = {i: anchor_of(specs[i], plain[i]['t']) for i in tr}
+
+    def nearest(i, exclude_self):
+        # the solved training member closest in lambda (another one for a training member)
+        cand = [j for j in tr if not (exclude_self and j == i)]
+        return min(cand, key=lambda j: (abs(specs[j].lam - specs[i].lam), j))
     data = []
     for i in tr:
         s = synth.system(specs[i])
         lay = tlayout(s)
-        data.append((specs[i], {b: lay.view(plain[i]['t'], b) for b in ('T2A', 'T2B', 'T2C')}))
+        data.append((specs[i], {b: lay.view(plain[i]['t'], b) for b in ('T2A', 'T2B', 'T2C')},
+                     anchors[nearest(i, True)]))
     X, y = WarmStart.samples(data)
     ws = WarmStart(seed=seed)
     ws.fit_scaling(X, y)
@@ -251,7 +285,8 @@ def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1
     for i in ev:
         s = synth.system(specs[i])
         lay = tlayout(s)
-        inits.append(ws.initial_t(s, specs[i].lam, lay))
+        a = nearest(i, False)
+        inits.append(ws.initial_t(s, specs[i].lam, lay, anchors[a], plain[a]['t']))
         mp2s.append(mp2_t(s, lay))
     warm, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=inits)
     t3 = time.perf_counter()

@@ -27,7 +27,30 @@ def test_features_keep_the_amplitude_symmetry():
         if name in ('T2A', 'T2C'):
             # antisymmetric mp2, symmetric features: mp2 * (1 + r(x)) stays antisymmetric
             assert np.allclose(m, -m.transpose(1, 0, 2, 3))
-            assert np.allclose(Xr[..., [0, 1, 2, 3, 4, 5]], Xr.transpose(1, 0, 2, 3, 4))
+            assert np.allclose(Xr, Xr.transpose(1, 0, 2, 3, 4))
+            assert np.allclose(Xr, Xr.transpose(0, 1, 3, 2, 4))
+
+
+def test_anchor_features_keep_the_symmetry():
+    """The anchor's converged ratio t/mp2 - 1 is symmetric where mp2 is antisymmetric."""
+    spec = synth.SynthSpec(8, 4, 16, 0.03, 4000, 1.1)
+    s = synth.system(spec)
+    lay = warmstart.tlayout(s)
+    rng = np.random.default_rng(3)
+    t = np.zeros(lay.t_size)
+    for name, X, mp2, shape in warmstart.system_blocks(s, 1.1):
+        # an antisymmetric stand-in for a converged T2: mp2 times a symmetric factor
+        f = 1.0 + 0.1 * rng.normal(size=shape)
+        if name in ('T2A', 'T2C'):
+            f = 0.25 * (f + f.transpose(1, 0, 2, 3) + f.transpose(0, 1, 3, 2) + f.transpose(1, 0, 3, 2))
+        lay.view(t, name)[...] = mp2.reshape(shape) * f
+    anchor = warmstart.anchor_of(spec, t)
+    s2 = synth.system(synth.SynthSpec(8, 4, 16, 0.03, 4000, 1.3))
+    for name, X, mp2, shape in warmstart.system_blocks(s2, 1.3, anchor):
+        Xr = X.reshape(shape + (warmstart.NFEAT,))
+        assert np.allclose(Xr[..., 7], 1.3 - 1.1)
+        if name in ('T2A', 'T2C'):
+            assert np.allclose(Xr, Xr.transpose(1, 0, 2, 3, 4))
             assert np.allclose(Xr, Xr.transpose(0, 1, 3, 2, 4))
 
 
