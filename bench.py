@@ -472,14 +472,20 @@ def main():
                         'launches_per_iter': st['launches'], 'flops_per_iter': st['flops']}
     head = results[headline]
 
-    # per-kernel roofline: eager sweep with events around every launch
+    # per-kernel roofline: eager sweep with events around every launch (and every launch's shape in a dump)
     ctx.set_precision(lib.PREC_SPLIT if headline == 'split' else lib.PREC_FP64, args.slices)
+    dump = os.path.join(ROOT, 'gpurun_out', f'bench_ops_rank{rank}.txt')
+    os.makedirs(os.path.dirname(dump), exist_ok=True)
+    if os.path.exists(dump):
+        os.remove(dump)
+    os.environ['CCQ_B200_PROFILE_DUMP'] = dump
     ctx.profile(True)
     for _ in range(2):
         ctx.iterate(it)
         it += 1
     prof = ctx.profile_get()
     ctx.profile(False)
+    del os.environ['CCQ_B200_PROFILE_DUMP']
     # dominant kernel of the headline leg = largest share of device time
     kname = max(('gett_f64', 'gett_split', 'assemble'), key=lambda k: prof[k]['ms'])
     per_sweep = {k: {'ms': v['ms'] / 2, 'launches': v['launches'] // 2, 'flops': v['flops'] / 2}
@@ -505,12 +511,39 @@ def main():
                 'fp64_equivalent_tflops': p_['flops'] / (p_['ms'] * 1e-3) / 1e12,
                 'note': 'time includes the slicing kernels of each split GETT'}
 
+    def per_launch_roofline(fp64_peak, hbm_gbs):
+        """gett_f64 launches against their own bound: max(FLOPs / DGEMM peak, algorithmic bytes / HBM)."""
+        bound = spent = 0.0
+        nl = 0
+        try:
+            lines = open(dump).read().split('\n')
+        except OSError:
+            return None
+        for ln in lines:
+            f = ln.split()
+            if len(f) < 13 or f[1] != 'GETT' or f[2] != '0':
+                continue
+            M, N, K, beta, ms, fl = int(f[4]), int(f[5]), int(f[6]), int(f[9]), float(f[10]), float(f[12])
+            if M * N == 0 or ms <= 0:
+                continue
+            keff = fl / (2.0 * M * N)
+            by = 8.0 * (M + N) * keff + (16.0 if beta else 8.0) * M * N
+            bound += max(fl / (fp64_peak * 1e12), by / (hbm_gbs * 1e9)) * 1e3
+            spent += ms
+            nl += 1
+        if not spent:
+            return None
+        return {'frac': bound / spent, 'bound_ms': bound / 2, 'spent_ms': spent / 2, 'launches': nl // 2,
+                'note': 'per launch max(2MNK / measured DGEMM peak, 8(M+N)K + 8 or 16 MN bytes / measured HBM), '
+                        'summed over the gett_f64 launches of 2 eager sweeps, over their summed event times'}
+
     if kname == 'assemble':
         # bytes: every gather term of every canonical element + the block written once (8 B each)
         roofline = {'bound': 'hbm', 'achieved': None, 'peak': peaks_file['hbm_gbs'], 'unit': 'GB/s', 'frac': None}
     else:
         roofline = dict(gett_line(kname))
     roofline.update({'kernel': kname, 'traffic': None, 'shares': shares, 'per_sweep': per_sweep,
+                     'per_launch_bound': per_launch_roofline(fp64_peak, peaks_file['hbm_gbs']),
                      'secondary': {k: gett_line(k) for k in ('gett_f64', 'gett_split') if k != kname},
                      'traffic_note': 'per-launch DRAM bytes vary by contraction shape; ncu figures for the dominant '
                                      'shapes are in profiles/gett_f64_ccsdt40_shapes.md and profiles/split_gett_o4v4.md',

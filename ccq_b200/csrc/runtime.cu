@@ -1206,12 +1206,12 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
             int k = op_class(c, o);
             c->prof_ms[k] += ms;
             c->prof_launch[k] += 1;
-            if (o.kind == OP_GETT)
-                c->prof_flops[k] += o.group_size ? o.group_flops : 2.0 * o.mnk[0] * o.mnk[1] * o.mnk[2];
+            const double fl = o.group_size ? o.group_flops : 2.0 * o.mnk[0] * o.mnk[1] * o.mnk[2];
+            if (o.kind == OP_GETT) c->prof_flops[k] += fl;
             if (df) {
                 if (o.kind == OP_GETT)
-                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f %d\n", i, k, o.tag.c_str(), o.mnk[0],
-                            o.mnk[1], o.mnk[2], o.akm, o.bkm, o.beta, ms, o.group_size);
+                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f %d %.6e\n", i, k, o.tag.c_str(),
+                            o.mnk[0], o.mnk[1], o.mnk[2], o.akm, o.bkm, o.beta, ms, o.group_size, fl);
                 else if (o.kind == OP_ASM)
                     fprintf(df, "%zu ASM %d %s %d %.6f\n", i, k, o.block.c_str(), o.asmargs.nterms, ms);
                 else
