@@ -1974,6 +1974,7 @@ static float time_cfg(ccq_b200_ctx *c, Op &o, const TuneCfg &t, double *scratch,
 int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double *ms_tuned) {
     try {
         if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "autotune: an iteration is pending");
         if (reps < 1) reps = 3;
         CK(cudaSetDevice(c->device));
         CK(cudaStreamSynchronize(c->stream));
