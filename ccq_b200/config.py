@@ -12,7 +12,9 @@ split), ``gpu_slices`` (int8 slices per operand), ``gpu_fp64_finish`` (|dE|
 below which the split mode hands over to FP64), ``gpu_graph`` (replay each
 sweep as one CUDA graph), ``gpu_autotune`` (time every contraction's tile and
 split-K candidates once before the first iteration and keep the fastest),
-``gpu_checkpoint_every`` (write the checkpoint every N iterations).  The
+``gpu_checkpoint_every`` (write the checkpoint every N iterations),
+``gpu_external_t`` (externally corrected CC: T3 / T4 from a .npz file, held
+fixed while T1 and T2 iterate).  The
 reference's ``fcidump``, ``restart`` and ``output_bin`` keys are served:
 ``restart`` resumes t_vec, T4 and the DIIS ring from ``output_bin``.
 """
@@ -62,6 +64,7 @@ class Config:
     gpu_fp64_finish: float = 1.0e-6
     gpu_graph: bool = True
     gpu_autotune: bool = False
+    gpu_external_t: str = ''
     act_occ: int = -1
     act_unocc: int = -1
     # derived (process_sys_data)
@@ -192,6 +195,8 @@ def _apply(cfg, key, val):
         cfg.gpu_graph = _logical(val)
     elif key == 'gpu_autotune':
         cfg.gpu_autotune = _logical(val)
+    elif key == 'gpu_external_t':
+        cfg.gpu_external_t = val
     elif key == 'act_occ':
         cfg.act_occ = int(val)
     elif key == 'act_unocc':

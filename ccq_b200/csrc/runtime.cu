@@ -114,6 +114,7 @@ struct Op {
     double group_flops = 0.0;  // FLOPs of a grouped launch (leader only)
     int group_size = 0;
     int split_choice = -1;     // -1 by shape (split_eligible); autotuned: 0 DMMA, 1 per-tile split kernel, 2 persistent
+    bool frozen = false;       // in a T3 / T4 phase of an externally corrected solve: not run
     std::vector<size_t> group_ops;   // every op of a grouped launch (leader only; members are skipped)
     std::vector<int> hcm, hcn; // output offset tables (grouping key)
     AsmArgs asmargs{};
@@ -257,6 +258,7 @@ struct ccq_b200_ctx {
     std::vector<void *> owned;
     double *tvec = nullptr;
     long long t_size = 0, vec_size = 0;
+    long long vec_full = 0, vec_t12 = 0;   // DIIS vector sizes: the method's and T1 + T2 only
     double *ring = nullptr;
     double *scratch = nullptr;  // residuum / gram / coef
     int *dinfo = nullptr;
@@ -442,6 +444,8 @@ void instantiate(ccq_b200_ctx *c) {
     c->t_size = off;
     // CR-CC(2,3) solves CCSD; its DIIS vector is T1 + T2 (the T3 slots stay zero)
     c->vec_size = (c->calc_type == "CCSD" || c->calc_type == "CR-CC(2,3)") ? tv_off["T3A"] : c->t_size;
+    c->vec_full = c->vec_size;
+    c->vec_t12 = tv_off["T3A"];
     // left amplitudes (L1A..L2C) share the T1/T2 layout in their own vector
     std::map<std::string, long long> lv_off;
     {
@@ -1047,6 +1051,7 @@ int op_class(const ccq_b200_ctx *c, const Op &o) {
 }
 
 void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
+    if (o.frozen) return;
     switch (o.kind) {
         case OP_GETT:
             if (o.skip || o.g.M == 0 || o.g.N == 0) break;
@@ -1135,7 +1140,7 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
     };
     for (size_t i = from; i < to; ++i) {
         Op &o = c->plan.ops[i];
-        if (o.kind == OP_PHASE) continue;
+        if (o.kind == OP_PHASE || o.frozen) continue;
         if (o.kind == OP_GETT && (o.skip || o.g.M == 0 || o.g.N == 0)) continue;
         const bool barrier = o.kind != OP_GETT ||
                              use_split(c, o);
@@ -1252,6 +1257,7 @@ long long count_sweep_launches(ccq_b200_ctx *c) {
     long long n = 0;
     for (size_t i = 0; i < c->cc_end; ++i) {
         const Op &o = c->plan.ops[i];
+        if (o.frozen) continue;
         if (o.kind == OP_GETT && o.g.M && o.g.N && !o.skip) {
             if (o.zero_first || o.g.K == 0) ++n;
             if (o.g.K)
@@ -2018,7 +2024,7 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
             }
             for (size_t i = 0; i < c->cc_end; ++i) {
                 Op &o = c->plan.ops[i];
-                if (o.kind != OP_GETT || o.skip || o.g.M == 0 || o.g.N == 0 || o.g.K == 0) {
+                if (o.kind != OP_GETT || o.skip || o.frozen || o.g.M == 0 || o.g.N == 0 || o.g.K == 0) {
                     run_op(c, o, c->stream);
                     continue;
                 }
@@ -2091,6 +2097,35 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
         c->gexec = c->lgexec = nullptr;
         if (ms_default) *ms_default = t0;
         if (ms_tuned) *ms_tuned = t1;
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+int ccq_b200_set_external(ccq_b200_ctx *c, int64_t on) {
+    try {
+        if (!c) throw Error(CCQ_B200_EINVAL, "null context");
+        if (c->calc_type != "CCSDT" && c->calc_type != "CCSDTQ")
+            throw Error(CCQ_B200_EINVAL, "set_external: a CCSDT or CCSDTQ context is required");
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "set_external: an iteration is pending");
+        // every operation of the T3 / T4 phases (their contractions, gathers and rhf copies)
+        std::string phase;
+        for (auto &o : c->plan.ops) {
+            if (o.kind == OP_PHASE) {
+                phase = o.arg0;
+                continue;
+            }
+            if (&o - &c->plan.ops[0] >= (long)c->cc_end) break;
+            o.frozen = on && phase.size() >= 2 && phase[0] == 'T' && (phase[1] == '3' || phase[1] == '4');
+        }
+        // DIIS over T1 + T2 (src/solve_cc.f90:66-72 with run%ext_cor)
+        c->vec_size = on ? c->vec_t12 : c->vec_full;
+        if (c->gexec) cudaGraphExecDestroy(c->gexec);
+        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
+        c->gexec = c->lgexec = nullptr;
         return 0;
     } catch (const Error &e) {
         return fail(e);

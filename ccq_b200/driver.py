@@ -177,6 +177,29 @@ def load_system(cfg, base_dir='.'):
     return dict(f_a=fa, f_b=fb, v_aa=vaa, v_ab=vab, v_bb=vbb, e_ref=eref)
 
 
+def load_external(ctx, cfg, path, out=print):
+    """Externally corrected CC: T3 (and for CCSDTQ T4) blocks from a .npz file (keys T3A..T3D, T4A..T4E,
+    optionally T1A..T2C as the starting T1, T2), held fixed while T1 and T2 iterate
+    (the role of ext_cor_driver's amplitudes, ``src/ext_cor/ext_cor.f90:12-149``)."""
+    if cfg.calc_type not in ('CCSDT', 'CCSDTQ'):
+        raise ValueError('CONFIGURATION ERROR: external amplitudes need calc_type CCSDT or CCSDTQ')
+    if not os.path.exists(path):
+        raise ValueError('CONFIGURATION ERROR: external amplitude file not found')
+    z = np.load(path)
+    lay = I.TLayout(I.Dims(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs))
+    t = np.zeros(lay.t_size)
+    for b in I.T_VEC_ORDER:
+        if b in z.files:
+            lay.view(t, b)[...] = z[b]
+    ctx.set_t(t)
+    if cfg.calc_type == 'CCSDTQ':
+        for b, shp in lay.t4_shape.items():
+            if b in z.files:
+                ctx.set_block(b, np.asarray(z[b]).reshape(shp))
+    ctx.set_external(True)
+    out('  External T3' + (' and T4' if cfg.calc_type == 'CCSDTQ' else '') + ' amplitudes from ' + path)
+
+
 def run(input_path, out=print, base_dir='.'):
     cfg = cfgmod.parse(input_path)
     if cfg.fcidump:
@@ -197,6 +220,9 @@ def run(input_path, out=print, base_dir='.'):
                       diis_space=cfg.diis_space)
     if cfg.calc_type == 'CCSDt':
         ctx.set_active(cfg.act_occ_b, cfg.act_unocc_a)
+    if cfg.gpu_external_t:
+        load_external(ctx, cfg, cfg.gpu_external_t if os.path.isabs(cfg.gpu_external_t)
+                      else os.path.join(base_dir, cfg.gpu_external_t), out)
     cfg.bin_file = cfg.bin_path()
     if not os.path.isabs(cfg.bin_file):
         cfg.bin_file = os.path.join(base_dir, cfg.bin_file)

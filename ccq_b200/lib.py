@@ -58,6 +58,7 @@ SIGNATURES = {
     'ccq_b200_autotune': (C.c_int, [C.c_void_p, I64, DP, DP]),
     'ccq_b200_force_tile': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_set_active': (C.c_int, [C.c_void_p, I64, I64]),
+    'ccq_b200_set_external': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_use_graph': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), DP, DP]),
     'ccq_b200_timing': (C.c_int, [C.c_void_p, DP, DP]),
@@ -265,6 +266,10 @@ class Context:
         a, b = C.c_double(), C.c_double()
         _err(self._lib.ccq_b200_autotune(self.ptr, reps, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def set_external(self, on=True):
+        """Externally corrected CC: T3 / T4 held at their set values, only T1 and T2 iterate."""
+        _err(self._lib.ccq_b200_set_external(self.ptr, int(bool(on))))
 
     def set_active(self, act_occ_b, act_unocc_a):
         """CCSDt: triples with >= 1 active occupied and >= 1 active virtual index (ccq's boundaries)."""

@@ -157,6 +157,14 @@ int ccq_b200_iterate_wait(ccq_b200_ctx *ctx, double *e_cor, double *residuum, in
  * *ms_default / *ms_tuned = summed per-contraction times before / after.
  * Re-run after ccq_b200_set_precision to tune the other mode. */
 int ccq_b200_autotune(ccq_b200_ctx *ctx, int64_t reps, double *ms_default, double *ms_tuned);
+/* Externally corrected CC (calc_type=CADFCIQMC, src/ext_cor/ext_cor.f90:12-149,
+ * src/update_cc.F90:104-109): on a CCSDT or CCSDTQ context, the T3 (and T4)
+ * amplitudes stay at the values given by ccq_b200_set_t / ccq_b200_block and
+ * only T1 and T2 iterate, with their full T3 / T4 contributions (T1-dressed);
+ * DIIS covers T1 + T2 as in the reference's ext_cor runs.  on = 0 restores
+ * the full method. */
+int ccq_b200_set_external(ccq_b200_ctx *ctx, int64_t on);
+
 /* Active-space CCSDt (calc_type=CCSDt, src/parser.f90:380-388 with
  * act_ind_t = 1): on a CCSDT context, keeps only the triples with at least
  * one active occupied and at least one active virtual index and holds the

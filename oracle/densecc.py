@@ -38,8 +38,11 @@ def active_mask(name, shape, dims, active):
 
 
 class DenseCC:
-    def __init__(self, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, method, shift=0.0, rhf=False, active=None):
+    def __init__(self, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, method, shift=0.0, rhf=False, active=None,
+                 external=False):
         self.active = active   # CCSDt: (act_occ_b, act_unocc_a), triples outside the active space held at zero
+        # externally corrected CC: T3 / T4 stay as given, only T1 and T2 are updated, DIIS over T1 + T2
+        self.external = external
         self.dims = dims
         self.method = method
         self.tranks = METHOD[method]
@@ -52,7 +55,7 @@ class DenseCC:
         self.so = SpinOrbitalSystem(self.fa, self.fb, v_aa, v_ab, v_bb, dims.oa, dims.ob)
         self.layout = I.TLayout(dims)
         self.t4 = {b: np.zeros(s) for b, s in self.layout.t4_shape.items()} if self.nmax >= 4 else {}
-        self.blocks = [b for b in S.BLOCK_ORDER if int(b[1]) <= self.nmax]
+        self.blocks = [b for b in S.BLOCK_ORDER if int(b[1]) <= (2 if external else self.nmax)]
 
     def _blocks(self, tvec):
         out = {b: self.layout.view(tvec, b) for b in I.T_VEC_ORDER if int(b[1]) <= self.nmax}
@@ -91,8 +94,8 @@ class DenseCC:
         ts = self.so.from_blocks({k: v for k, v in blocks.items() if int(k[1]) <= 2}, 2)
         return self.so.energy(ts)
 
-    def solve(self, diis_space=5, max_iter=60, tol=1e-8, log=None):
-        tvec = np.zeros(self.layout.t_size)
-        vs = self.layout.vec_size(self.method)
+    def solve(self, diis_space=5, max_iter=60, tol=1e-8, log=None, t0=None):
+        tvec = np.zeros(self.layout.t_size) if t0 is None else np.array(t0, dtype=np.float64)
+        vs = self.layout.vec_size('CCSD' if self.external else self.method)
         e, it, failed, hist = S.jacobi_iter(self.update, self.energy, tvec, vs, diis_space, max_iter, tol, log)
         return e, it, failed, hist, tvec

@@ -35,3 +35,39 @@ def random_t(dims, seed, scale=0.02, nmax=3):
         for b, shp in lay.t4_shape.items():
             t4[b] = S.antisym_fill(b, rng.normal(0, scale, shp))
     return t, t4
+
+
+def fci_cluster_amplitudes(so, nmax=4):
+    """Exact cluster amplitudes of the FCI ground state of a SpinOrbitalSystem.
+
+    The FCI vector psi (Sz of the reference, <Phi|psi> = 1) gives C_n, its
+    n-fold excitation coefficients in the amplitude convention of
+    oracle.detcc; exp(T)|Phi> = psi then fixes T_n = C_n - [exp(T_1 + .. +
+    T_{n-1})|Phi>]_n level by level.  Returns ({n: T_n[a.., i..]}, E_FCI - E_ref).
+    """
+    from oracle.detcc import DetCC
+    dc = DetCC(so.h, so.v, so.O)
+    fs = dc.fs
+    states = fs.states
+    pc = np.array([bin(int(x)).count('1') for x in states])
+    sel = np.where(pc == so.O)[0]
+    # Sz sector of the reference: as many alpha spin orbitals occupied as in the reference
+    amask = sum(1 << p for p in range(so.N) if so.spin[p] == 0)
+    nref = bin(((1 << so.O) - 1) & amask).count('1')
+    sel = sel[np.array([bin(int(x) & amask).count('1') for x in states[sel]]) == nref]
+    H = np.zeros((len(sel), len(sel)))
+    for k, x in enumerate(sel):
+        e = np.zeros(1 << so.N)
+        e[x] = 1.0
+        H[:, k] = dc.apply_h(e)[sel]
+    w, U = np.linalg.eigh(0.5 * (H + H.T))
+    psi = np.zeros(1 << so.N)
+    psi[sel] = U[:, 0]
+    psi /= psi[(1 << so.O) - 1]
+    ts = {}
+    for n in range(1, nmax + 1):
+        C = dc.residual({}, n, w=psi)
+        if ts:
+            C = C - dc.residual({}, n, w=dc.exp_t(ts, dc.phi))
+        ts[n] = C
+    return ts, float(w[0]) - dc.e_ref()
