@@ -13,7 +13,8 @@ plus the DIIS ring) exceeds the 126 MB L2, so no flush is needed between steps.
 stream), whole job: max over ranks of the time / (ranks x K).  Multi-GPU runs
 are independent replicas (one solve per GPU, no collective on the data path).
 ``e2e`` is the same metric through the C ABI with the T vector in pinned host
-memory: set_t + iterate + get_t per step.  ``--impl reference`` times the CPU
+memory: every step copies it to the device and back (ccq_b200_iterate_host,
+whose block copies overlap the sweep).  ``--impl reference`` times the CPU
 restatement of the reference algorithm (numpy + threaded BLAS) on this host.
 
 Besides the headline legs (FP64 and split, each autotuned first), the line
@@ -550,16 +551,17 @@ def main():
                      'note': 'achieved = algorithmic FLOPs of all launches of that kernel in 2 eager sweeps (CUDA '
                              'events around every launch) / their summed durations'})
 
-    # end-to-end through the C ABI with host buffers
+    # end-to-end through the C ABI with host buffers: every step copies the t_vec in from pinned host
+    # memory and back out (ccq_b200_iterate_host: the block copies overlap the sweep)
     pinned = torch.empty(ctx.t_size, dtype=torch.float64, pin_memory=True)
     pinned.copy_(torch.from_numpy(ctx.get_t()))
+    ctx.iterate_host(it, pinned.data_ptr(), pinned.data_ptr())   # captures the graph with its copies
+    it += 1
     barrier(world)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        ctx.set_t_ptr(pinned.data_ptr(), ctx.t_size)
-        ctx.iterate(it)
+        ctx.iterate_host(it, pinned.data_ptr(), pinned.data_ptr())
         it += 1
-        ctx.get_t_ptr(pinned.data_ptr(), ctx.t_size)
     torch.cuda.synchronize()
     barrier(world)
     e2e_s = allmax(time.perf_counter() - t0, world) / (world * args.steps)

@@ -299,6 +299,16 @@ struct ccq_b200_ctx {
     cudaGraphExec_t gexec = nullptr;
     int device = 0;
     SplitWorkspace split{};
+    // host round trip of ccq_b200_iterate_host: each t_vec block is copied to host_out as soon as its
+    // last write of the sweep is done (copy stream cstream, joined into the sweep's stream at its end)
+    double *host_out = nullptr;
+    cudaGraphExec_t gexec_host = nullptr;
+    double *gexec_host_ptr = nullptr;
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t cjoin = nullptr;
+    std::vector<cudaEvent_t> cev;
+    std::vector<std::pair<size_t, std::string>> out_after;   // (op index, block) of every block's last write
+    bool out_ready = false;
 
     void *dalloc(size_t bytes) {
         void *p = nullptr;
@@ -309,6 +319,10 @@ struct ccq_b200_ctx {
     ~ccq_b200_ctx() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (lgexec) cudaGraphExecDestroy(lgexec);
+        if (gexec_host) cudaGraphExecDestroy(gexec_host);
+        for (auto e : cev) cudaEventDestroy(e);
+        if (cjoin) cudaEventDestroy(cjoin);
+        if (cstream) cudaStreamDestroy(cstream);
         for (auto e : opev) cudaEventDestroy(e);
         if (cap_ev) cudaEventDestroy(cap_ev);
         for (auto st : side) cudaStreamDestroy(st);
@@ -1113,6 +1127,59 @@ void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
 // copies, zeroing, split GETTs, whose slicing shares one workspace) is a
 // barrier on the capturing stream.  Independent contractions then run on side
 // streams at the same time.
+// every t_vec block resident on the device, and the last sweep op that writes it
+void prepare_copy_out(ccq_b200_ctx *c) {
+    if (c->out_ready) return;
+    c->out_after.clear();
+    for (auto &b : c->plan.bufs) {
+        if (b.kind != "amp") continue;
+        const DevBuf &d = c->bufs.at(b.name);
+        if (!d.ptr || d.ptr < c->tvec || d.ptr >= c->tvec + c->t_dev) continue;
+        size_t last = (size_t)-1;
+        for (size_t i = 0; i < c->cc_end; ++i) {
+            const Op &o = c->plan.ops[i];
+            if ((o.kind == OP_ASM && o.block == b.name) || (o.kind == OP_COPY && o.arg0 == b.name)) last = i;
+        }
+        c->out_after.push_back({last, b.name});
+    }
+    if (!c->cstream) {
+        CK(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->cjoin, cudaEventDisableTiming));
+    }
+    if (c->cev.size() < c->out_after.size()) {
+        for (size_t k = c->cev.size(); k < c->out_after.size(); ++k) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            c->cev.push_back(e);
+        }
+    }
+    c->out_ready = true;
+}
+
+void copy_block_out(ccq_b200_ctx *c, size_t k, cudaStream_t after) {
+    const DevBuf &d = c->bufs.at(c->out_after[k].second);
+    CK(cudaEventRecord(c->cev[k], after));
+    CK(cudaStreamWaitEvent(c->cstream, c->cev[k], 0));
+    CK(cudaMemcpyAsync(c->host_out + (d.ptr - c->tvec), d.ptr, sizeof(double) * d.numel, cudaMemcpyDeviceToHost,
+                       c->cstream));
+}
+
+// copies of the blocks whose last write is op i (after it has been issued on stream st)
+void copy_out_after(ccq_b200_ctx *c, size_t i, cudaStream_t st) {
+    if (!c->host_out || c->plan.ops[i].frozen) return;
+    for (size_t k = 0; k < c->out_after.size(); ++k)
+        if (c->out_after[k].first == i) copy_block_out(c, k, st);
+}
+
+// blocks the sweep does not write (held fixed) go at its end; then the copy stream joins st
+void copy_out_finish(ccq_b200_ctx *c, cudaStream_t st) {
+    if (!c->host_out) return;
+    for (size_t k = 0; k < c->out_after.size(); ++k)
+        if (c->out_after[k].first == (size_t)-1 || c->plan.ops[c->out_after[k].first].frozen) copy_block_out(c, k, st);
+    CK(cudaEventRecord(c->cjoin, c->cstream));
+    CK(cudaStreamWaitEvent(st, c->cjoin, 0));
+}
+
 void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
     constexpr int NSIDE = 6;
     if (c->side.empty()) {
@@ -1149,6 +1216,7 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
             run_op(c, o, c->stream);
             CK(cudaEventRecord(c->opev[i], c->stream));
             gate = c->opev[i];
+            copy_out_after(c, i, c->stream);
             continue;
         }
         std::vector<size_t> deps;
@@ -1197,6 +1265,7 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
         if (prof) CK(cudaEventRecord(c->pev[2 * i], c->stream));
         run_op(c, o, c->stream);
         if (prof) CK(cudaEventRecord(c->pev[2 * i + 1], c->stream));
+        copy_out_after(c, i, c->stream);
     }
     CK(cudaGetLastError());
     if (prof) {
@@ -1228,8 +1297,11 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
 }
 
 void sweep(ccq_b200_ctx *c) {
+    // with host_out set, the captured graph also holds the copy-out of every finished block
+    if (c->host_out) prepare_copy_out(c);
+    cudaGraphExec_t &ge = c->host_out ? c->gexec_host : c->gexec;
     if (c->use_graph && !c->profile) {
-        if (!c->gexec) {
+        if (!ge) {
             cudaGraph_t g;
             long long l0 = c->launches;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1238,19 +1310,32 @@ void sweep(ccq_b200_ctx *c) {
                     run_ops(c, 0, c->cc_end);
                 else
                     run_ops_dag(c, 0, c->cc_end);
+                copy_out_finish(c, c->stream);
             } catch (...) {
                 cudaStreamEndCapture(c->stream, &g);
                 throw;
             }
             CK(cudaStreamEndCapture(c->stream, &g));
-            CK(cudaGraphInstantiate(&c->gexec, g, 0));
+            CK(cudaGraphInstantiate(&ge, g, 0));
             CK(cudaGraphDestroy(g));
             c->launches = l0 + (c->launches - l0);
         }
-        CK(cudaGraphLaunch(c->gexec, c->stream));
+        CK(cudaGraphLaunch(ge, c->stream));
     } else {
         run_ops(c, 0, c->cc_end);
+        copy_out_finish(c, c->stream);
     }
+}
+
+
+// every captured graph of the context (kernel arguments, op flags and copy targets are recorded in them)
+void drop_graphs(ccq_b200_ctx *c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
+    if (c->gexec_host) cudaGraphExecDestroy(c->gexec_host);
+    c->gexec = c->lgexec = c->gexec_host = nullptr;
+    c->gexec_host_ptr = nullptr;
+    c->out_ready = false;
 }
 
 long long count_sweep_launches(ccq_b200_ctx *c) {
@@ -1736,6 +1821,9 @@ static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
         launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
         launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
         c->launches += 3;
+        // the extrapolation rewrote T1 .. T3: the host copy is taken again
+        if (c->host_out)
+            CK(cudaMemcpyAsync(c->host_out, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost, c->stream));
     }
     CK(cudaEventRecord(c->ev2, c->stream));
     CK(cudaMemcpyAsync(c->hpin, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1765,6 +1853,49 @@ static void iterate_finish(ccq_b200_ctx *c, double *e_cor, double *res, int64_t 
     if (e_cor) *e_cor = c->hpin[0];
     if (res) *res = std::sqrt(std::sqrt(c->hpin[1]));
     if (did_diis) *did_diis = diis;
+}
+
+int ccq_b200_iterate_host(ccq_b200_ctx *c, int64_t iter, const double *t_in, double *t_out, int64_t n,
+                          double *e_cor, double *res, int64_t *did_diis) {
+    try {
+        if (!c || iter < 1 || !t_in || !t_out) throw Error(CCQ_B200_EINVAL, "iterate_host: bad argument");
+        if (n != c->t_size) throw Error(CCQ_B200_EINVAL, "iterate_host: size must equal t_size");
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "iterate_host: an iteration is pending");
+        CK(cudaSetDevice(c->device));
+        CK(cudaMemcpyAsync(c->tvec, t_in, sizeof(double) * c->t_dev, cudaMemcpyHostToDevice, c->stream));
+        cudaPointerAttributes pa{};
+        const bool pinned = cudaPointerGetAttributes(&pa, t_out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (!pinned) {
+            // pageable memory cannot take asynchronous copies inside a captured sweep: copy after it
+            iterate_launch(c, iter);
+            iterate_finish(c, e_cor, res, did_diis);
+            CK(cudaMemcpy(t_out, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost));
+            if (c->t_dev < n) std::fill(t_out + c->t_dev, t_out + n, 0.0);
+            return 0;
+        }
+        if (c->gexec_host_ptr != t_out) {
+            // the copy targets are part of the captured graph
+            if (c->gexec_host) cudaGraphExecDestroy(c->gexec_host);
+            c->gexec_host = nullptr;
+            c->gexec_host_ptr = t_out;
+        }
+        c->host_out = t_out;
+        try {
+            iterate_launch(c, iter);
+        } catch (...) {
+            c->host_out = nullptr;
+            throw;
+        }
+        c->host_out = nullptr;
+        iterate_finish(c, e_cor, res, did_diis);
+        if (c->t_dev < n) std::fill(t_out + c->t_dev, t_out + n, 0.0);
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
 }
 
 int ccq_b200_iterate(ccq_b200_ctx *c, int64_t iter, double *e_cor, double *res, int64_t *did_diis) {
@@ -2092,9 +2223,7 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
             throw;
         }
         release();
-        if (c->gexec) cudaGraphExecDestroy(c->gexec);
-        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
-        c->gexec = c->lgexec = nullptr;
+        drop_graphs(c);
         if (ms_default) *ms_default = t0;
         if (ms_tuned) *ms_tuned = t1;
         return 0;
@@ -2123,9 +2252,7 @@ int ccq_b200_set_external(ccq_b200_ctx *c, int64_t on) {
         }
         // DIIS over T1 + T2 (src/solve_cc.f90:66-72 with run%ext_cor)
         c->vec_size = on ? c->vec_t12 : c->vec_full;
-        if (c->gexec) cudaGraphExecDestroy(c->gexec);
-        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
-        c->gexec = c->lgexec = nullptr;
+        drop_graphs(c);
         return 0;
     } catch (const Error &e) {
         return fail(e);
@@ -2152,9 +2279,7 @@ int ccq_b200_set_active(ccq_b200_ctx *c, int64_t act_occ_b, int64_t act_unocc_a)
             a.act_vir_hi[1] = (int)(act_unocc_a - occ_b);
         }
         // kernel arguments are recorded in the captured graphs
-        if (c->gexec) cudaGraphExecDestroy(c->gexec);
-        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
-        c->gexec = c->lgexec = nullptr;
+        drop_graphs(c);
         return 0;
     } catch (const Error &e) {
         return fail(e);
@@ -2174,9 +2299,7 @@ int ccq_b200_force_tile(ccq_b200_ctx *c, int64_t tile) {
         o.g.kchunk = tile == 3 ? (o.g.K + 15) / 16 * 16 : gett_f64_kchunk(o.g.M, o.g.N, o.g.K);
         o.zero_first = (o.g.K + o.g.kchunk - 1) / o.g.kchunk > 1 && o.beta == 0;
     }
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
-    c->gexec = c->lgexec = nullptr;
+    drop_graphs(c);
     return 0;
 }
 
@@ -2196,10 +2319,7 @@ int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {
                 }
             return SplitSizes{ma, mb, mc};
         }() : SplitSizes{0, 0, 0}, (int)nslices);
-        if (c->gexec) {
-            cudaGraphExecDestroy(c->gexec);
-            c->gexec = nullptr;
-        }
+        drop_graphs(c);
         c->precision = (int)mode;
         c->nslices = (int)nslices;
         return 0;
@@ -2214,9 +2334,7 @@ int ccq_b200_use_graph(ccq_b200_ctx *c, int64_t enable) {
     if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
     if (enable < 0 || enable > 2) return fail(Error(CCQ_B200_EINVAL, "use_graph: 0, 1 or 2"));
     if ((int)enable != c->use_graph) {
-        if (c->gexec) cudaGraphExecDestroy(c->gexec);
-        if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
-        c->gexec = c->lgexec = nullptr;
+        drop_graphs(c);
     }
     c->use_graph = (int)enable;
     return 0;

@@ -49,6 +49,7 @@ SIGNATURES = {
     'ccq_b200_energy': (C.c_int, [C.c_void_p, DP]),
     'ccq_b200_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
     'ccq_b200_iterate_async': (C.c_int, [C.c_void_p, I64]),
+    'ccq_b200_iterate_host': (C.c_int, [C.c_void_p, I64, C.c_void_p, C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
     'ccq_b200_iterate_wait': (C.c_int, [C.c_void_p, DP, DP, C.POINTER(I64)]),
     'ccq_b200_lambda_init': (C.c_int, [C.c_void_p, C.c_double]),
     'ccq_b200_lambda_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
@@ -232,6 +233,14 @@ class Context:
     def iterate(self, it):
         e, r, d = C.c_double(), C.c_double(), I64()
         _err(self._lib.ccq_b200_iterate(self.ptr, it, C.byref(e), C.byref(r), C.byref(d)))
+        return e.value, r.value, bool(d.value)
+
+    def iterate_host(self, it, t_in_ptr, t_out_ptr):
+        """One iteration from host t_vec t_in to host t_vec t_out (pointers to t_size doubles, pinned
+        for overlap): block copies overlap the sweep.  Returns (e_cor, residuum, did_diis)."""
+        e, r, d = C.c_double(), C.c_double(), I64()
+        _err(self._lib.ccq_b200_iterate_host(self.ptr, it, C.c_void_p(t_in_ptr), C.c_void_p(t_out_ptr), self.t_size,
+                                             C.byref(e), C.byref(r), C.byref(d)))
         return e.value, r.value, bool(d.value)
 
     def iterate_async(self, it):

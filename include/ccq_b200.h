@@ -141,6 +141,16 @@ int ccq_b200_energy(ccq_b200_ctx *ctx, double *e_cor);
 int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
                      double *residuum, int64_t *did_diis);
 
+/* One iteration from a host t_vec to a host t_vec (the reference's loop when
+ * it keeps cc%t_vec on the host): t_in is copied to the device, the sweep
+ * runs, and every T1..T3 block is copied to t_out as soon as the sweep has
+ * written it for the last time, overlapping the rest of the sweep (after a
+ * DIIS step the whole vector is copied again).  t_in may equal t_out.  With
+ * pageable t_out the copy-out follows the sweep instead of overlapping it.
+ * Returns what ccq_b200_iterate does. */
+int ccq_b200_iterate_host(ccq_b200_ctx *ctx, int64_t iter, const double *t_in, double *t_out, int64_t n,
+                          double *e_cor, double *residuum, int64_t *did_diis);
+
 /* ccq_b200_iterate in two halves, for many independent solves at once (one
  * context per Hamiltonian, each on its own stream): _async enqueues the
  * iteration and returns; _wait blocks until it is done and returns its

@@ -1,0 +1,47 @@
+"""ccq_b200_iterate_host: one iteration from a host t_vec to a host t_vec with the
+block copies overlapped with the sweep gives what iterate + get_t give, across
+DIIS steps, in every graph mode, with pinned or pageable host memory."""
+import numpy as np
+import pytest
+
+from ccq_b200 import lib
+from tests.helpers import random_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(s, method, graph):
+    d = s['dims']
+    c = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, method, s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'])
+    c.use_graph(graph)
+    return c
+
+
+@pytest.mark.parametrize('method,graph,pinned', [('CCSDT', 1, True), ('CCSDT', 2, False), ('CCSDT', 0, True),
+                                                 ('CCSD', 1, True), ('CCSDTQ', 1, False)])
+def test_iterate_host_equals_iterate_and_get_t(method, graph, pinned):
+    import torch
+    s = random_system(7, 3, 2, seed=12, sigma=0.08) if method != 'CCSDTQ' else random_system(5, 2, 2, seed=12)
+    a = _ctx(s, method, graph)
+    b = _ctx(s, method, graph)
+    n = a.t_size
+    if pinned:
+        buf = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+        pin, pout = buf.data_ptr(), buf.data_ptr()
+        view = buf.numpy()
+    else:
+        tin = np.zeros(n)
+        tout = np.zeros(n)
+        pin, pout = tin.ctypes.data, tout.ctypes.data
+    for it in range(1, 9):    # DIIS at iteration 6
+        ea, ra, da = a.iterate(it)
+        ta = a.get_t()
+        eb, rb, db = b.iterate_host(it, pin, pout)
+        tb = view.copy() if pinned else tout.copy()
+        if not pinned:
+            tin[...] = tout
+        assert da == db
+        assert abs(ea - eb) < 1e-12 and abs(ra - rb) < 1e-12
+        np.testing.assert_allclose(tb, ta, atol=1e-12, rtol=0)
+    a.close()
+    b.close()
