@@ -95,6 +95,8 @@ class Config:
         return f'tvec_{self.label}.bin' if self.label else 'tvec.bin'
 
     def calc_macros(self):
+        if self.calc_type in ('CCT3', 'CCt3'):
+            self.calc_type = 'CC(t;3)'    # src/parser.f90:400-401
         ct = self.calc_type
         if ct == 'CCSD':
             self.lvl_t, self.lvl_q = False, False
@@ -107,12 +109,20 @@ class Config:
             if self.act_occ == -1 and self.act_unocc == -1:
                 raise ValueError('CONFIGURATION ERROR: Active space methods require an active space')
             self.lvl_t, self.lvl_q = True, False
+        elif ct == 'CC(t;3)':
+            # src/parser.f90:400-411: CCSDt, then hbar, left CCSD and the MM(2,3) correction over the
+            # triples outside the active space.  ccq checks the active space only for CCSDt
+            # (parser.f90:251-254); without one its act_occ_b = occ_b + 1 and act_unocc_a = occ_a - 1
+            # lie outside the ranges its sorted integrals are built for, so it is required here too.
+            if self.act_occ == -1 and self.act_unocc == -1:
+                raise ValueError('CONFIGURATION ERROR: Active space methods require an active space')
+            self.lvl_t, self.lvl_q = True, False
         elif ct == 'CR-CC(2,3)':
             # src/parser.f90:368-377: CCSD, then hbar, left CCSD and the MM(2,3) correction
             self.lvl_t, self.lvl_q = False, False
         else:
             raise ValueError(f'calc_type {ct!r} is not served by this engine '
-                             '(CCSD, CCSDT, CCSDTQ, CCSDt, CR-CC(2,3) are; the others stay on the CPU program)')
+                             '(CCSD, CCSDT, CCSDTQ, CCSDt, CC(t;3), CR-CC(2,3) are; the others stay on the CPU program)')
         return self
 
 

@@ -289,13 +289,16 @@ __global__ void __launch_bounds__(256) crcc_sum_kernel(CrccArgs a) {
         for (int k = 0; k < 2; ++k)
             if (a.spin[k] == a.spin[k + 1] && (x[k] >= x[k + 1] || x[3 + k] >= x[4 + k])) canon = false;
         if (!canon) continue;
-        const double lm = __ldg(a.L + t) * __ldg(a.M + t);
         int po[3], pv[3], s[3];
         for (int k = 0; k < 3; ++k) {
             s[k] = a.spin[k];
             po[k] = x[k];
             pv[k] = a.off[s[k]] + x[3 + k];
         }
+        // crcc23's active-space skip (src/mm_correct.f90:131,190,244,300)
+        if (max(po[0], max(po[1], po[2])) >= a.act_occ_lo && min(pv[0], min(pv[1], pv[2])) < a.act_vir_hi)
+            continue;
+        const double lm = __ldg(a.L + t) * __ldg(a.M + t);
         double da = 0.0, db = 0.0;
         for (int k = 0; k < 3; ++k) {
             da += __ldg(a.fd[s[k]] + po[k]) - __ldg(a.fd[s[k]] + pv[k]);

@@ -38,6 +38,10 @@ struct CrccArgs {
     const double *w1[4], *w2[4];
     double *e23;           // four sums, accumulated
     long long total;
+    // triples already iterated in an active space (CC(t;3)) are left out of the sums:
+    // those with an occupied index >= act_occ_lo and a virtual index (full range) < act_vir_hi;
+    // act_occ_lo = n leaves none out
+    int act_occ_lo, act_vir_hi;
 };
 
 void launch_crdiag(const CrDiagArgs &a, cudaStream_t s);

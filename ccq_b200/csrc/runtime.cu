@@ -618,6 +618,8 @@ void instantiate(ccq_b200_ctx *c) {
                 r.w2[q] = c->bufs.at(std::string("W2") + char('A' + q)).ptr;
             }
             r.e23 = c->bufs.at("E23").ptr;
+            r.act_occ_lo = (int)c->n;
+            r.act_vir_hi = 0;
         }
         if (o.kind == OP_CRDIAG) {
             CrDiagArgs &g = c->crd;
@@ -2264,11 +2266,18 @@ int ccq_b200_set_external(ccq_b200_ctx *c, int64_t on) {
 int ccq_b200_set_active(ccq_b200_ctx *c, int64_t act_occ_b, int64_t act_unocc_a) {
     try {
         if (!c) throw Error(CCQ_B200_EINVAL, "null context");
-        if (c->calc_type != "CCSDT") throw Error(CCQ_B200_EINVAL, "set_active: a CCSDT context is required");
+        if (c->calc_type != "CCSDT" && !c->has_crcc)
+            throw Error(CCQ_B200_EINVAL, "set_active: a CCSDT or CR-CC(2,3) context is required");
         const long long occ_a = c->froz + c->oa, occ_b = c->froz + c->ob, orbs = occ_a + c->va;
         if (act_occ_b < c->froz || act_occ_b > occ_b || act_unocc_a < occ_a || act_unocc_a > orbs)
             throw Error(CCQ_B200_EINVAL, "set_active: froz <= act_occ_b <= occ_b and occ_a <= act_unocc_a <= orbs");
         for (auto &o : c->plan.ops) {
+            if (o.kind == OP_CRCC) {
+                // CC(t;3): the correction covers the triples outside the active space
+                o.crcc.act_occ_lo = (int)(act_occ_b - c->froz);
+                o.crcc.act_vir_hi = (int)(act_unocc_a - c->froz);
+                continue;
+            }
             if (o.kind != OP_ASM || o.block[1] != '3' || o.asmargs.mode != 0) continue;
             AsmArgs &a = o.asmargs;
             // spatial orbitals above act_occ_b (occupied) and up to act_unocc_a (virtual) are active,

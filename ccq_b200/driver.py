@@ -213,12 +213,15 @@ def run(input_path, out=print, base_dir='.'):
     out(f"  Reference energy {sysd['e_ref']:.12f}")
     out('Coupled cluster')
     out('---------------')
-    # CCSDt runs the CCSDT plan with the triples held to the active space
-    ctype = 'CCSDT' if cfg.calc_type == 'CCSDt' else cfg.calc_type
-    ctx = lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, ctype, sysd['f_a'], sysd['f_b'],
-                      sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
-                      diis_space=cfg.diis_space)
-    if cfg.calc_type == 'CCSDt':
+    # CCSDt (and the CCSDt part of CC(t;3)) runs the CCSDT plan with the triples held to the active space
+    active = cfg.calc_type in ('CCSDt', 'CC(t;3)')
+
+    def context(ctype):
+        return lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, ctype, sysd['f_a'], sysd['f_b'],
+                           sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
+                           diis_space=cfg.diis_space)
+    ctx = context('CCSDT' if active else cfg.calc_type)
+    if active:
         ctx.set_active(cfg.act_occ_b, cfg.act_unocc_a)
     if cfg.gpu_external_t:
         load_external(ctx, cfg, cfg.gpu_external_t if os.path.isabs(cfg.gpu_external_t)
@@ -237,6 +240,21 @@ def run(input_path, out=print, base_dir='.'):
             r.e23 = ctx.crcc23()
             print_cct3(out, sysd['e_ref'], r.e_cor, r.e23)
             r.e_ccsd = r.e_cor
+            r.e_cor = r.e_cor + r.e23[3]
+            r.failed = r.failed or r.left.failed
+        elif cfg.calc_type == 'CC(t;3)':
+            # hbar2 + solve_lcc + crcc23 (src/calc_driver.f90:55-73) on the CCSDt T1 and T2
+            # (hbar2 reads t_vec(1:pos(6)-1), src/hbar.f90:71-73), the sums over the triples
+            # outside the active space
+            t = ctx.get_t()
+            ctx.close()
+            ctx = context('CR-CC(2,3)')
+            ctx.set_active(cfg.act_occ_b, cfg.act_unocc_a)
+            ctx.set_t(t[:ctx.t_size])
+            r.left = solve_lcc(ctx, cfg, r.e_cor, out)
+            r.e23 = ctx.crcc23()
+            print_cct3(out, sysd['e_ref'], r.e_cor, r.e23)
+            r.e_ccsdt = r.e_cor
             r.e_cor = r.e_cor + r.e23[3]
             r.failed = r.failed or r.left.failed
     finally:

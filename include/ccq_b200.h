@@ -181,7 +181,11 @@ int ccq_b200_set_external(ccq_b200_ctx *ctx, int64_t on);
  * others at zero.  Active: spatial orbitals act_occ_b < p <= occ (occupied)
  * and occ < p <= act_unocc_a (virtual), both spins, with ccq's
  * act_occ_b = max(occ_b - act_occ, froz), act_unocc_a = min(occ_a + act_unocc,
- * orbs) (src/parser.f90:495-499; 1-based). */
+ * orbs) (src/parser.f90:495-499; 1-based).
+ * On a CR-CC(2,3) context (CC(t;3), src/parser.f90:400-411): ccq_b200_crcc23
+ * sums only the triples outside that active space, the skip of crcc23
+ * (src/mm_correct.f90:61-62,131,190,244,300), for amplitudes set from a
+ * CCSDt solve. */
 int ccq_b200_set_active(ccq_b200_ctx *ctx, int64_t act_occ_b, int64_t act_unocc_a);
 
 /* Pins every contraction to one GETT kernel family: 0 = by shape, 1 = 64 x 64

@@ -226,8 +226,10 @@ class BlockCRCC(BlockCC):
     layout of ``t_vec``.
     """
 
-    def __init__(self, plan_text, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, shift=0.0):
+    def __init__(self, plan_text, f_a, f_b, v_aa, v_ab, v_bb, dims: I.Dims, shift=0.0, active=None):
         super().__init__(plan_text, f_a, f_b, v_aa, v_ab, v_bb, dims, 'CCSD', shift)
+        # CC(t;3): (act_occ_b, act_unocc_a); the sums leave out the triples of that active space
+        self.active = active
         self.lvec = np.zeros(self.layout.t_size)
         for b in L_BLOCKS:
             self.buf[b] = self.layout.view(self.lvec, 'T' + b[1:])
@@ -308,7 +310,12 @@ class BlockCRCC(BlockCC):
         M, L = b['M3' + x], b['L3' + x]
         spins = S.block_spins(name)
         off = [self.dims.oa, self.dims.ob]
-        idx = np.nonzero(S.canonical_mask(name, M.shape))
+        keep = S.canonical_mask(name, M.shape)
+        if self.active is not None:
+            # crcc23's skip of the active-space triples (src/mm_correct.f90:131,190,244,300)
+            from oracle.densecc import active_mask
+            keep = keep & ~active_mask(name, M.shape, self.dims, self.active)
+        idx = np.nonzero(keep)
         lm = L[idx] * M[idx]
         occ = [idx[k] for k in range(3)]
         vir = [idx[3 + k] + off[spins[k]] for k in range(3)]

@@ -337,7 +337,10 @@ class DenseCRCC:
                 dd += self.w2[x, z, y]
         return da, db, dc, dd
 
-    def energies(self):
+    def energies(self, active=None):
+        """The four corrections; ``active = (act_occ_b, act_unocc_a)`` (CC(t;3)) leaves out the
+        triples with an occupied spatial orbital above act_occ_b and a virtual one up to
+        act_unocc_a (``src/mm_correct.f90:61-62,131``)."""
         M = self.moments()
         L = self.left_projections()
         self.M3, self.L3 = M, L
@@ -348,6 +351,12 @@ class DenseCRCC:
         for occ, vir in unique_triples(O, V):
             if sorted(spin[list(occ)]) != sorted(spin[[O + a for a in vir]]):
                 continue
+            if active is not None:
+                froz = self.dims.froz
+                top = max(so.sp[i][0] for i in occ) + froz + 1        # 1-based spatial orbitals
+                low = min(so.sp[O + a][0] for a in vir) + froz + 1
+                if top > active[0] and low <= active[1]:
+                    continue
             lm = L[vir + occ] * M[vir + occ]
             ds = self.denominators(occ, vir)
             for q in range(4):
