@@ -67,6 +67,9 @@ class Config:
     gpu_external_t: str = ''
     act_occ: int = -1
     act_unocc: int = -1
+    ext_cor_file: str = ''
+    ext_cor_sd: bool = True
+    ext_cor_file_h5: bool = False
     # derived (process_sys_data)
     froz: int = 0
     occ_a: int = 0
@@ -117,12 +120,15 @@ class Config:
             if self.act_occ == -1 and self.act_unocc == -1:
                 raise ValueError('CONFIGURATION ERROR: Active space methods require an active space')
             self.lvl_t, self.lvl_q = True, False
+        elif ct == 'CADFCIQMC':
+            # src/parser.f90:341-347: CCSD-level iterations with T3 and T4 from the walker file
+            self.lvl_t, self.lvl_q = False, False
         elif ct == 'CR-CC(2,3)':
             # src/parser.f90:368-377: CCSD, then hbar, left CCSD and the MM(2,3) correction
             self.lvl_t, self.lvl_q = False, False
         else:
             raise ValueError(f'calc_type {ct!r} is not served by this engine '
-                             '(CCSD, CCSDT, CCSDTQ, CCSDt, CC(t;3), CR-CC(2,3) are; the others stay on the CPU program)')
+                             '(CCSD, CCSDT, CCSDTQ, CCSDt, CC(t;3), CR-CC(2,3), CADFCIQMC are; the others stay on the CPU program)')
         return self
 
 
@@ -177,6 +183,12 @@ def _apply(cfg, key, val):
         cfg.restart = True
     elif key == 'label':
         cfg.label = val
+    elif key == 'ext_cor_file':
+        cfg.ext_cor_file = val
+    elif key == 'ext_cor_sd':
+        cfg.ext_cor_sd = _logical(val)
+    elif key == 'ext_cor_file_h5':
+        cfg.ext_cor_file_h5 = True
     elif key in ('symfile', 'sym_file'):
         cfg.sym_file = val
     elif key == 'onebody':

@@ -200,6 +200,23 @@ def load_external(ctx, cfg, path, out=print):
     out('  External T3' + (' and T4' if cfg.calc_type == 'CCSDTQ' else '') + ' amplitudes from ' + path)
 
 
+def load_walkers(ctx, cfg, path, out=print):
+    """CAD-FCIQMC (external_correction_driver, ``src/ext_cor/ext_cor.f90:12-144``): the cluster analysis
+    of the walker file gives T3 and T4, held fixed while T1 and T2 iterate from the analysed T1, T2
+    (from zero with ext_cor_sd=.false.)."""
+    out('Cluster analysis')
+    out('----------------')
+    t, t4, info = lib.walkers_read(path, cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, cfg.occ_a + cfg.occ_b,
+                                   with_sd=cfg.ext_cor_sd)
+    out(f"  {info['records']} determinants read from {path}; {info['quadruples']} quadruples, "
+        f"{info['higher']} higher excitations skipped; Hartree-Fock coefficient {info['c_hf']:.10g}")
+    ctx.set_t(t)
+    for b, blk in t4.items():
+        ctx.set_block(b, blk)
+    ctx.set_external(True)
+    out(f"\n  {'External correlation energy':>27}  {ctx.energy():16.10f}\n")
+
+
 def run(input_path, out=print, base_dir='.'):
     cfg = cfgmod.parse(input_path)
     if cfg.fcidump:
@@ -220,9 +237,19 @@ def run(input_path, out=print, base_dir='.'):
         return lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, ctype, sysd['f_a'], sysd['f_b'],
                            sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
                            diis_space=cfg.diis_space)
-    ctx = context('CCSDT' if active else cfg.calc_type)
+    walkers = None
+    if cfg.calc_type == 'CADFCIQMC':
+        if cfg.ext_cor_file_h5:
+            raise ValueError('CONFIGURATION ERROR: HDF5 walker files (ext_cor_file_h5) need an HDF5 library, '
+                             'which this build does not have')
+        walkers = cfg.ext_cor_file if os.path.isabs(cfg.ext_cor_file) else os.path.join(base_dir, cfg.ext_cor_file)
+        if not cfg.ext_cor_file or not os.path.exists(walkers):
+            raise ValueError('CONFIGURATION ERROR: Walkers file not found')
+    ctx = context('CCSDT' if active else 'CCSDTQ' if walkers else cfg.calc_type)
     if active:
         ctx.set_active(cfg.act_occ_b, cfg.act_unocc_a)
+    if walkers:
+        load_walkers(ctx, cfg, walkers, out)
     if cfg.gpu_external_t:
         load_external(ctx, cfg, cfg.gpu_external_t if os.path.isabs(cfg.gpu_external_t)
                       else os.path.join(base_dir, cfg.gpu_external_t), out)

@@ -74,6 +74,7 @@ SIGNATURES = {
     'ccq_b200_fcidump_header': (C.c_int, [C.c_char_p, C.POINTER(I64), C.POINTER(I64)]),
     'ccq_b200_fcidump_read': (C.c_int, [C.c_char_p, I64, DP, DP, DP]),
     'ccq_b200_fcidump_read_device': (C.c_int, [C.c_char_p, I64, DP, C.c_void_p, DP, C.c_void_p]),
+    'ccq_b200_walkers_read': (C.c_int, [C.c_char_p, C.c_void_p, I64, I64, DP, I64, DP, I64, DP]),
 }
 
 
@@ -129,6 +130,30 @@ def fcidump_read_device(path, norb, e2_dev_ptr, stream=0):
     _err(lib.ccq_b200_fcidump_read_device(os.fsencode(path), norb, _p(e1), C.c_void_p(e2_dev_ptr), C.byref(en),
                                           C.c_void_p(stream)))
     return np.ascontiguousarray(e1), en.value
+
+
+def walkers_read(path, froz, occ_a, occ_b, orbs, nel, with_sd=True, t4=True):
+    """Cluster amplitudes of a FCIQMC walker file: (t_vec with T1..T3, {T4A..T4E: block} or None,
+    dict(c_hf, records, quadruples, higher))."""
+    from . import integrals as I
+    lib = load()
+    lay = I.TLayout(I.Dims(froz, occ_a, occ_b, orbs))
+    t = np.zeros(lay.t_size)
+    n4 = sum(int(np.prod(s)) for s in lay.t4_shape.values())
+    t4v = np.zeros(n4) if t4 else None
+    info = np.zeros(4)
+    dims = Dims(froz, occ_a, occ_b, orbs)
+    _err(lib.ccq_b200_walkers_read(os.fsencode(path), C.byref(dims), nel, int(bool(with_sd)), _p(t), t.size,
+                                   _p(t4v) if t4 else None, n4 if t4 else 0, _p(info)))
+    blocks = None
+    if t4:
+        blocks, off = {}, 0
+        for b in I.T4_ORDER:
+            shp = lay.t4_shape[b]
+            k = int(np.prod(shp))
+            blocks[b] = t4v[off:off + k].reshape(shp)
+            off += k
+    return t, blocks, dict(c_hf=info[0], records=int(info[1]), quadruples=int(info[2]), higher=int(info[3]))
 
 
 def checkpoint_info(path):

@@ -228,6 +228,23 @@ int ccq_b200_fcidump_read(const char *path, int64_t norb, double *e1, double *e2
 int ccq_b200_fcidump_read_device(const char *path, int64_t norb, double *e1, double *e2_dev, double *enuc,
                                  void *stream);
 
+/* ---- FCIQMC walker files (calc_type=CADFCIQMC) ------------------------------
+ * Replaces parse_fciqmc_c3 (src/ext_cor/ext_cor.f90:146-283), the C4 pass of
+ * process_fciqmc_c4 (src/ext_cor/contract_t4.f90:12-125) and the cluster
+ * analysis (cluster_analysis_up_t3, src/ext_cor/cluster_analysis.f90:10-258;
+ * the C4 / T1..T3 products of drive_t4_contraction, contract_t4.f90:241-479).
+ * Reads records "c_id coef occ_1 .. occ_m" (m = nel - 2 froz spin orbitals,
+ * numbered from the first unfrozen one, odd alpha, even beta), divides every
+ * CI coefficient by the Hartree-Fock one and writes T = ln(1 + C) rank by
+ * rank: t_vec (t_size = the T1..T3 size, ccq's t_vec layout) holds T1 and T2
+ * (zero unless with_sd, the ext_cor_sd key) and T3 on every triple; t4 (may be
+ * NULL; t4_size = the five T4 blocks in the layout of ccq_b200_block, T4A..T4E
+ * one after the other) holds T4 on every quadruple, C4 entering where the file
+ * has one.  info[0..3] = the Hartree-Fock coefficient, records read,
+ * distinct quadruples, records above quadruples (skipped).  Host only. */
+int ccq_b200_walkers_read(const char *path, const ccq_b200_dims *dims, int64_t nel, int64_t with_sd,
+                          double *t_vec, int64_t t_size, double *t4, int64_t t4_size, double *info);
+
 /* ---- learned warm start ---------------------------------------------------------
  * A per-amplitude multilayer perceptron (no counterpart in the reference, which
  * starts every solve from T = 0): y = w3 . tanh(W2 tanh(W1 x + b1) + b2) + b3 with

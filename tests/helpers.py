@@ -47,6 +47,21 @@ def fci_cluster_amplitudes(so, nmax=4):
     """
     from oracle.detcc import DetCC
     dc = DetCC(so.h, so.v, so.O)
+    psi, e = fci_state(so, dc)
+    ts = {}
+    for n in range(1, nmax + 1):
+        C = dc.residual({}, n, w=psi)
+        if ts:
+            C = C - dc.residual({}, n, w=dc.exp_t(ts, dc.phi))
+        ts[n] = C
+    return ts, e
+
+
+def fci_state(so, dc=None):
+    """FCI ground state of a SpinOrbitalSystem in the Sz sector of the reference, as a Fock-space
+    vector of oracle.detcc with <Phi|psi> = 1, and E_FCI - E_ref."""
+    from oracle.detcc import DetCC
+    dc = dc or DetCC(so.h, so.v, so.O)
     fs = dc.fs
     states = fs.states
     pc = np.array([bin(int(x)).count('1') for x in states])
@@ -64,10 +79,4 @@ def fci_cluster_amplitudes(so, nmax=4):
     psi = np.zeros(1 << so.N)
     psi[sel] = U[:, 0]
     psi /= psi[(1 << so.O) - 1]
-    ts = {}
-    for n in range(1, nmax + 1):
-        C = dc.residual({}, n, w=psi)
-        if ts:
-            C = C - dc.residual({}, n, w=dc.exp_t(ts, dc.phi))
-        ts[n] = C
-    return ts, float(w[0]) - dc.e_ref()
+    return psi, float(w[0]) - dc.e_ref()
