@@ -1125,9 +1125,12 @@ void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
 // ops[from, to) issued for stream capture as a DAG.  Every GETT waits only for
 // the GETTs it reads from, the last overwrite of its output and the earlier
 // readers of that output; beta = 1 writers of one buffer do not wait for each
-// other (their epilogues add with reductions).  Everything else (assembles,
-// copies, zeroing, split GETTs, whose slicing shares one workspace) is a
-// barrier on the capturing stream.  Independent contractions then run on side
+// other (their epilogues add with reductions).  Jacobi and copy assembles,
+// buffer copies and zeroing are nodes of the same kind (they overwrite their
+// output), so an assemble overlaps the next block's contractions that do not
+// read it.  The rest (split GETTs, whose slicing shares one workspace, and the
+// left-solve and CR-CC(2,3) kernels that accumulate scalars) is a barrier on
+// the capturing stream.  Independent contractions then run on side
 // streams at the same time.
 // every t_vec block resident on the device, and the last sweep op that writes it
 void prepare_copy_out(ccq_b200_ctx *c) {
@@ -1199,6 +1202,8 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
     };
     std::map<std::string, BufState> st;
     std::vector<size_t> pending;
+    // CCQ_B200_DAG_SERIAL set: assembles, copies and zeroing are barriers (the earlier schedule, for comparison)
+    const bool serial_nodes = getenv("CCQ_B200_DAG_SERIAL") != nullptr;
     cudaEvent_t gate = c->cap_ev;   // the last barrier (or the capture's start)
     CK(cudaEventRecord(gate, c->stream));
     int rr = 0;
@@ -1211,8 +1216,11 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         Op &o = c->plan.ops[i];
         if (o.kind == OP_PHASE || o.frozen) continue;
         if (o.kind == OP_GETT && (o.skip || o.g.M == 0 || o.g.N == 0)) continue;
-        const bool barrier = o.kind != OP_GETT ||
-                             use_split(c, o);
+        // Jacobi / copy assembles, buffer copies and zeroing are nodes too: each reads its term
+        // buffers (and its own block) and overwrites one buffer
+        const bool plain_node = !serial_nodes && ((o.kind == OP_ASM && o.asmargs.mode != 2) ||
+                                                  o.kind == OP_COPY || o.kind == OP_ZERO);
+        const bool barrier = (o.kind != OP_GETT && !plain_node) || (o.kind == OP_GETT && use_split(c, o));
         if (barrier) {
             join();
             run_op(c, o, c->stream);
@@ -1223,15 +1231,52 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         }
         std::vector<size_t> deps;
         auto add = [&](const std::vector<size_t> &v) { deps.insert(deps.end(), v.begin(), v.end()); };
-        std::vector<std::string> ins = {o.a.buf, o.b.buf};
-        for (size_t m : o.group_ops) {
-            ins.push_back(c->plan.ops[m].a.buf);
-            ins.push_back(c->plan.ops[m].b.buf);
+        std::vector<std::string> ins;
+        std::string out;
+        bool overwrite = true;
+        if (o.kind == OP_GETT) {
+            ins = {o.a.buf, o.b.buf};
+            for (size_t m : o.group_ops) {
+                ins.push_back(c->plan.ops[m].a.buf);
+                ins.push_back(c->plan.ops[m].b.buf);
+            }
+            out = o.c.buf;
+            // a grouped launch carries the beta of its first member (g.beta), not its own
+            overwrite = !o.g.beta || o.zero_first || o.g.K == 0;
+        } else if (o.kind == OP_ASM) {
+            for (auto &t : o.terms) ins.push_back(t.second.buf);
+            ins.push_back(o.block);
+            out = o.block;
+        } else if (o.kind == OP_COPY) {
+            ins = {o.arg1};
+            out = o.arg0;
+        } else {
+            out = o.arg0;
         }
-        for (auto &b : ins) add(st[b].writers);
-        BufState &cs = st[o.c.buf];
-        // a grouped launch carries the beta of its first member (g.beta), not its own
-        const bool overwrite = !o.g.beta || o.zero_first || o.g.K == 0;
+        // the Z/X work buffers of different block phases share one arena: an access also waits for
+        // every earlier access to a buffer whose memory overlaps
+        auto alias_deps = [&](const std::string &nm) {
+            auto it = c->bufs.find(nm);
+            if (it == c->bufs.end() || !it->second.ptr) return;
+            const double *lo = it->second.ptr, *hi = lo + std::max(it->second.numel, 1LL);
+            for (auto &kv : st) {
+                if (kv.first == nm) continue;
+                auto jt = c->bufs.find(kv.first);
+                if (jt == c->bufs.end() || !jt->second.ptr) continue;
+                const double *l2 = jt->second.ptr, *h2 = l2 + std::max(jt->second.numel, 1LL);
+                if (l2 < hi && lo < h2) {
+                    add(kv.second.writers);
+                    add(kv.second.readers);
+                    add(kv.second.full);
+                }
+            }
+        };
+        for (auto &b : ins) {
+            add(st[b].writers);
+            alias_deps(b);
+        }
+        alias_deps(out);
+        BufState &cs = st[out];
         add(cs.readers);
         add(overwrite ? cs.writers : cs.full);
         cudaStream_t sd = c->side[rr++ % NSIDE];
@@ -1241,6 +1286,7 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         for (size_t d : deps) CK(cudaStreamWaitEvent(sd, c->opev[d], 0));
         run_op(c, o, sd);
         CK(cudaEventRecord(c->opev[i], sd));
+        copy_out_after(c, i, sd);
         pending.push_back(i);
         for (auto &b : ins) st[b].readers.push_back(i);
         if (overwrite) {
