@@ -250,12 +250,10 @@ void each_canonical(const Space &sp, int m, int nb, F f) {
 // writes v at every antisymmetric copy of the canonical excitation (h, p) into a dense block
 void fill_copies(double *blk, const Space &sp, int m, int nb, const Orb *h, const Orb *p, double v) {
     const int na = m - nb;
-    int perm[4][4];
-    std::vector<int> g[4];
-    for (int q = 0; q < na; ++q) g[0].push_back(q), g[2].push_back(q);
-    for (int q = 0; q < nb; ++q) g[1].push_back(q), g[3].push_back(q);
-    (void)perm;
-    std::vector<int> a0 = g[0], a1 = g[1], a2 = g[2], a3 = g[3];
+    // positions within the alpha holes, beta holes, alpha particles and beta particles
+    std::vector<int> a0, a1, a2, a3;
+    for (int q = 0; q < na; ++q) a0.push_back(q), a2.push_back(q);
+    for (int q = 0; q < nb; ++q) a1.push_back(q), a3.push_back(q);
     do {
         do {
             do {
