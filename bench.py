@@ -15,7 +15,8 @@ are independent replicas (one solve per GPU, no collective on the data path).
 ``e2e`` is the same metric through the C ABI with the T vector in pinned host
 memory: every step copies it to the device and back (ccq_b200_iterate_host,
 whose block copies overlap the sweep).  ``--impl reference`` times the CPU
-restatement of the reference algorithm (numpy + threaded BLAS) on this host.
+executor of this repository's CCSDT plan (numpy + threaded BLAS) on this host
+(ccq itself cannot be built: no Fortran compiler).
 
 Besides the headline legs (FP64 and split, each autotuned first), the line
 carries the convergence of the headline path to tol against the FP64 oracle
@@ -30,6 +31,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -107,7 +109,7 @@ class Clocks:
     def __init__(self, local):
         self.local = local
         self.proc = None
-        self.path = os.path.join(ROOT, 'gpurun_out', f'clocks_rank{local}.csv')
+        self.path = os.path.join(tempfile.gettempdir(), f'ccq_b200_clocks_rank{local}_{os.getpid()}.csv')
         self.stamps = []   # (host time, line count) when the timed window opens and closes
 
     def start(self):
@@ -222,8 +224,22 @@ def golden_c2():
     return None
 
 
+# FLOPs of one CCSDT iteration of the reference's own algorithm at 40 orbitals (o = 8, v = 32 per
+# spin): a static count over its egemm calls (2 k1 k2 k3 with the i1, i2, i3 set before each call)
+# and its explicit OpenMP loop bodies over the unique triples (2 per product term per inner
+# iteration) in src/cc/t1A..t3D_update.f90: GEMMs 4.8e10 + T3 loops 1.62e11.  This engine's plan
+# does more FLOPs for the same residuals (every term is a GETT of an antisymmetry-restricted view).
+REFERENCE_FLOPS_C2 = 2.10e11
+
+BASELINE_KIND = ('numpy executor of this repository\'s CCSDT contraction plan (oracle/blockcc.py, threaded '
+                 'BLAS); ccq itself cannot be built here or on the GPU box (no Fortran compiler)')
+
+
 def cpu_reference(system, steps, warmup, budget_s=150.0):
-    """Oracle (numpy restatement of the reference algorithm) on this host's cores."""
+    """The oracle port on this host's cores: oracle/blockcc.py executing the CCSDT plan in numpy.
+
+    This is the repository's own formulation run on the CPU, not ccq's Fortran diagram code (which no
+    compiler here can build); it is a reported baseline, not the reference's own speed."""
     from oracle.blockcc import BlockCC
     try:
         from threadpoolctl import threadpool_info
@@ -273,8 +289,7 @@ def run_reference(args, rank, world):
         'data': 'synthetic (seeded generator, no molecular integrals)',
         'config': {'workload': WORKLOAD, 'parallelism': 'cpu threads', 'l2': 'working set > L2'},
         'cpu_baseline': {'value': r['s_per_iter'], 'unit': 's/iter', 'cores': r['cores'], 'kind': 'port',
-                         'sample': f"{r['iters_timed']} full CCSDT iteration(s) after {w} warm-up, numpy restatement "
-                                   'of the reference algorithm (ccq has no Fortran compiler on this image)'},
+                         'sample': f"{r['iters_timed']} full CCSDT iteration(s) after {w} warm-up; " + BASELINE_KIND},
         'e2e': {'value': r['s_per_iter'], 'unit': 's/iter', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line), flush=True)
@@ -406,7 +421,92 @@ def time_leg(ctx, it0, steps, world):
     return ms, es
 
 
+# ---------------------------------------------------------------------------
+# single-kernel and single-sweep cases for profiler captures (small device footprint):
+#   python bench.py --case egemm K1 K2 K3 [repeats]
+#   python bench.py --case egemm_split K1 K2 K3 [slices] [tile|persistent]
+#   python bench.py --case sweep fp64|split OUTFILE [warm-up iterations] [0|1|2|3|tune]
+#   python bench.py --case warmstart CCSDT|CCSDTQ NORB NEL [COUNT TRAIN EPOCHS]
+# egemm runs ccq_b200_egemm (the FP64 GETT kernel) on random column-major operands; the vvvv
+# ladder of the CCSDT T3 update at 40 orbitals is (1024, 16384, 1024).
+# ---------------------------------------------------------------------------
+def run_case(argv):
+    from ccq_b200 import lib
+    kind = argv[0]
+    if kind == 'egemm':
+        k1, k2, k3 = (int(x) for x in argv[1:4])
+        rep = int(argv[4]) if len(argv) > 4 else 1
+        rng = np.random.default_rng(0)
+        A = np.asfortranarray(rng.normal(size=(k3, k1)))
+        B = np.asfortranarray(rng.normal(size=(k3, k2)))
+        for _ in range(rep):
+            t0 = time.perf_counter()
+            C = lib.egemm(k1, k2, k3, A, B)
+            dt = time.perf_counter() - t0
+        ref = B[:, :64].T @ A[:, :64]
+        err = float(np.abs(C[:64, :64] - ref).max())
+        print(f'egemm {k1}x{k2}x{k3}: wall {dt * 1e3:.2f} ms (incl. copies), max err {err:.2e}')
+        assert err < 1e-9
+    elif kind == 'egemm_split':
+        k1, k2, k3 = (int(x) for x in argv[1:4])
+        S = int(argv[4]) if len(argv) > 4 else 4
+        persistent = (argv[5] == 'persistent') if len(argv) > 5 else None
+        rng = np.random.default_rng(0)
+        A = np.asfortranarray(rng.normal(size=(k3, k1)))
+        B = np.asfortranarray(rng.normal(size=(k3, k2)))
+        for _ in range(3 if persistent is not None else 1):
+            C = lib.egemm_split(k1, k2, k3, A, B, S, persistent=persistent)
+        ref = B[:, :64].T @ A[:, :64]
+        err = float(np.abs(C[:64, :64] - ref).max())
+        # the split bound: 2^(-7S+2) k3 max|A| max|B|
+        bound = 2.0 ** (-7 * S + 2) * k3 * np.abs(A[:, :64]).max() * np.abs(B[:, :64]).max()
+        print(f'egemm_split {k1}x{k2}x{k3} S={S}: max err {err:.2e} (bound {bound:.2e})')
+        assert err <= bound
+    elif kind == 'sweep':
+        # per-operation device times of one CCSDT sweep on the 40-orbital workload
+        import os
+        from ccq_b200 import synth
+        prec = argv[1] if len(argv) > 1 else 'fp64'
+        out = argv[2] if len(argv) > 2 else 'ops_profile.txt'
+        warm = int(argv[3]) if len(argv) > 3 else 3
+        family = argv[4] if len(argv) > 4 else '0'   # kernel family to force (0..3) or 'tune'
+        s = synth.system(synth.C2)
+        d = s['dims']
+        # a one-vector DIIS ring keeps the device footprint small for profiler captures
+        ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CCSDT', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                          s['v_bb'], diis_space=1)
+        ctx.set_precision(lib.PREC_SPLIT if prec == 'split' else lib.PREC_FP64, 4)
+        if family == 'tune':
+            print('autotune (ms before, after):', ctx.autotune(3))
+        elif family != '0':
+            ctx.force_tile(int(family))
+        for it in range(1, warm + 1):
+            ctx.iterate(it)
+        if os.path.exists(out):
+            os.remove(out)
+        os.environ['CCQ_B200_PROFILE_DUMP'] = out
+        ctx.profile(True)
+        ctx.iterate(warm + 1)
+        print(ctx.profile_get())
+        ctx.close()
+    elif kind == 'warmstart':
+        # the learned warm start on a lambda-swept family: METHOD NORB NEL [COUNT TRAIN EPOCHS]
+        import json
+        from ccq_b200 import warmstart
+        method, norb, nel = argv[1], int(argv[2]), int(argv[3])
+        count = int(argv[4]) if len(argv) > 4 else 200
+        train = int(argv[5]) if len(argv) > 5 else 150
+        epochs = int(argv[6]) if len(argv) > 6 else 600
+        r = warmstart.study(method, norb, nel, count, train, epochs=epochs, log=print)
+        print(json.dumps(r))
+    else:
+        raise SystemExit(f'unknown case {kind}')
+
+
+
 def main():
+    if len(sys.argv) > 2 and sys.argv[1] == '--case':
+        return run_case(sys.argv[2:])
     args = parse()
     import torch
     rank, world, local = dist_init(args.gpus)
@@ -475,8 +575,7 @@ def main():
 
     # per-kernel roofline: eager sweep with events around every launch (and every launch's shape in a dump)
     ctx.set_precision(lib.PREC_SPLIT if headline == 'split' else lib.PREC_FP64, args.slices)
-    dump = os.path.join(ROOT, 'gpurun_out', f'bench_ops_rank{rank}.txt')
-    os.makedirs(os.path.dirname(dump), exist_ok=True)
+    dump = os.path.join(tempfile.gettempdir(), f'ccq_b200_ops_rank{rank}_{os.getpid()}.txt')
     if os.path.exists(dump):
         os.remove(dump)
     os.environ['CCQ_B200_PROFILE_DUMP'] = dump
@@ -606,8 +705,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference(s, 1, 0, budget_s=60.0)
         cpu = {'value': r['s_per_iter'], 'unit': 's/iter', 'cores': r['cores'], 'kind': 'port',
-               'sample': 'first CCSDT iteration of the same workload (one full update sweep + energy + ring), numpy '
-                         'restatement of the reference algorithm with threaded BLAS'}
+               'sample': 'first CCSDT iteration of the same workload (one full update sweep + energy + ring); '
+                         + BASELINE_KIND}
     if rank == 0:
         line = {
             'metric': METRIC, 'value': head['s_per_iter'], 'unit': 's/iter', 'n_gpus': world,
@@ -617,7 +716,13 @@ def main():
             'data': 'synthetic (seeded generator, no molecular integrals)',
             'config': {'workload': WORKLOAD, 'precision': headline, 'parallelism': f'replicas x{world}',
                        'l2': 'working set (T3 4x134 MB + DIIS ring) > 126 MB L2, no flush'},
-            'tflops': head['tflops'], 'legs': results, 'autotune': tuning or None,
+            'tflops': head['tflops'],
+            'flops_per_iter': head['flops_per_iter'],
+            'flops_reference_per_iter': REFERENCE_FLOPS_C2,
+            'tflops_reference_count': REFERENCE_FLOPS_C2 / head['s_per_iter'] / 1e12,
+            'flops_note': 'tflops = this engine\'s own GETT FLOPs per iteration / time; tflops_reference_count = the '
+                          'reference algorithm\'s static FLOP count per iteration / the same time',
+            'legs': results, 'autotune': tuning or None,
             'speedup_split_vs_fp64': (results['fp64']['s_per_iter'] / results['split']['s_per_iter']
                                       if 'split' in results else None),
             'roofline': roofline,

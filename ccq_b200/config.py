@@ -24,6 +24,21 @@ import math
 from dataclasses import dataclass, field
 
 
+# get_acc_opts (src/parser.f90:527-542): key -> number of factors
+ACC_KEYS = {'t2t2_t2': 5, 't3_t2': 2, 't1t3_t2': 4, 't2t2_t3': 3, 't2t3_t3': 5}
+
+
+def _reals(val, n, key):
+    """List-directed read of n reals (Fortran ``read(val, *) array``): blanks or commas separate."""
+    toks = [t for t in val.replace(',', ' ').split() if t]
+    if len(toks) < n:
+        raise ValueError(f'CONFIGURATION ERROR: {key} needs {n} real values')
+    try:
+        return [float(t.replace('d', 'e').replace('D', 'E')) for t in toks[:n]]
+    except ValueError:
+        raise ValueError(f'CONFIGURATION ERROR: {key} must be {n} reals') from None
+
+
 def _logical(val):
     v = val.strip().lower().strip('.')
     if v in ('true', 't', 'yes', '1'):
@@ -70,6 +85,17 @@ class Config:
     ext_cor_file: str = ''
     ext_cor_sd: bool = True
     ext_cor_file_h5: bool = False
+    # ACC diagram factors (acc_t, src/cc_types.f90:12-20), all 1.0 by default (src/parser.f90:838-842)
+    acc: dict = field(default_factory=lambda: {k: [1.0] * n for k, n in ACC_KEYS.items()})
+    # keys that get_calc_macros overwrites for every served calc_type (src/parser.f90:339-432)
+    lvl_t_key: bool = False
+    lvl_q_key: bool = False
+    act_ind_t: int = 0
+    act_ind_q: int = 0
+    sorted_ints: bool = False
+    echo: bool = False
+    output_log: str = ''
+    lines: list = field(default_factory=list)
     # derived (process_sys_data)
     froz: int = 0
     occ_a: int = 0
@@ -90,6 +116,10 @@ class Config:
         self.act_occ_b = max(self.occ_b - self.act_occ, self.froz)
         self.act_unocc_a = min(self.occ_a + self.act_unocc, self.orbs)
         return self
+
+    def acc_default(self):
+        """True when every ACC factor is 1.0 (the CC methods as derived)."""
+        return all(x == 1.0 for v in self.acc.values() for x in v)
 
     def bin_path(self):
         """Checkpoint file: output_bin, else tvec_<label>.bin (tvec.bin without a label)."""
@@ -126,6 +156,11 @@ class Config:
         elif ct == 'CR-CC(2,3)':
             # src/parser.f90:368-377: CCSD, then hbar, left CCSD and the MM(2,3) correction
             self.lvl_t, self.lvl_q = False, False
+        elif ct == 'DCSD-MC':
+            # src/parser.f90:350-358: CADFCIQMC-type external correction with the T2^2 diagrams of the
+            # doubles scaled by (1, 0, 1/2, 1/2, 0), the dropped fractions taken from the walker T2
+            self.acc['t2t2_t2'] = [1.0, 0.0, 0.5, 0.5, 0.0]
+            self.lvl_t, self.lvl_q = False, False
         else:
             raise ValueError(f'calc_type {ct!r} is not served by this engine '
                              '(CCSD, CCSDT, CCSDTQ, CCSDt, CC(t;3), CR-CC(2,3), CADFCIQMC are; the others stay on the CPU program)')
@@ -134,6 +169,7 @@ class Config:
 
 def parse_lines(lines):
     cfg = Config()
+    cfg.lines = [ln.rstrip('\n') for ln in lines]
     for raw in lines:
         line = raw.rstrip('\n')
         if '#' in line or '!' in line:
@@ -223,6 +259,26 @@ def _apply(cfg, key, val):
         cfg.act_occ = int(val)
     elif key == 'act_unocc':
         cfg.act_unocc = int(val)
+    elif key in ACC_KEYS:
+        cfg.acc[key] = _reals(val, ACC_KEYS[key], key)
+    elif key in ('lvl_t', 'lvl_q'):
+        # read, checked, then overwritten by get_calc_macros for every served calc_type
+        try:
+            setattr(cfg, key + '_key', _logical(val))
+        except ValueError:
+            raise ValueError(f'CONFIGURATION ERROR: {key} must logical') from None
+    elif key in ('act_ind_t', 'act_ind_q'):
+        setattr(cfg, key, int(val))
+    elif key == 'sorted_ints':
+        # ccq's sorted-integral code path for CCSDt; the integrals here are always resident in full
+        cfg.sorted_ints = _logical(val)
+    elif key in ('print_config', 'echo'):
+        cfg.echo = True
+    elif key == 'output_log':
+        cfg.output_log = val
+    elif key == 'ext_cor':
+        # honoured by ccq only for calc_type=dev (src/parser.f90:619-623)
+        cfg.extra[key] = val
     else:
         cfg.extra[key] = val
 

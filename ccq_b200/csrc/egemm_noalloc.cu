@@ -76,6 +76,8 @@ extern "C" int ccq_b200_egemm_dev_noalloc(int64_t k1, int64_t k2, int64_t k3, co
     if (k1 == 0 || k2 == 0) return 0;
     if (!C || (k3 > 0 && (!A || !B))) return CCQ_B200_EINVAL;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // a launch error pending from earlier work on this thread is not this call's
+    (void)cudaGetLastError();
     int *t = nullptr;
     int rc = table_address(&t);
     if (rc) return rc;

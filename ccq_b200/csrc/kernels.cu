@@ -646,22 +646,32 @@ cudaError_t skinny_attr() {
     return e;
 }
 
+// The shared-memory limits set by cudaFuncSetAttribute belong to the current
+// device, so they are set once per device (the first GETT launch or context
+// creation on each device), not once per process.
+constexpr int kPrepDevices = 64;
+
 cudaError_t gett_f64_prepare() {
-    static std::once_flag once;
-    static cudaError_t err = cudaSuccess;
-    std::call_once(once, [] {
-        err = skinny_attr<16, false, SST>();
-        if (err == cudaSuccess) err = skinny_attr<16, true, SST>();
-        if (err == cudaSuccess) err = skinny_attr<32, false, SST>();
-        if (err == cudaSuccess) err = skinny_attr<32, true, SST>();
-        if (err == cudaSuccess) err = skinny_attr<16, false, 2>();
-        if (err == cudaSuccess) err = skinny_attr<16, true, 2>();
-        if (err == cudaSuccess) err = skinny_attr<32, false, 2>();
-        if (err == cudaSuccess) err = skinny_attr<32, true, 2>();
-        if (err == cudaSuccess) err = gett_attr<false, 3>();
-        if (err == cudaSuccess) err = gett_attr<true, 3>();
+    static std::once_flag once[kPrepDevices];
+    static cudaError_t err[kPrepDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kPrepDevices) return cudaErrorInvalidDevice;
+    std::call_once(once[dev], [dev] {
+        cudaError_t r = skinny_attr<16, false, SST>();
+        if (r == cudaSuccess) r = skinny_attr<16, true, SST>();
+        if (r == cudaSuccess) r = skinny_attr<32, false, SST>();
+        if (r == cudaSuccess) r = skinny_attr<32, true, SST>();
+        if (r == cudaSuccess) r = skinny_attr<16, false, 2>();
+        if (r == cudaSuccess) r = skinny_attr<16, true, 2>();
+        if (r == cudaSuccess) r = skinny_attr<32, false, 2>();
+        if (r == cudaSuccess) r = skinny_attr<32, true, 2>();
+        if (r == cudaSuccess) r = gett_attr<false, 3>();
+        if (r == cudaSuccess) r = gett_attr<true, 3>();
+        err[dev] = r;
     });
-    return err;
+    return err[dev];
 }
 
 // ---------------------------------------------------------------------------

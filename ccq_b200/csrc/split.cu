@@ -715,13 +715,10 @@ CUtensorMap make_map(signed char *base, long long rows, long long Kp, int S, int
 template <int S, int NT, int STAGES>
 void launch_split_persistent(const CUtensorMap &ta, const CUtensorMap &tb, const SplitArgs &a, cudaStream_t s) {
     const int tiles = ((a.M + TM - 1) / TM) * ((a.N + NT - 1) / NT);
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms < 1) sms = 148;
-    }
+    int dev = 0, sms = 0;   // SM count of the current device (one CTA per SM)
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms < 1) sms = 148;
     const int grid = std::min(tiles, sms);
     split_gett_persistent<S, NT, STAGES><<<grid, 320, Persist<S, NT, STAGES>::SMEM, s>>>(ta, tb, a);
 }

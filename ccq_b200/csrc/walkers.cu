@@ -124,17 +124,21 @@ void gen_patterns(int hleft, int pleft, std::vector<std::pair<int, int>> &cur, s
     }
 }
 
-const std::vector<Pattern> &patterns(int n) {
-    static std::vector<Pattern> pats[5];
-    static bool done = false;
-    if (!done) {
+struct PatternTables {
+    std::vector<Pattern> pats[5];
+    PatternTables() {
         for (int m = 1; m <= 4; ++m) {
             std::vector<std::pair<int, int>> cur;
             gen_patterns((1 << m) - 1, (1 << m) - 1, cur, pats[m]);
         }
-        done = true;
     }
-    return pats[n];
+};
+
+// built once, on first use, by whichever thread gets there first (a function-local
+// static is initialised exactly once even when several threads read walker files)
+const std::vector<Pattern> &patterns(int n) {
+    static const PatternTables tables;
+    return tables.pats[n];
 }
 
 // dense spin block of rank m with nb beta electrons: [o_a..][o_b..][v_a..][v_b..], C order

@@ -225,6 +225,25 @@ def run(input_path, out=print, base_dir='.'):
             raise ValueError('CONFIGURATION ERROR: FCIDUMP file not found')
         cfgmod.apply_fcidump(cfg, fp)
     cfg.calc_macros()
+    if not cfg.acc_default():
+        bad = ', '.join(f'{k}={v}' for k, v in cfg.acc.items() if any(x != 1.0 for x in v))
+        raise ValueError(f'CONFIGURATION ERROR: ACC diagram factors other than 1.0 are not served by this '
+                         f'engine ({bad}); CCSD, CCSDT, CCSDTQ and their variants run with all factors 1.0')
+    if cfg.output_log:
+        # output_log (src/parser.f90:719-720): the calculation's output also goes to that file
+        path = cfg.output_log if os.path.isabs(cfg.output_log) else os.path.join(base_dir, cfg.output_log)
+        log = open(path, 'w')
+        out0 = out
+
+        def out(line, _log=log, _out=out0):
+            _out(line)
+            _log.write(line + '\n')
+            _log.flush()
+    if cfg.echo:
+        # print_config / echo: the input file as read
+        out('Input configuration')
+        for ln in cfg.lines:
+            out('  ' + ln)
     sysd = load_system(cfg, base_dir)
     out('Calculation parameters: ' + cfgmod.format_config(cfg))
     out(f"  Reference energy {sysd['e_ref']:.12f}")

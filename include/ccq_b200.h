@@ -95,7 +95,10 @@ void egemm2_(const int64_t *k2, const int64_t *k3, const double *A, const double
  * be at most 65536 (else CCQ_B200_ERANGE, nothing enqueued).  The first call on
  * a device looks up that array's address; make that first call before any
  * stream capture.  All calls share the one array: calls that overlap on the
- * GPU (different streams, no ordering between them) race on it. */
+ * GPU (different streams, no ordering between them) race on it.  The return
+ * code reports argument and launch errors only (a launch error left pending by
+ * earlier, unrelated work is cleared on entry and not blamed on this call);
+ * errors during execution surface on the stream, like any kernel's. */
 int ccq_b200_egemm_dev_noalloc(int64_t k1, int64_t k2, int64_t k3,
                                const double *A, const double *B, double *C, void *stream);
 

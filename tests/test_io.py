@@ -29,10 +29,12 @@ def test_defaults():
 
 
 def test_unknown_calc_type():
-    # active-space CCSDt stays on the reference's CPU program
+    # CCSDt without an active space is a configuration error (src/parser.f90:251-254)
     c = config.Config(calc_type='CCSDt')
     with pytest.raises(ValueError):
         c.calc_macros()
+    with pytest.raises(ValueError, match='not served'):
+        config.Config(calc_type='stoch-CC').calc_macros()
 
 
 def test_crcc23_macros():
@@ -84,3 +86,47 @@ def test_spin_blocks_antisymmetric():
     np.testing.assert_allclose(vaa, -vaa.transpose(1, 0, 2, 3), atol=1e-15)
     np.testing.assert_allclose(vaa, -vaa.transpose(0, 1, 3, 2), atol=1e-15)
     np.testing.assert_allclose(vab, vab.transpose(2, 3, 0, 1), atol=1e-15)
+
+
+def test_acc_keys_parsed(tmp_path):
+    # get_acc_opts (src/parser.f90:527-542): list-directed reals, blanks or commas
+    p = tmp_path / 'x.inp'
+    p.write_text('nel=4\nnvir=4\ncalc_type=CCSD\nt2t2_t2=1.0, 0.0 0.5,0.5 0\nt3_t2=1d0 0.5D0\n')
+    c = config.parse(str(p)).calc_macros()
+    assert c.acc['t2t2_t2'] == [1.0, 0.0, 0.5, 0.5, 0.0]
+    assert c.acc['t3_t2'] == [1.0, 0.5]
+    assert c.acc['t1t3_t2'] == [1.0] * 4 and not c.acc_default()
+    p.write_text('nel=4\nnvir=4\ncalc_type=CCSD\nt2t3_t3=1 1\n')
+    with pytest.raises(ValueError):
+        config.parse(str(p))
+
+
+def test_acc_defaults_and_dcsd_macro():
+    c = config.Config(calc_type='CCSD').calc_macros()
+    assert c.acc_default()
+    # DCSD-MC sets t2t2_t2 after the keys are read (src/parser.f90:350-358)
+    c = config.Config(calc_type='DCSD-MC').calc_macros()
+    assert c.acc['t2t2_t2'] == [1.0, 0.0, 0.5, 0.5, 0.0] and not c.acc_default()
+
+
+def test_run_keys(tmp_path):
+    p = tmp_path / 'x.inp'
+    p.write_text('nel=4\nnvir=4\ncalc_type=CCSD\nlvl_t=.true.\nsorted_ints=.true.\necho\noutput_log=o.log\n')
+    c = config.parse(str(p)).calc_macros()
+    # lvl_t is read and checked, then get_calc_macros decides (src/parser.f90:360-366)
+    assert c.lvl_t_key and not c.lvl_t and c.sorted_ints and c.echo and c.output_log == 'o.log'
+    p.write_text('nel=4\nnvir=4\ncalc_type=CCSD\nlvl_q=maybe\n')
+    with pytest.raises(ValueError, match='lvl_q must logical'):
+        config.parse(str(p))
+
+
+def test_acc_factors_refused_by_driver(tmp_path):
+    # a deck whose ACC factors differ from 1.0 must not run as plain CC
+    from ccq_b200 import driver
+    p = tmp_path / 'x.inp'
+    p.write_text('nel=4\nnvir=4\ncalc_type=CCSDT\nt3_t2=0.0 1.0\n')
+    with pytest.raises(ValueError, match='ACC diagram factors'):
+        driver.run(str(p), out=lambda x: None, base_dir=str(tmp_path))
+    p.write_text('nel=4\nnvir=4\ncalc_type=DCSD-MC\next_cor_file=w\n')
+    with pytest.raises(ValueError, match='ACC diagram factors'):
+        driver.run(str(p), out=lambda x: None, base_dir=str(tmp_path))
