@@ -25,7 +25,10 @@ CASES = ['ccsdt_open_n10', 'ccsdt_froz_n10', 'ccsdt_rhf_n10', 'ccsdtq_open_n7']
 
 
 def _fixture(name):
-    data = json.load(open(os.path.join(GOLDEN, 'dense_midsize.json')))
+    p = os.path.join(GOLDEN, 'dense_midsize.json')
+    if not os.path.exists(p):
+        pytest.skip('dense_midsize.json not generated')
+    data = json.load(open(p))
     if name not in data:
         pytest.skip(f'{name} not in dense_midsize.json')
     return data[name]
