@@ -144,6 +144,10 @@ class Clocks:
         sm, smax, reasons = [], [], set()
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
         lines = open(self.path).readlines()
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         window = 'timed region'
         if len(self.stamps) == 2 and None not in self.stamps and self.stamps[1] > self.stamps[0]:
             lines = lines[self.stamps[0]:self.stamps[1]]
@@ -230,6 +234,16 @@ def golden_c2():
 # iteration) in src/cc/t1A..t3D_update.f90: GEMMs 4.8e10 + T3 loops 1.62e11.  This engine's plan
 # does more FLOPs for the same residuals (every term is a GETT of an antisymmetry-restricted view).
 REFERENCE_FLOPS_C2 = 2.10e11
+
+# DRAM bytes (read + write) per gett_f64 launch in one tuned split-precision sweep of this workload,
+# from one ncu capture of every GETT launch of that sweep (dram__bytes_read.sum + dram__bytes_write.sum,
+# a single-pass metric set, full size): 22.0 GB over 490 launches of the 64x64, skinny and small-K
+# families.  Command: `ncu --nvtx --nvtx-include "sweep/" --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none --csv
+# python bench.py --case sweep split /tmp/ops_split.txt 3 tune`.
+GETT_F64_TRAFFIC = 44.93e6
+GETT_F64_TRAFFIC_NOTE = ('traffic = DRAM bytes per gett_f64 launch (mean over the 490 launches of one tuned split '
+                         'sweep, ncu dram__bytes_read.sum + dram__bytes_write.sum, captured at full size)')
 
 BASELINE_KIND = ('numpy executor of this repository\'s CCSDT contraction plan (oracle/blockcc.py, threaded '
                  'BLAS); ccq itself cannot be built here or on the GPU box (no Fortran compiler)')
@@ -399,6 +413,8 @@ def batch_leg(rank, world):
     return {'workload': '64 x CCSD, norb ~ U{16..48} (seed 1000+i), nel = 2 floor(norb/5), L = 2 norb, sigma 0.03, '
                         'tol 1e-8', 'solves_per_s': len(specs) / solve_s, 'solve_wall_s': solve_s,
             'setup_wall_s': setup_s, 'e2e_solves_per_s': len(specs) / (solve_s + setup_s),
+            'setup_thread_s': {'integrals': sum(r['synth_s'] for r in res),
+                               'contexts': sum(r['context_s'] for r in res)},
             'failed': sum(r['failed'] for r in res), 'iterations_total': sum(r['iterations'] for r in res),
             'device_ms_sum': sum(r['device_ms'] for r in res),
             'max_dE_vs_oracle': de, 'iterations_match_oracle': it_ok,
@@ -486,7 +502,13 @@ def run_case(argv):
             os.remove(out)
         os.environ['CCQ_B200_PROFILE_DUMP'] = out
         ctx.profile(True)
+        import torch
+        torch.cuda.synchronize()
+        # an NVTX range around the profiled sweep: `ncu --nvtx --nvtx-include "sweep/"` captures its launches only
+        torch.cuda.nvtx.range_push('sweep')
         ctx.iterate(warm + 1)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         print(ctx.profile_get())
         ctx.close()
     elif kind == 'warmstart':
@@ -613,10 +635,11 @@ def main():
 
     def per_launch_roofline(fp64_peak, hbm_gbs):
         """gett_f64 launches against their own bound: max(FLOPs / DGEMM peak, algorithmic bytes / HBM)."""
-        bound = spent = 0.0
+        bound = spent = alg_bytes = 0.0
         nl = 0
         try:
             lines = open(dump).read().split('\n')
+            os.remove(dump)
         except OSError:
             return None
         for ln in lines:
@@ -631,9 +654,11 @@ def main():
             bound += max(fl / (fp64_peak * 1e12), by / (hbm_gbs * 1e9)) * 1e3
             spent += ms
             nl += 1
+            alg_bytes += by
         if not spent:
             return None
         return {'frac': bound / spent, 'bound_ms': bound / 2, 'spent_ms': spent / 2, 'launches': nl // 2,
+                'algorithmic_bytes_per_launch': alg_bytes / nl,
                 'note': 'per launch max(2MNK / measured DGEMM peak, 8(M+N)K + 8 or 16 MN bytes / measured HBM), '
                         'summed over the gett_f64 launches of 2 eager sweeps, over their summed event times'}
 
@@ -642,11 +667,13 @@ def main():
         roofline = {'bound': 'hbm', 'achieved': None, 'peak': peaks_file['hbm_gbs'], 'unit': 'GB/s', 'frac': None}
     else:
         roofline = dict(gett_line(kname))
-    roofline.update({'kernel': kname, 'traffic': None, 'shares': shares, 'per_sweep': per_sweep,
-                     'per_launch_bound': per_launch_roofline(fp64_peak, peaks_file['hbm_gbs']),
+    plb = per_launch_roofline(fp64_peak, peaks_file['hbm_gbs'])
+    roofline.update({'kernel': kname, 'traffic': GETT_F64_TRAFFIC if kname == 'gett_f64' else None,
+                     'shares': shares, 'per_sweep': per_sweep, 'per_launch_bound': plb,
                      'secondary': {k: gett_line(k) for k in ('gett_f64', 'gett_split') if k != kname},
-                     'traffic_note': 'per-launch DRAM bytes vary by contraction shape; ncu figures for the dominant '
-                                     'shapes are in profiles/gett_f64_ccsdt40_shapes.md and profiles/split_gett_o4v4.md',
+                     'traffic_note': GETT_F64_TRAFFIC_NOTE + (
+                         '; algorithmic bytes per launch of this run: %.1f MB' % (plb['algorithmic_bytes_per_launch'] / 1e6)
+                         if plb else ''),
                      'note': 'achieved = algorithmic FLOPs of all launches of that kernel in 2 eager sweeps (CUDA '
                              'events around every launch) / their summed durations'})
 

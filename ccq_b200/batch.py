@@ -56,11 +56,15 @@ def shard(specs, world):
 
 class Instance:
     def __init__(self, spec, calc_type='CCSD', diis_space=5, graph=True):
+        t0 = time.perf_counter()
         s = synth.system(spec)
         d = s['dims']
         self.spec = spec
+        t1 = time.perf_counter()
         self.ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, calc_type, s['f_a'], s['f_b'], s['v_aa'],
                                s['v_ab'], s['v_bb'], diis_space=diis_space)
+        # host seconds spent generating the integrals and creating the context (threads overlap them)
+        self.t_synth, self.t_ctx = t1 - t0, time.perf_counter() - t1
         # one stream per instance: the instances overlap one another, so each replays a
         # single-stream graph (mode 2) rather than its own concurrent one
         self.ctx.use_graph(2 if graph else 0)
@@ -112,14 +116,24 @@ def create_instances(specs, calc_type='CCSD', diis_space=5, graph=True, threads=
 
 
 def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, graph=True, t_init=None,
-                keep_t=False):
+                keep_t=False, chunk=None):
     """Solve every instance; returns (results, timings).
 
     ``results[i]`` = dict(e_cor, iterations, failed, device_ms) (plus ``t``, the
     converged t_vec, with ``keep_t``); ``t_init[i]`` (a t_vec) replaces the
     T = 0 start of instance i.  Timings: wall seconds of context creation and
-    of the iterations.
+    of the iterations.  ``chunk`` bounds the number of contexts alive at once
+    (the instances are solved in consecutive groups of that size).
     """
+    if chunk and len(specs) > chunk:
+        res, tim = [], {'setup_s': 0.0, 'solve_s': 0.0}
+        for k in range(0, len(specs), chunk):
+            r, t = solve_batch(specs[k:k + chunk], tol, max_iter, calc_type, diis_space, graph,
+                               None if t_init is None else t_init[k:k + chunk], keep_t)
+            res += r
+            tim['setup_s'] += t['setup_s']
+            tim['solve_s'] += t['solve_s']
+        return res, tim
     t0 = time.perf_counter()
     insts = create_instances(specs, calc_type, diis_space, graph)
     if t_init is not None:
@@ -136,7 +150,8 @@ def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, g
                 x.step_finish(tol, max_iter)
             active = [x for x in active if not x.done]
         t2 = time.perf_counter()
-        res = [dict(e_cor=x.e, iterations=x.it, failed=x.failed, device_ms=x.device_ms) for x in insts]
+        res = [dict(e_cor=x.e, iterations=x.it, failed=x.failed, device_ms=x.device_ms, synth_s=x.t_synth,
+                    context_s=x.t_ctx) for x in insts]
         if keep_t:
             for r, x in zip(res, insts):
                 r['t'] = x.ctx.get_t()

@@ -1416,9 +1416,25 @@ int ccq_b200_last_error(char *buf, int64_t len) {
     return 0;
 }
 
+static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
+                     const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
+                     int64_t diis_space, ccq_b200_ctx **out, bool rowmajor);
+
 int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
                   const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
                   int64_t diis_space, ccq_b200_ctx **out) {
+    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, false);
+}
+
+int ccq_b200_init_rowmajor(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
+                           const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
+                           int64_t diis_space, ccq_b200_ctx **out) {
+    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, true);
+}
+
+static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
+                     const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
+                     int64_t diis_space, ccq_b200_ctx **out, bool rowmajor) {
     ccq_b200_ctx *c = nullptr;
     try {
         if (!dims || !calc_type || !f_a || !f_b || !v_aa || !v_ab || !v_bb || !out)
@@ -1466,15 +1482,19 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         // host-side integral preparation
         long long orbs = dims->orbs;
         std::vector<double> FA(n * n), FB(n * n);
+        // element (p, q) of f and (p, q, r, s) of v: column-major (Fortran) arrays, or row-major ones
+        // (ccq_b200_init_rowmajor)
+        auto F2 = [&](const double *x, long long p, long long q) {
+            return rowmajor ? x[q + orbs * p] : x[p + orbs * q];
+        };
         for (long long p = 0; p < n; ++p)
             for (long long q = 0; q < n; ++q) {
-                FA[p * n + q] = f_a[(p + fr) + orbs * (q + fr)];
-                FB[p * n + q] = f_b[(p + fr) + orbs * (q + fr)];
+                FA[p * n + q] = F2(f_a, p + fr, q + fr);
+                FB[p * n + q] = F2(f_b, p + fr, q + fr);
             }
         std::vector<double> HA(FA), HB(FB);
-        // v(p,q,r,s) of the Fortran (column-major) arrays
         auto V = [&](const double *x, long long p, long long q, long long r, long long s) {
-            return x[p + n * (q + n * (r + n * s))];
+            return rowmajor ? x[s + n * (r + n * (q + n * p))] : x[p + n * (q + n * (r + n * s))];
         };
         for (long long p = 0; p < n; ++p)
             for (long long q = 0; q < n; ++q) {
@@ -1511,19 +1531,24 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double
         // two-electron blocks: the column-major arrays go up as they are (staged in the
         // dressed buffer of the same size, which the first dressing overwrites) and
         // are reordered to [p][q][r][s] on the device
+        // (row-major arrays are already [p][q][r][s] and go straight into place)
         auto up4 = [&](const char *name, const char *stage, const double *f) {
             DevBuf &d = c->bufs.at(name);
             DevBuf &st = c->bufs.at(stage);
             const long long ne = n * n * n * n;
             if (d.numel != ne || st.numel != ne) throw Error(CCQ_B200_EPLAN, std::string("size of ") + name);
+            if (rowmajor) {
+                CK(cudaMemcpyAsync(d.ptr, f, sizeof(double) * ne, cudaMemcpyHostToDevice, c->stream));
+                return;
+            }
             CK(cudaMemcpyAsync(st.ptr, f, sizeof(double) * ne, cudaMemcpyHostToDevice, c->stream));
             launch_f2c4(st.ptr, d.ptr, n, c->stream);
         };
         up4("VAA0", "VAA", v_aa);
         up4("VAB0", "VAB", v_ab);
         up4("VBB0", "VBB", v_bb);
+        // this context's stream only: contexts created by other host threads keep running
         CK(cudaStreamSynchronize(c->stream));
-        CK(cudaDeviceSynchronize());
         stamp("upload");
         *out = c;
         return 0;

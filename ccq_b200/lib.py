@@ -41,6 +41,8 @@ SIGNATURES = {
     'ccq_b200_egemm2': (C.c_int, [I64, I64, DP, DP, DP]),
     'ccq_b200_init': (C.c_int, [C.POINTER(Dims), C.c_char_p, DP, DP, DP, DP, DP, I64, C.c_double, I64,
                                 C.POINTER(C.c_void_p)]),
+    'ccq_b200_init_rowmajor': (C.c_int, [C.POINTER(Dims), C.c_char_p, DP, DP, DP, DP, DP, I64, C.c_double, I64,
+                                C.POINTER(C.c_void_p)]),
     'ccq_b200_sizes': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(I64)]),
     'ccq_b200_set_t': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_get_t': (C.c_int, [C.c_void_p, DP, I64]),
@@ -219,11 +221,18 @@ class Context:
         self._lib = lib
         self.ptr = C.c_void_p()
         d = Dims(froz, occ_a, occ_b, orbs)
-        # Fortran (column-major) layout, as sys%ints arrays are in ccq
-        self._keep = [np.asfortranarray(x, dtype=np.float64) for x in (f_a, f_b, v_aa, v_ab, v_bb)]
+        arrs = (f_a, f_b, v_aa, v_ab, v_bb)
+        if all(isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous for x in arrs):
+            # row-major arrays go in as they are (ccq_b200_init_rowmajor): no transposed copies
+            self._keep = arrs
+            init = lib.ccq_b200_init_rowmajor
+        else:
+            # Fortran (column-major) layout, as sys%ints arrays are in ccq
+            self._keep = [np.asfortranarray(x, dtype=np.float64) for x in arrs]
+            init = lib.ccq_b200_init
         fa, fb, vaa, vab, vbb = self._keep
-        _err(lib.ccq_b200_init(C.byref(d), calc_type.encode(), _p(fa), _p(fb), _p(vaa), _p(vab), _p(vbb),
-                               int(bool(rhf)), float(shift), int(diis_space), C.byref(self.ptr)))
+        _err(init(C.byref(d), calc_type.encode(), _p(fa), _p(fb), _p(vaa), _p(vab), _p(vbb),
+                  int(bool(rhf)), float(shift), int(diis_space), C.byref(self.ptr)))
         self._keep = None
         ts, vs = I64(), I64()
         _err(lib.ccq_b200_sizes(self.ptr, C.byref(ts), C.byref(vs)))

@@ -253,8 +253,193 @@ def tlayout(s):
     return I.TLayout(s['dims'])
 
 
+T1_T3 = ('T1A', 'T1B', 'T3A', 'T3B', 'T3C', 'T3D')
+
+
+def bracket(train_lams, lam, exclude=None):
+    """Linear interpolation in lambda between solved family members: [(index, weight), ...].
+
+    The nearest member below lam and the nearest above (``exclude`` left out);
+    at an end of the family the two nearest on the one side (linear
+    extrapolation); a single member when only one is left."""
+    idx = [k for k in range(len(train_lams)) if k != exclude]
+    lo = [k for k in idx if train_lams[k] <= lam]
+    hi = [k for k in idx if train_lams[k] > lam]
+    lo = sorted(lo, key=lambda k: (lam - train_lams[k], k))
+    hi = sorted(hi, key=lambda k: (train_lams[k] - lam, k))
+    if lo and hi:
+        a, b = lo[0], hi[0]
+    elif len(lo) >= 2:
+        a, b = lo[0], lo[1]
+    elif len(hi) >= 2:
+        a, b = hi[0], hi[1]
+    else:
+        return [((lo or hi)[0], 1.0)]
+    la, lb = train_lams[a], train_lams[b]
+    wb = (lam - la) / (lb - la)
+    return [(a, 1.0 - wb), (b, wb)]
+
+
+def start_transfer(s, lam, layout, anchor, t_anchor):
+    """No network: T2 = mp2 (1 + the anchor's converged ratio), T1 and T3 copied from the anchor."""
+    t = np.array(t_anchor, dtype=np.float64)
+    for name, X, mp2, shape in system_blocks(s, lam):
+        layout.view(t, name)[...] = (mp2 * (1.0 + anchor[1][name].reshape(-1))).reshape(shape)
+    return t
+
+
+def start_interp(s, lam, layout, members):
+    """No network: members = [(weight, anchor, t_vec)] of ``bracket``; every amplitude (T1, T2, T3)
+    interpolated linearly in lambda between the two members."""
+    t = np.zeros(layout.t_size)
+    for w, anc, tv in members:
+        t += w * np.asarray(tv)
+    return t
+
+
+# ---------------------------------------------------------------------------
+# Two-anchor start with learned corrections to T2 and T3.
+#
+# The base is a linear interpolation in lambda between the two solved members
+# that bracket the target (``bracket``), for every amplitude.  Two networks
+# then correct it element by element,
+#     T2 = t2_int (1 + net2(x)),   T3 = t3_int (1 + net3(x)),
+# with features symmetric under the amplitudes' antisymmetry, so the start
+# keeps every antisymmetry of the stored blocks.  The interpolation's error is
+# mostly its second-order term, w_lo w_hi (lambda_hi - lambda_lo)^2 t''/2,
+# so the features carry that weight, lambda and the two members' relative
+# difference; the networks learn the curvature from the solved members.
+# Without the networks (zero corrections) this is the ``interp`` start.
+# ---------------------------------------------------------------------------
+T2_BLOCKS = ('T2A', 'T2B', 'T2C')
+T3_BLOCKS = ('T3A', 'T3B', 'T3C', 'T3D')
+
+
+def _orbital_axes(s, shape_names):
+    """Orbital energies along each axis of a stored block (names like 'oa', 'vb')."""
+    d = s['dims']
+    fr = d.froz
+    fa = np.diag(s['f_a'])[fr:]
+    fb = np.diag(s['f_b'])[fr:]
+    ax = {'oa': fa[:d.oa], 'ob': fb[:d.ob], 'va': fa[d.oa:], 'vb': fb[d.ob:]}
+    return [ax[n] for n in shape_names]
+
+
+def _sum_axes(vecs, shape, first=0):
+    """sum_k vecs[k] broadcast along axis first + k of an array of the given shape."""
+    out = np.zeros(shape)
+    for k, v in enumerate(vecs):
+        out = out + v.reshape([-1 if j == first + k else 1 for j in range(len(shape))])
+    return out
+
+
+def _curvature_weight(members):
+    """w_lo w_hi (lambda_hi - lambda_lo)^2: the factor of the interpolation's second-order error."""
+    if len(members) < 2:
+        return 0.0
+    (w1, l1), (w2, l2) = [(m[0], m[3]) for m in members[:2]]
+    return float(w1 * w2 * (l2 - l1) ** 2)
+
+
+def interp_features(s, lam, members, layout, blocks, rng=None, per_block=None, cut=1e-3):
+    """[(name, X [n, 8], base [n], sel, shape)] for the given blocks: base = the interpolated
+    amplitudes (members = [(weight, anchor, t_vec, lambda)]) on the elements sel (|base| above
+    cut * max |base|; with rng, per_block of them drawn with probability proportional to base^2, so
+    that an unweighted mean-squared loss on the ratio weighs each element by its amplitude squared,
+    the way the amplitudes enter the iteration's error).
+
+    Features: gap, occupied and virtual energy sums, log |base|, lambda, the two members' relative
+    difference (t_hi - t_lo) / base, the weight of the upper member and the curvature weight."""
+    out = []
+    hw = _curvature_weight(members)
+    for name in blocks:
+        shape = layout.shape[name]
+        if not np.prod(shape):
+            continue
+        base = sum(w * np.asarray(layout.view(tv, name)).reshape(-1) for w, anc, tv, la in members)
+        amax = np.abs(base).max()
+        if amax == 0.0:
+            continue
+        sel = np.nonzero(np.abs(base) > cut * amax)[0]
+        if rng is not None and per_block:
+            w = base[sel] ** 2
+            sel = np.sort(rng.choice(sel, per_block, replace=True, p=w / w.sum()))
+        names = I.BLOCK_SHAPES[name]
+        h = len(names) // 2
+        ax = _orbital_axes(s, names)
+        eo = _sum_axes(ax[:h], shape).reshape(-1)[sel]
+        ev = _sum_axes(ax[h:], shape, h).reshape(-1)[sel]
+        b = base[sel]
+        if len(members) >= 2:
+            lo, hi = sorted(members[:2], key=lambda m: m[3])
+            d = (np.asarray(layout.view(hi[2], name)).reshape(-1)[sel] -
+                 np.asarray(layout.view(lo[2], name)).reshape(-1)[sel]) / b
+            whi = hi[0]
+        else:
+            d = np.zeros_like(b)
+            whi = 1.0
+        X = np.stack([ev - eo, eo, ev, np.log(np.abs(b)), np.full(b.shape, lam), np.clip(d, -4.0, 4.0),
+                      np.full(b.shape, whi), np.full(b.shape, hw)], axis=-1)
+        out.append((name, X, b, sel, shape))
+    return out
+
+
+def interp_start(s, lam, layout, members):
+    """The base of the two-anchor start (T1, T2, T3 interpolated), no network."""
+    return start_interp(s, lam, layout, [(w, anc, tv) for w, anc, tv, la in members])
+
+
+class TwoAnchorWarmStart:
+    """net2 (T2) and net3 (T3) over the interpolated start; trained and evaluated by the library's
+    kernels (``ccq_b200_mlp_*``)."""
+
+    def __init__(self, seed=0):
+        self.net2 = WarmStart(seed=seed)
+        self.net3 = WarmStart(seed=seed + 1)
+
+    @staticmethod
+    def samples(items, layout_of, per_block=20000, seed=0, cut=1e-3):
+        """items = [(spec, t_vec (converged), members)]: (X2, y2, X3, y3) with targets t / base - 1
+        clipped to [-0.5, 0.5], per_block elements per block and member drawn as in interp_features."""
+        rng = np.random.default_rng(seed)
+        xs = {2: [], 3: []}
+        ys = {2: [], 3: []}
+        for spec, tvec, members in items:
+            s = synth.system(spec)
+            lay = layout_of(s)
+            for lvl, blocks in ((2, T2_BLOCKS), (3, T3_BLOCKS)):
+                for name, X, b, sel, shape in interp_features(s, spec.lam, members, lay, blocks, rng, per_block,
+                                                              cut):
+                    t = np.asarray(lay.view(tvec, name)).reshape(-1)[sel]
+                    xs[lvl].append(X)
+                    ys[lvl].append(np.clip(t / b - 1.0, -0.5, 0.5))
+        cat = lambda v, w: np.concatenate(v) if v else np.zeros(w)  # noqa: E731
+        return cat(xs[2], (0, NFEAT)), cat(ys[2], 0), cat(xs[3], (0, NFEAT)), cat(ys[3], 0)
+
+    def train(self, X2, y2, X3, y3, epochs=600, log=None):
+        h2 = h3 = []
+        if X2.shape[0]:
+            self.net2.fit_scaling(X2, y2)
+            h2 = self.net2.train(X2, y2, epochs=epochs, log=log)
+        if X3.shape[0]:
+            self.net3.fit_scaling(X3, y3)
+            h3 = self.net3.train(X3, y3, epochs=epochs, log=log)
+        return h2, h3
+
+    def initial_t(self, s, lam, layout, members, use_t2=True, use_t3=True):
+        """The interpolated t_vec with the networks' corrections on T2 (use_t2) and T3 (use_t3)."""
+        t = interp_start(s, lam, layout, members)
+        for use, net, blocks in ((use_t2, self.net2, T2_BLOCKS), (use_t3, self.net3, T3_BLOCKS)):
+            if not use:
+                continue
+            for name, X, b, sel, shape in interp_features(s, lam, members, layout, blocks):
+                v = layout.view(t, name).reshape(-1)
+                v[sel] = b * (1.0 + np.clip(net.predict_ratio(X), -0.5, 0.5))
+        return t
+
+
 def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1e-8, epochs=600, seed=C4_SEED,
-          log=None):
+          log=None, ablation=True, chunk=50):
     """Plain solves of the whole family, training on ``train`` of them, warm-started
     solves of the rest; iterations to tol and |dE| between the two starts."""
     import time
@@ -262,7 +447,7 @@ def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1
     specs = [synth.SynthSpec(norb, nel, 2 * norb, 0.03, seed, float(l)) for l in np.linspace(0.5, 2.0, count)]
     tr, ev = c4_split(count, train, seed)
     t0 = time.perf_counter()
-    plain, _ = batch.solve_batch(specs, tol=tol, calc_type=method, keep_t=True)
+    plain, _ = batch.solve_batch(specs, tol=tol, calc_type=method, keep_t=True, chunk=chunk)
     t1 = time.perf_counter()
     anchors = {i: anchor_of(specs[i], plain[i]['t']) for i in tr}
 
@@ -288,16 +473,57 @@ def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1
         a = nearest(i, False)
         inits.append(ws.initial_t(s, specs[i].lam, lay, anchors[a], plain[a]['t']))
         mp2s.append(mp2_t(s, lay))
-    warm, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=inits)
+    warm, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=inits, chunk=chunk)
     t3 = time.perf_counter()
-    mp2r, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=mp2s)
+    mp2r, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=mp2s, chunk=chunk)
+    legs = {}
+    if ablation:
+        # the same anchors without the network: the nearest member's converged amplitudes as they are,
+        # its T2/MP2 ratio transferred, and a linear interpolation in lambda between two members
+        tl = [specs[j].lam for j in tr]
+        starts = {'anchor': [], 'transfer': [], 'interp': []}
+        for i in ev:
+            s = synth.system(specs[i])
+            lay = tlayout(s)
+            a = nearest(i, False)
+            starts['anchor'].append(np.array(plain[a]['t']))
+            starts['transfer'].append(start_transfer(s, specs[i].lam, lay, anchors[a], plain[a]['t']))
+            mem = [(w, anchors[tr[k]], plain[tr[k]]['t']) for k, w in bracket(tl, specs[i].lam)]
+            starts['interp'].append(start_interp(s, specs[i].lam, lay, mem))
+        # the two-anchor start with its networks (T2 and T3 corrections over the interpolation)
+        tw = time.perf_counter()
+        items = []
+        for k, i in enumerate(tr):
+            mem = [(w, anchors[tr[j]], plain[tr[j]]['t'], specs[tr[j]].lam) for j, w in bracket(tl, specs[i].lam, k)]
+            items.append((specs[i], plain[i]['t'], mem))
+        two = TwoAnchorWarmStart(seed=seed)
+        X2, Y2, X3, Y3 = two.samples(items, tlayout, seed=seed)
+        h2, h3 = two.train(X2, Y2, X3, Y3, epochs=epochs)
+        starts['two_anchor_net_t2'] = []
+        starts['two_anchor_net'] = []
+        for i in ev:
+            s = synth.system(specs[i])
+            lay = tlayout(s)
+            mem = [(w, anchors[tr[k]], plain[tr[k]]['t'], specs[tr[k]].lam) for k, w in bracket(tl, specs[i].lam)]
+            starts['two_anchor_net_t2'].append(two.initial_t(s, specs[i].lam, lay, mem, use_t3=False))
+            starts['two_anchor_net'].append(two.initial_t(s, specs[i].lam, lay, mem))
+        legs['two_anchor_training'] = {'t2_samples': int(X2.shape[0]), 't3_samples': int(X3.shape[0]),
+                                       'loss_t2': [h2[0][1], h2[-1][1]] if h2 else None,
+                                       'loss_t3': [h3[0][1], h3[-1][1]] if h3 else None,
+                                       'seconds': time.perf_counter() - tw}
+        for name, st in starts.items():
+            rr, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=st, chunk=chunk)
+            it_ = np.array([r['iterations'] for r in rr], dtype=float)
+            legs[name] = {'iterations_mean': float(it_.mean()),
+                          'max_dE': float(max(abs(plain[i]['e_cor'] - r['e_cor']) for i, r in zip(ev, rr))),
+                          'failed': int(sum(r['failed'] for r in rr))}
     pi = np.array([plain[i]['iterations'] for i in ev], dtype=float)
     wi = np.array([r['iterations'] for r in warm], dtype=float)
     mi = np.array([r['iterations'] for r in mp2r], dtype=float)
     de = max(abs(plain[i]['e_cor'] - r['e_cor']) for i, r in zip(ev, warm))
     return {'method': method, 'norb': norb, 'nel': nel, 'family': count, 'train': len(tr), 'eval': len(ev),
             'tol': tol, 'plain_iterations_mean': float(pi.mean()), 'warm_iterations_mean': float(wi.mean()),
-            'mp2_start_iterations_mean': float(mi.mean()),
+            'mp2_start_iterations_mean': float(mi.mean()), 'no_network': legs,
             'iteration_reduction': float(1.0 - wi.sum() / pi.sum()), 'max_dE': float(de),
             'failed': int(sum(r['failed'] for r in warm) + sum(plain[i]['failed'] for i in ev)),
             'train_samples': int(X.shape[0]), 'loss_history': hist,

@@ -117,6 +117,19 @@ int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type,
                   int64_t rhf, double shift, int64_t diis_space,
                   ccq_b200_ctx **out);
 
+/* ccq_b200_init for hosts that hold the integrals row-major (C order:
+ * f[p][q] over orbs x orbs, v[p][q][r][s] over the active range), such as
+ * numpy or C++ arrays.  No counterpart in the reference, whose arrays are
+ * Fortran-ordered; it spares such a host two transposed copies of every
+ * (orbs-froz)^4 block (one on the host to reach Fortran order, one on the
+ * device back to the engine's row-major layout).  Same semantics, sizes and
+ * error codes as ccq_b200_init otherwise. */
+int ccq_b200_init_rowmajor(const ccq_b200_dims *dims, const char *calc_type,
+                           const double *f_a, const double *f_b,
+                           const double *v_aa, const double *v_ab, const double *v_bb,
+                           int64_t rhf, double shift, int64_t diis_space,
+                           ccq_b200_ctx **out);
+
 /* Length of t_vec (get_t_sizes, cc_utils.f90:479-559) and of the DIIS
  * vector (solve_cc.f90:66-77). */
 int ccq_b200_sizes(const ccq_b200_ctx *ctx, int64_t *t_size, int64_t *vec_size);
