@@ -57,6 +57,7 @@ def parse():
     p.add_argument('--no-tune', action='store_true', help='keep the shape heuristics (no autotuning sweep)')
     p.add_argument('--no-crcc', action='store_true', help='skip the CR-CC(2,3) leg (32 orbitals)')
     p.add_argument('--no-batch', action='store_true', help='skip the batched CCSD leg (64 Hamiltonians)')
+    p.add_argument('--no-ccsdt', action='store_true', help='skip the active-space CCSDt leg (40 orbitals)')
     p.add_argument('--no-warmstart', action='store_true',
                    help='skip the learned warm-start study (200 CCSDT Hamiltonians at 24 orbitals, about 40 s)')
     return p.parse_args()
@@ -381,6 +382,33 @@ def crcc_leg(cpu_sample=True):
                                f'({t_l:.2f} s) and the corrections ({t_t:.2f} s) with the numpy executor, scaled by '
                                f'the GPU run\'s iteration counts'}
     return out
+
+
+def ccsdt_active_leg(s, steps=10, warmup=3, act_occ=2, act_unocc=6):
+    """Active-space CCSDt on the 40-orbital CCSDT workload (act_occ = 2, act_unocc = 6: ccq's
+    act_occ_b = occ_b - 2, act_unocc_a = occ_a + 6): the T3 residual contractions run over the active
+    triples only.  FP64, graph replay, CUDA events per iteration (median)."""
+    from ccq_b200 import lib
+    d = s['dims']
+    act = (d.occ_b - act_occ, d.occ_a + act_unocc)
+    ctx = lib.Context(d.froz, d.occ_a, d.occ_b, d.orbs, 'CCSDt', s['f_a'], s['f_b'], s['v_aa'], s['v_ab'],
+                      s['v_bb'], active=act)
+    ctx.use_graph(True)
+    it = 1
+    for _ in range(warmup):
+        ctx.iterate(it)
+        it += 1
+    ms = []
+    for _ in range(steps):
+        ctx.iterate(it)
+        ms.append(ctx.timing()[1])
+        it += 1
+    st = ctx.stats()
+    ctx.close()
+    return {'workload': f'CCSDt, 40 spatial orbitals, act_occ={act_occ}, act_unocc={act_unocc} '
+                        f'(act_occ_b={act[0]}, act_unocc_a={act[1]}), FP64',
+            's_per_iter': float(np.median(ms)) / 1e3, 'flops_per_iter': st['flops'],
+            'launches_per_iter': st['launches'], 'iterations_timed': steps}
 
 
 def batch_leg(rank, world):
@@ -712,6 +740,16 @@ def main():
 
     batched = None if args.no_batch else batch_leg(rank, world)
 
+    ccsdt_act = None
+    if rank == 0 and not args.no_ccsdt:
+        try:
+            ccsdt_act = ccsdt_active_leg(s)
+            ccsdt_act['ccsdt_fp64_s_per_iter'] = results['fp64']['s_per_iter']
+            ccsdt_act['speedup_vs_ccsdt_fp64'] = results['fp64']['s_per_iter'] / ccsdt_act['s_per_iter']
+            ccsdt_act['flops_fraction_of_ccsdt'] = ccsdt_act['flops_per_iter'] / results['fp64']['flops_per_iter']
+        except Exception as ex:  # noqa: BLE001
+            ccsdt_act = {'error': f'{type(ex).__name__}: {str(ex)[:200]}'}
+
     warm = None
     if rank == 0 and not args.no_warmstart:
         try:
@@ -758,6 +796,7 @@ def main():
                     'd2h_bytes_per_step': bytes_t + 16},
             'gpu_launches': head['launches_per_iter'] * args.steps,
             'clocks': clk, 'convergence': conv, 'crcc23': crcc, 'batched_ccsd': batched, 'warm_start': warm,
+            'ccsdt_active': ccsdt_act,
             'peaks': {'live': peaks_live, 'file': peaks_file, 'file_kind': peaks_kind},
         }
         print(json.dumps(line), flush=True)

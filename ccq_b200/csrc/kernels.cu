@@ -934,7 +934,8 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
     const long long step = (long long)gridDim.x * blockDim.x * ASM_EPT;
     for (long long base = (long long)blockIdx.x * blockDim.x * ASM_EPT; base < a.total; base += step) {
         int x[ASM_EPT][RK];
-        bool act[ASM_EPT];
+        bool act[ASM_EPT];    // an element of the block
+        bool need[ASM_EPT];   // ... whose residual is gathered (inside the active space when one is set)
         double R[ASM_EPT];
 #pragma unroll
         for (int e = 0; e < ASM_EPT; ++e) {
@@ -944,6 +945,19 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
 #pragma unroll
             for (int d = 0; d < RK; ++d) x[e][d] = 0;
             if (act[e]) canonical_element<RK, Off>(a, (Off)lin, x[e]);
+            need[e] = act[e];
+            if (a.act && act[e]) {
+                // CCSDt: at least one active occupied and one active virtual index
+                bool occ = false, vir = false;
+#pragma unroll
+                for (int d = 0; d < RK; ++d) {
+                    if (d < RK / 2)
+                        occ = occ || x[e][d] >= a.act_occ_lo;
+                    else
+                        vir = vir || x[e][d] < a.act_vir_hi[a.spin[d]];
+                }
+                need[e] = occ && vir;
+            }
         }
         for (int c = 0; c < nch; ++c) {
             __syncthreads();
@@ -990,7 +1004,7 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
                     Off off = 0;
 #pragma unroll
                     for (int d = 0; d < RK; ++d) off += (Off)q.tst[d] * x[e][d];
-                    v[e] = act[e] ? __ldg(p + off) : 0.0;
+                    v[e] = need[e] ? __ldg(p + off) : 0.0;
                 }
 #pragma unroll
                 for (int e = 0; e < ASM_EPT; ++e) R[e] += q.coef * v[e];
@@ -1002,7 +1016,7 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
                 {
 #pragma unroll
                     for (int e = 0; e < ASM_EPT; ++e) {
-                        if (!act[e]) continue;
+                        if (!need[e]) continue;
                         double sg = q.coef;
                         int y[RK];
 #pragma unroll
@@ -1053,17 +1067,8 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
                         D += a.fdiag[a.spin[d]][a.nocc[a.spin[d]] + x[e][d]];
                 }
                 tnew = a.T[toff] - R[e] / D;
-                if (a.act) {
-                    bool occ = false, vir = false;
-#pragma unroll
-                    for (int d = 0; d < RK; ++d) {
-                        if (d < RK / 2)
-                            occ = occ || x[e][d] >= a.act_occ_lo;
-                        else
-                            vir = vir || x[e][d] < a.act_vir_hi[a.spin[d]];
-                    }
-                    if (!(occ && vir)) tnew = 0.0;
-                }
+                // triples outside the active space stay zero
+                if (!need[e]) tnew = 0.0;
             } else {
                 tnew = R[e];
             }

@@ -99,6 +99,9 @@ struct Op {
     ViewSpec c, a, b;
     std::string tag;
     std::vector<std::vector<std::string>> restrict_groups;   // R= annotation
+    // labels whose range starts above their view's own start (sub-ranges of an active-space
+    // restriction): the offset, so that restriction groups compare the labels' full-range values
+    std::map<std::string, long long> lshift;
     // ASSEMBLE
     std::string block, mode;
     std::vector<std::pair<double, ViewSpec>> terms;
@@ -298,6 +301,7 @@ struct ccq_b200_ctx {
     int use_graph = 0;
     cudaGraphExec_t gexec = nullptr;
     int device = 0;
+    long long act_occ_b = -1, act_unocc_a = -1;   // CCSDt: the active space the plan was restricted to
     SplitWorkspace split{};
     // host round trip of ccq_b200_iterate_host: each t_vec block is copied to host_out as soon as its
     // last write of the sweep is done (copy stream cstream, joined into the sweep's stream at its end)
@@ -382,7 +386,7 @@ bool has(const Resolved &r, const std::string &l) { return r.stride.count(l) > 0
 // Restricted groups (label lists) are enumerated for increasing values only.
 void build_table(const std::vector<std::string> &labels, const std::map<std::string, long long> &extent,
                  const Resolved &x, const Resolved *y, const std::vector<std::vector<std::string>> &groups,
-                 std::vector<int> &tx, std::vector<int> &ty) {
+                 const std::map<std::string, long long> &shift, std::vector<int> &tx, std::vector<int> &ty) {
     tx.clear();
     ty.clear();
     std::vector<std::vector<int>> gidx;   // positions in `labels` of each group's members, in group order
@@ -395,9 +399,11 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
         if (pos.size() == g.size()) gidx.push_back(pos);
     }
     const size_t nd = labels.size();
-    std::vector<long long> idx(nd, 0), ev(nd), sx(nd), sy(nd, 0);
+    std::vector<long long> idx(nd, 0), ev(nd), sx(nd), sy(nd, 0), sh(nd, 0);
     long long total = 1;
     for (size_t d = 0; d < nd; ++d) {
+        auto it = shift.find(labels[d]);
+        if (it != shift.end()) sh[d] = it->second;
         ev[d] = extent.at(labels[d]);
         sx[d] = x.stride.at(labels[d]);
         if (y) sy[d] = y->stride.at(labels[d]);
@@ -411,7 +417,7 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
         bool ok = true;
         for (auto &g : gidx)
             for (size_t q = 1; q < g.size(); ++q)
-                if (idx[g[q]] <= idx[g[q - 1]]) ok = false;
+                if (idx[g[q]] + sh[g[q]] <= idx[g[q - 1]] + sh[g[q - 1]]) ok = false;
         if (ok) {
             long long ox = 0, oy = 0;
             for (size_t d = 0; d < nd; ++d) {
@@ -430,6 +436,145 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
             }
             idx[d] = 0;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Active-space CCSDt at its own cost.  ccq's CCSDt keeps only the triples with
+// at least one active occupied and one active virtual index (spatial orbitals
+// above act_occ_b, up to act_unocc_a; src/parser.f90:495-499,
+// src/utils/cc_utils.f90:560-630).  The residual terms of a T3 block (the Z
+// buffers its Jacobi assemble reads) are then needed only on the elements whose
+// occupied labels hold an active index and whose virtual labels hold one: a set
+// that every permutation of the labels keeps, so the assemble's permuted and
+// sorted reads of an active triple stay inside it.  Each GETT that writes such a
+// Z is replaced by GETTs over a disjoint cover of that set by rectangles (on
+// each side: the first k-1 labels inactive, the k-th active, the rest free),
+// whose views take the labels' sub-ranges.  Labels of a restriction group keep
+// their order by comparing full-range values (Op::lshift).
+// ---------------------------------------------------------------------------
+struct ActiveSpace {
+    long long occ_lo = 0;          // occupied index (from froz) >= occ_lo is active, both spins
+    long long vir_hi[2] = {0, 0};  // virtual index (from occ of the spin) < vir_hi[spin] is active
+};
+
+std::string num_token(ccq_b200_ctx *c, long long v) {
+    std::string t = "#" + std::to_string(v);
+    c->size[t] = v;
+    return t;
+}
+
+void restrict_to_active(ccq_b200_ctx *c, const ActiveSpace &as) {
+    std::map<std::string, int> t3z;   // Z buffer -> 1 if read only by T3 Jacobi assembles
+    for (auto &o : c->plan.ops)
+        if (o.kind == OP_ASM && o.block.size() == 3 && o.block[1] == '3' && o.mode == "jacobi")
+            for (auto &t : o.terms)
+                if (t.second.buf[0] == 'Z') t3z[t.second.buf] = 1;
+    for (auto &o : c->plan.ops) {
+        if (o.kind == OP_GETT) {
+            t3z.erase(o.a.buf);
+            t3z.erase(o.b.buf);
+        }
+        if (o.kind == OP_ASM && !(o.block.size() == 3 && o.block[1] == '3' && o.mode == "jacobi"))
+            for (auto &t : o.terms) t3z.erase(t.second.buf);
+    }
+    const long long full_o[2] = {c->oa, c->ob}, full_v[2] = {c->va, c->vb};
+    struct Lab {
+        std::string name;
+        int spin;
+        bool occ;
+    };
+    // (label, start, extent) assignments of one side's rectangles
+    using Rect = std::vector<std::pair<std::string, std::pair<long long, long long>>>;
+    auto side_rects = [&](std::vector<Lab> labs, const std::vector<std::vector<std::string>> &groups, bool occ) {
+        // a restriction group (increasing values) contributes its largest occupied / smallest virtual
+        // label first: once that one is inactive, so are the others
+        auto rank = [&](const std::string &l) {
+            for (auto &g : groups)
+                for (size_t q = 0; q < g.size(); ++q)
+                    if (g[q] == l) return occ ? -(long long)q : (long long)q;
+            return 0LL;
+        };
+        std::stable_sort(labs.begin(), labs.end(), [&](const Lab &a, const Lab &b) { return rank(a.name) < rank(b.name); });
+        std::vector<Rect> out;
+        for (size_t k = 0; k < labs.size(); ++k) {
+            Rect r;
+            bool empty = false;
+            for (size_t j = 0; j <= k; ++j) {
+                const Lab &l = labs[j];
+                long long n = occ ? full_o[l.spin] : full_v[l.spin];
+                long long cut = occ ? std::min(std::max(as.occ_lo, 0LL), n)
+                                    : std::min(std::max(as.vir_hi[l.spin], 0LL), n);
+                // occupied: inactive [0, cut), active [cut, n); virtual: active [0, cut), inactive [cut, n)
+                bool active = j == k;
+                long long lo = occ ? (active ? cut : 0) : (active ? 0 : cut);
+                long long hi = occ ? (active ? n : cut) : (active ? cut : n);
+                if (hi <= lo) empty = true;
+                r.push_back({l.name, {lo, hi - lo}});
+            }
+            if (!empty) out.push_back(r);
+        }
+        return out;
+    };
+    std::vector<Op> ops;
+    for (auto &o : c->plan.ops) {
+        if (o.kind != OP_GETT || !t3z.count(o.c.buf)) {
+            ops.push_back(o);
+            continue;
+        }
+        std::vector<Lab> occ, vir;
+        bool ok = true;
+        for (auto &ax : o.c.axes) {
+            const std::string &z = ax.size;
+            if (z == "oa" || z == "ob") occ.push_back({ax.label, z == "ob", true});
+            else if (z == "va" || z == "vb") vir.push_back({ax.label, z == "vb", false});
+            else ok = false;
+        }
+        if (!ok || occ.empty() || vir.empty()) {
+            ops.push_back(o);
+            continue;
+        }
+        auto ro = side_rects(occ, o.restrict_groups, true), rv = side_rects(vir, o.restrict_groups, false);
+        for (auto &a : ro)
+            for (auto &b : rv) {
+                Op q = o;
+                Rect r = a;
+                r.insert(r.end(), b.begin(), b.end());
+                for (auto &lr : r) {
+                    const long long lo = lr.second.first, ext = lr.second.second;
+                    for (ViewSpec *v : {&q.c, &q.a, &q.b})
+                        for (auto &ax : v->axes)
+                            if (ax.label == lr.first) {
+                                ax.start = num_token(c, tok(c, ax.start) + lo);
+                                ax.size = num_token(c, ext);
+                            }
+                    if (lo) q.lshift[lr.first] = lo;
+                }
+                ops.push_back(q);
+            }
+    }
+    c->plan.ops = ops;
+}
+
+// The T3 Jacobi assembles hold the triples outside the active space at zero (and gather only the
+// active ones); CR-CC(2,3) contexts (CC(t;3)) skip the active triples in the correction instead.
+void apply_active_masks(ccq_b200_ctx *c, long long act_occ_b, long long act_unocc_a) {
+    const long long occ_a = c->froz + c->oa, occ_b = c->froz + c->ob;
+    for (auto &o : c->plan.ops) {
+        if (o.kind == OP_CRCC) {
+            // CC(t;3): the correction covers the triples outside the active space
+            o.crcc.act_occ_lo = (int)(act_occ_b - c->froz);
+            o.crcc.act_vir_hi = (int)(act_unocc_a - c->froz);
+            continue;
+        }
+        if (o.kind != OP_ASM || o.block[1] != '3' || o.asmargs.mode != 0) continue;
+        AsmArgs &a = o.asmargs;
+        // spatial orbitals above act_occ_b (occupied) and up to act_unocc_a (virtual) are active,
+        // for both spins; indices here count from froz (occupied) and from occ (virtual)
+        a.act = 1;
+        a.act_occ_lo = (int)(act_occ_b - c->froz);
+        a.act_vir_hi[0] = (int)(act_unocc_a - occ_a);
+        a.act_vir_hi[1] = (int)(act_unocc_a - occ_b);
     }
 }
 
@@ -710,12 +855,13 @@ void instantiate(ccq_b200_ctx *c) {
                     throw Error(CCQ_B200_EPLAN, "restriction group spans index modes");
                 }
                 for (auto &l : g)
-                    if (ext[l] != ext[g[0]]) throw Error(CCQ_B200_EPLAN, "restriction group with unequal extents");
+                    if (ext[l] != ext[g[0]] && o.lshift.empty())
+                        throw Error(CCQ_B200_EPLAN, "restriction group with unequal extents");
             }
             std::vector<int> am, ak, bn, bk, cm, cn;
-            build_table(ml, ext, A, &C, o.restrict_groups, am, cm);
-            build_table(kl, ext, A, &B, o.restrict_groups, ak, bk);
-            build_table(nl, ext, B, &C, o.restrict_groups, bn, cn);
+            build_table(ml, ext, A, &C, o.restrict_groups, o.lshift, am, cm);
+            build_table(kl, ext, A, &B, o.restrict_groups, o.lshift, ak, bk);
+            build_table(nl, ext, B, &C, o.restrict_groups, o.lshift, bn, cn);
             o.hcm = cm;
             o.hcn = cn;
             if (ml.empty()) { am.assign(1, 0); cm.assign(1, 0); }
@@ -1418,23 +1564,33 @@ int ccq_b200_last_error(char *buf, int64_t len) {
 
 static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
                      const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
-                     int64_t diis_space, ccq_b200_ctx **out, bool rowmajor);
+                     int64_t diis_space, ccq_b200_ctx **out, bool rowmajor, int64_t act_occ_b,
+                     int64_t act_unocc_a);
 
 int ccq_b200_init(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
                   const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
                   int64_t diis_space, ccq_b200_ctx **out) {
-    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, false);
+    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, false, -1, -1);
 }
 
 int ccq_b200_init_rowmajor(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
                            const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
                            int64_t diis_space, ccq_b200_ctx **out) {
-    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, true);
+    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, true, -1, -1);
+}
+
+int ccq_b200_init_ex(const ccq_b200_dims *dims, const char *calc_type, const ccq_b200_init_opts *opts,
+                     const double *f_a, const double *f_b, const double *v_aa, const double *v_ab,
+                     const double *v_bb, int64_t rhf, double shift, int64_t diis_space, ccq_b200_ctx **out) {
+    if (!opts) return fail(Error(CCQ_B200_EINVAL, "null options"));
+    return init_impl(dims, calc_type, f_a, f_b, v_aa, v_ab, v_bb, rhf, shift, diis_space, out, opts->rowmajor != 0,
+                     opts->act_occ_b, opts->act_unocc_a);
 }
 
 static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const double *f_a, const double *f_b,
                      const double *v_aa, const double *v_ab, const double *v_bb, int64_t rhf, double shift,
-                     int64_t diis_space, ccq_b200_ctx **out, bool rowmajor) {
+                     int64_t diis_space, ccq_b200_ctx **out, bool rowmajor, int64_t act_occ_b,
+                     int64_t act_unocc_a) {
     ccq_b200_ctx *c = nullptr;
     try {
         if (!dims || !calc_type || !f_a || !f_b || !v_aa || !v_ab || !v_bb || !out)
@@ -1446,14 +1602,26 @@ static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const dou
         if (fr < 0 || oa < 1 || ob < 1 || va < 1 || vb < 1)
             throw Error(CCQ_B200_EINVAL, "invalid dimensions (need at least one occupied and virtual per spin)");
         std::string ct(calc_type);
+        // CCSDt: the CCSDT plan restricted to ccq's active space (src/parser.f90:380-388)
+        const bool active = ct == "CCSDt";
+        if (active) {
+            if (act_occ_b < fr || act_occ_b > dims->occ_b || act_unocc_a < dims->occ_a || act_unocc_a > dims->orbs)
+                throw Error(CCQ_B200_EINVAL, "CCSDt: froz <= act_occ_b <= occ_b and occ_a <= act_unocc_a <= orbs");
+            ct = "CCSDT";
+        } else if (act_occ_b >= 0 || act_unocc_a >= 0) {
+            throw Error(CCQ_B200_EINVAL, "an active space is given only with calc_type CCSDt");
+        }
         if (ct != "CCSD" && ct != "CCSDT" && ct != "CCSDTQ" && ct != "CR-CC(2,3)")
-            throw Error(CCQ_B200_EINVAL, "calc_type must be CCSD, CCSDT, CCSDTQ or CR-CC(2,3)");
+            throw Error(CCQ_B200_EINVAL, "calc_type must be CCSD, CCSDT, CCSDt, CCSDTQ or CR-CC(2,3)");
         if (rhf && oa != ob) throw Error(CCQ_B200_EINVAL, "rhf requires occ_a == occ_b");
         const char *text = find_plan(ct, rhf != 0);
         if (!text) throw Error(CCQ_B200_EPLAN, "no plan for " + ct);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(CCQ_B200_ENODEV, "no CUDA device");
         c = new ccq_b200_ctx();
+        // CCQ_B200_TRACE_INIT=1: stage times of context creation on stderr
+        c->trace_init = getenv("CCQ_B200_TRACE_INIT") != nullptr;
+        c->t_init0 = std::chrono::steady_clock::now();
         CK(cudaGetDevice(&c->device));
         CK(gett_f64_prepare());
         CK(preload_kernels((int)diis_space));
@@ -1473,11 +1641,18 @@ static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const dou
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
         CK(cudaEventCreate(&c->ev2));
-        // CCQ_B200_TRACE_INIT=1: stage times of context creation on stderr
-        c->trace_init = getenv("CCQ_B200_TRACE_INIT") != nullptr;
-        c->t_init0 = std::chrono::steady_clock::now();
         auto stamp = [&](const char *what) { trace_stamp(c, what); };
+        stamp("stream/events");
         c->plan = parse_plan(text);
+        if (active) {
+            ActiveSpace as;
+            as.occ_lo = act_occ_b - fr;
+            as.vir_hi[0] = act_unocc_a - dims->occ_a;
+            as.vir_hi[1] = act_unocc_a - dims->occ_b;
+            restrict_to_active(c, as);
+            c->act_occ_b = act_occ_b;
+            c->act_unocc_a = act_unocc_a;
+        }
         stamp("parse");
         // host-side integral preparation
         long long orbs = dims->orbs;
@@ -1549,6 +1724,7 @@ static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const dou
         up4("VBB0", "VBB", v_bb);
         // this context's stream only: contexts created by other host threads keep running
         CK(cudaStreamSynchronize(c->stream));
+        if (active) apply_active_masks(c, act_occ_b, act_unocc_a);
         stamp("upload");
         *out = c;
         return 0;
@@ -2342,22 +2518,9 @@ int ccq_b200_set_active(ccq_b200_ctx *c, int64_t act_occ_b, int64_t act_unocc_a)
         const long long occ_a = c->froz + c->oa, occ_b = c->froz + c->ob, orbs = occ_a + c->va;
         if (act_occ_b < c->froz || act_occ_b > occ_b || act_unocc_a < occ_a || act_unocc_a > orbs)
             throw Error(CCQ_B200_EINVAL, "set_active: froz <= act_occ_b <= occ_b and occ_a <= act_unocc_a <= orbs");
-        for (auto &o : c->plan.ops) {
-            if (o.kind == OP_CRCC) {
-                // CC(t;3): the correction covers the triples outside the active space
-                o.crcc.act_occ_lo = (int)(act_occ_b - c->froz);
-                o.crcc.act_vir_hi = (int)(act_unocc_a - c->froz);
-                continue;
-            }
-            if (o.kind != OP_ASM || o.block[1] != '3' || o.asmargs.mode != 0) continue;
-            AsmArgs &a = o.asmargs;
-            // spatial orbitals above act_occ_b (occupied) and up to act_unocc_a (virtual) are active,
-            // for both spins; indices here count from froz (occupied) and from occ (virtual)
-            a.act = 1;
-            a.act_occ_lo = (int)(act_occ_b - c->froz);
-            a.act_vir_hi[0] = (int)(act_unocc_a - occ_a);
-            a.act_vir_hi[1] = (int)(act_unocc_a - occ_b);
-        }
+        if (c->act_occ_b >= 0 && (act_occ_b != c->act_occ_b || act_unocc_a != c->act_unocc_a))
+            throw Error(CCQ_B200_EINVAL, "set_active: a CCSDt context keeps the active space it was created with");
+        apply_active_masks(c, act_occ_b, act_unocc_a);
         // kernel arguments are recorded in the captured graphs
         drop_graphs(c);
         return 0;

@@ -249,13 +249,14 @@ def run(input_path, out=print, base_dir='.'):
     out(f"  Reference energy {sysd['e_ref']:.12f}")
     out('Coupled cluster')
     out('---------------')
-    # CCSDt (and the CCSDt part of CC(t;3)) runs the CCSDT plan with the triples held to the active space
+    # CCSDt (and the CCSDt part of CC(t;3)): the CCSDT plan restricted to the active triples
     active = cfg.calc_type in ('CCSDt', 'CC(t;3)')
 
     def context(ctype):
+        act = (cfg.act_occ_b, cfg.act_unocc_a) if ctype == 'CCSDt' else None
         return lib.Context(cfg.froz, cfg.occ_a, cfg.occ_b, cfg.orbs, ctype, sysd['f_a'], sysd['f_b'],
                            sysd['v_aa'], sysd['v_ab'], sysd['v_bb'], rhf=cfg.rhf, shift=cfg.shift,
-                           diis_space=cfg.diis_space)
+                           diis_space=cfg.diis_space, active=act)
     walkers = None
     if cfg.calc_type == 'CADFCIQMC':
         if cfg.ext_cor_file_h5:
@@ -264,9 +265,7 @@ def run(input_path, out=print, base_dir='.'):
         walkers = cfg.ext_cor_file if os.path.isabs(cfg.ext_cor_file) else os.path.join(base_dir, cfg.ext_cor_file)
         if not cfg.ext_cor_file or not os.path.exists(walkers):
             raise ValueError('CONFIGURATION ERROR: Walkers file not found')
-    ctx = context('CCSDT' if active else 'CCSDTQ' if walkers else cfg.calc_type)
-    if active:
-        ctx.set_active(cfg.act_occ_b, cfg.act_unocc_a)
+    ctx = context('CCSDt' if active else 'CCSDTQ' if walkers else cfg.calc_type)
     if walkers:
         load_walkers(ctx, cfg, walkers, out)
     if cfg.gpu_external_t:

@@ -33,6 +33,10 @@ class Dims(C.Structure):
     _fields_ = [('froz', I64), ('occ_a', I64), ('occ_b', I64), ('orbs', I64)]
 
 
+class InitOpts(C.Structure):
+    _fields_ = [('rowmajor', I64), ('act_occ_b', I64), ('act_unocc_a', I64)]
+
+
 SIGNATURES = {
     'ccq_b200_egemm': (C.c_int, [I64, I64, I64, DP, DP, DP]),
     'ccq_b200_egemm_split': (C.c_int, [I64, I64, I64, DP, DP, DP, I64]),
@@ -43,6 +47,11 @@ SIGNATURES = {
                                 C.POINTER(C.c_void_p)]),
     'ccq_b200_init_rowmajor': (C.c_int, [C.POINTER(Dims), C.c_char_p, DP, DP, DP, DP, DP, I64, C.c_double, I64,
                                 C.POINTER(C.c_void_p)]),
+    'ccq_b200_init_ex': (C.c_int, [C.POINTER(Dims), C.c_char_p, C.c_void_p, DP, DP, DP, DP, DP, I64, C.c_double,
+                                   I64, C.POINTER(C.c_void_p)]),
+    'ccq_b200_t_size_act': (I64, [C.POINTER(Dims), I64, I64]),
+    'ccq_b200_t_compress': (C.c_int, [C.POINTER(Dims), I64, I64, DP, I64, DP, I64]),
+    'ccq_b200_t_expand': (C.c_int, [C.POINTER(Dims), I64, I64, DP, I64, DP, I64]),
     'ccq_b200_sizes': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(I64)]),
     'ccq_b200_set_t': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_get_t': (C.c_int, [C.c_void_p, DP, I64]),
@@ -171,6 +180,32 @@ def checkpoint_info(path):
                 with_ring=bool(ring.value), state=st)
 
 
+def t_size_act(froz, occ_a, occ_b, orbs, act_occ_b, act_unocc_a):
+    """Length of ccq's compressed CCSDt T vector (get_t_sizes_act)."""
+    n = load().ccq_b200_t_size_act(C.byref(Dims(froz, occ_a, occ_b, orbs)), act_occ_b, act_unocc_a)
+    if n < 0:
+        _err(int(n))
+    return int(n)
+
+
+def t_compress(dims, act_occ_b, act_unocc_a, t_full):
+    """Full-block T vector -> ccq's compressed CCSDt T vector (dims = (froz, occ_a, occ_b, orbs))."""
+    d = Dims(*dims)
+    t = np.ascontiguousarray(t_full, dtype=np.float64)
+    out = np.empty(t_size_act(*dims, act_occ_b, act_unocc_a))
+    _err(load().ccq_b200_t_compress(C.byref(d), act_occ_b, act_unocc_a, _p(t), t.size, _p(out), out.size))
+    return out
+
+
+def t_expand(dims, act_occ_b, act_unocc_a, t_act, n_full):
+    """ccq's compressed CCSDt T vector -> full-block T vector of length n_full."""
+    d = Dims(*dims)
+    t = np.ascontiguousarray(t_act, dtype=np.float64)
+    out = np.empty(n_full)
+    _err(load().ccq_b200_t_expand(C.byref(d), act_occ_b, act_unocc_a, _p(t), t.size, _p(out), out.size))
+    return out
+
+
 def egemm(k1, k2, k3, A, B):
     """C(k2,k1) = B(k3,k2)^T A(k3,k1) on Fortran-ordered host arrays."""
     lib = load()
@@ -216,7 +251,8 @@ class Context:
     """A resident CC solve on the current CUDA device."""
 
     def __init__(self, froz, occ_a, occ_b, orbs, calc_type, f_a, f_b, v_aa, v_ab, v_bb,
-                 rhf=False, shift=0.0, diis_space=5):
+                 rhf=False, shift=0.0, diis_space=5, active=None):
+        """active = (act_occ_b, act_unocc_a) with calc_type 'CCSDt' (ccq_b200_init_ex)."""
         lib = load()
         self._lib = lib
         self.ptr = C.c_void_p()
@@ -231,8 +267,17 @@ class Context:
             self._keep = [np.asfortranarray(x, dtype=np.float64) for x in arrs]
             init = lib.ccq_b200_init
         fa, fb, vaa, vab, vbb = self._keep
-        _err(init(C.byref(d), calc_type.encode(), _p(fa), _p(fb), _p(vaa), _p(vab), _p(vbb),
-                  int(bool(rhf)), float(shift), int(diis_space), C.byref(self.ptr)))
+        if active is not None or calc_type == 'CCSDt':
+            m1, m2 = active if active is not None else (-1, -1)
+            opts = InitOpts(int(init == lib.ccq_b200_init_rowmajor), int(m1), int(m2))
+            _err(lib.ccq_b200_init_ex(C.byref(d), calc_type.encode(), C.cast(C.pointer(opts), C.c_void_p), _p(fa),
+                                      _p(fb), _p(vaa), _p(vab), _p(vbb), int(bool(rhf)), float(shift),
+                                      int(diis_space), C.byref(self.ptr)))
+        else:
+            _err(init(C.byref(d), calc_type.encode(), _p(fa), _p(fb), _p(vaa), _p(vab), _p(vbb),
+                      int(bool(rhf)), float(shift), int(diis_space), C.byref(self.ptr)))
+        self.dims = d
+        self.active = active
         self._keep = None
         ts, vs = I64(), I64()
         _err(lib.ccq_b200_sizes(self.ptr, C.byref(ts), C.byref(vs)))

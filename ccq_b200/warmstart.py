@@ -1,19 +1,25 @@
-"""Learned warm start of the T2 amplitudes (lambda-swept Hamiltonian family).
+"""Learned warm start over a family of Hamiltonians (lambda-swept off-diagonal ERIs).
 
-The reference starts every solve from T = 0, so its first sweep produces the
-MP2 doubles t = -<ij||ab> / D (D = f_aa + f_bb - f_ii - f_jj).  Here a small
-network predicts the remaining correction per amplitude,
+The reference starts every solve from T = 0.  Here a new member of a family
+whose other members are solved starts from a prediction:
 
-    t2_init = mp2 * (1 + r),   r = net(features)
-
-where the features are symmetric under the antisymmetry of the amplitude
-(gap D, the occupied and virtual orbital-energy sums, log |mp2|, log |v|, the
-family parameter lambda, and, from the nearest solved member of the family
-(the anchor), its converged ratio t/mp2 - 1 at the same element and the lambda
-distance to it), so t2_init keeps the antisymmetry of mp2 and vanishes where
-mp2 does.  T1 and T3 start from the anchor's converged values (zero without an
-anchor); T4 is built by the first sweep.  The exact CC iteration to the same
-tol decides the result: the warm start only changes where the iteration starts.
+  * base: the amplitudes of the two solved members that bracket its lambda,
+    interpolated linearly in lambda (every T1, T2 and T3 element);
+  * learned correction: two small networks (net2 for T2, net3 for T3,
+    8 -> 32 -> 32 -> 1, tanh, FP32) predict each element's ratio to the base,
+        t = t_int (1 + net(x)),
+    from features that are symmetric under the amplitudes' antisymmetry (gap,
+    occupied and virtual orbital-energy sums, log |t_int|, lambda, the two
+    members' relative difference, the upper member's weight, and the weight
+    w_lo w_hi (lambda_hi - lambda_lo)^2 of the interpolation's second-order
+    error), so the start keeps every antisymmetry of the stored blocks.  The
+    networks learn the curvature of t(lambda) that the interpolation misses:
+    trained on the solved members, each predicted from its two neighbours,
+    with elements drawn with probability proportional to t_int^2 so that the
+    mean-squared loss weighs them as they weigh in the iteration's error.
+T4 is built by the first sweep.  The exact CC iteration to the same tol
+decides the result: the start only changes where the iteration begins, and
+the plain T = 0 start is the fallback.
 
 Training and inference run in this library's kernels (``ccq_b200_mlp_*``,
 ``csrc/mlp.cu``): forward, backward (mean-squared loss) and Adam, FP32.
@@ -67,69 +73,6 @@ def _check(code):
         raise lib.CCQB200Error(code, 'warm-start network kernel failed')
 
 
-def block_features(fdiag_o, fdiag_v, v_block, lam, anchor_ratio=None, dlam=0.0):
-    """Features and MP2 amplitudes of one stored T2 block.
-
-    fdiag_o = (occ energies of the two occupied axes), fdiag_v likewise;
-    v_block[i, j, a, b] = <ij||ab> in the block's spin pattern; anchor_ratio =
-    the anchor's converged t/mp2 - 1 on this block (zero without an anchor),
-    dlam = lambda - the anchor's lambda.
-    Returns (X [N, NFEAT], mp2 [N]) over every stored element, and the block shape.
-    """
-    eo1, eo2 = fdiag_o
-    ev1, ev2 = fdiag_v
-    eo = eo1[:, None, None, None] + eo2[None, :, None, None]
-    ev = ev1[None, None, :, None] + ev2[None, None, None, :]
-    gap = ev - eo
-    mp2 = -v_block / gap
-    shape = v_block.shape
-    tiny = 1e-300
-    ar = np.zeros(shape) if anchor_ratio is None else np.asarray(anchor_ratio).reshape(shape)
-    X = np.stack([gap, np.broadcast_to(eo, shape), np.broadcast_to(ev, shape),
-                  np.log(np.abs(mp2) + tiny), np.log(np.abs(v_block) + tiny),
-                  np.full(shape, lam), ar, np.full(shape, dlam)], axis=-1).reshape(-1, NFEAT)
-    return X, mp2.reshape(-1), shape
-
-
-def ratios(mp2, t, cut=1e-6):
-    """t / mp2 - 1 where |mp2| exceeds cut * max |mp2| (else 0), clipped to [-2, 2]."""
-    r = np.zeros_like(mp2)
-    m = np.abs(mp2) > cut * np.abs(mp2).max()
-    r[m] = np.clip((t[m] - mp2[m]) / mp2[m], -2.0, 2.0)
-    return r
-
-
-def anchor_of(spec, t):
-    """(lambda, {block: converged t/mp2 - 1}) of a solved family member (t: its t_vec)."""
-    s = synth.system(spec)
-    lay = tlayout(s)
-    out = {}
-    for name, X, mp2, shape in system_blocks(s, spec.lam):
-        out[name] = ratios(mp2, np.asarray(lay.view(t, name)).reshape(-1)).reshape(shape)
-    return spec.lam, out
-
-
-def system_blocks(s, lam, anchor=None):
-    """(name, X, mp2, shape) for T2A, T2B, T2C of a system from ``synth.system``;
-    anchor = ``anchor_of`` of the nearest solved family member, or None."""
-    d = s['dims']
-    fr = d.froz
-    fa = np.diag(s['f_a'])[fr:]
-    fb = np.diag(s['f_b'])[fr:]
-    oa, ob = d.oa, d.ob
-    vaa, vab, vbb = s['v_aa'], s['v_ab'], s['v_bb']
-    out = []
-    for name, (eoa, eob, eva, evb, v) in (
-            ('T2A', (fa[:oa], fa[:oa], fa[oa:], fa[oa:], vaa[:oa, :oa, oa:, oa:])),
-            ('T2B', (fa[:oa], fb[:ob], fa[oa:], fb[ob:], vab[:oa, :ob, oa:, ob:])),
-            ('T2C', (fb[:ob], fb[:ob], fb[ob:], fb[ob:], vbb[:ob, :ob, ob:, ob:]))):
-        ar = None if anchor is None else anchor[1][name]
-        dl = 0.0 if anchor is None else lam - anchor[0]
-        X, mp2, shape = block_features((eoa, eob), (eva, evb), np.asarray(v), lam, ar, dl)
-        out.append((name, X, mp2, shape))
-    return out
-
-
 class WarmStart:
     """The network plus its feature / target standardisation."""
 
@@ -154,25 +97,6 @@ class WarmStart:
         self.xmu = np.zeros(NFEAT) if xmu is None else np.asarray(xmu)
         self.xsd = np.ones(NFEAT) if xsd is None else np.asarray(xsd)
         self.ysd = float(ysd)
-
-    # -- data -------------------------------------------------------------------
-    @staticmethod
-    def samples(specs_and_t2, cut=1e-6):
-        """Training samples from (spec, {block: converged T2 array}, anchor) triples.
-
-        Target r = (t - mp2) / mp2 on elements whose |mp2| exceeds cut * max|mp2|,
-        clipped to [-2, 2].
-        """
-        xs, ys = [], []
-        for spec, t2, anchor in specs_and_t2:
-            s = synth.system(spec)
-            for name, X, mp2, shape in system_blocks(s, spec.lam, anchor):
-                t = np.asarray(t2[name]).reshape(-1)
-                m = np.abs(mp2) > cut * np.abs(mp2).max()
-                r = np.clip((t[m] - mp2[m]) / mp2[m], -2.0, 2.0)
-                xs.append(X[m])
-                ys.append(r)
-        return np.concatenate(xs), np.concatenate(ys)
 
     def fit_scaling(self, X, y):
         self.xmu = X.mean(axis=0)
@@ -222,15 +146,6 @@ class WarmStart:
                                            torch.cuda.current_stream().cuda_stream))
         return Y.cpu().numpy().astype(np.float64) * self.ysd
 
-    def initial_t(self, s, lam, layout, anchor=None, t_anchor=None):
-        """A full t_vec (reference layout): T2 = mp2 (1 + r); T1 and T3 from the anchor's
-        converged t_vec ``t_anchor`` when given, else zero."""
-        t = np.zeros(layout.t_size) if t_anchor is None else np.array(t_anchor, dtype=np.float64)
-        for name, X, mp2, shape in system_blocks(s, lam, anchor):
-            r = np.clip(self.predict_ratio(X), -2.0, 2.0)
-            layout.view(t, name)[...] = (mp2 * (1.0 + r)).reshape(shape)
-        return t
-
     # -- persistence -------------------------------------------------------------
     def save(self, path):
         np.savez(path, params=self.params, xmu=self.xmu, xsd=self.xsd, ysd=self.ysd)
@@ -242,18 +157,26 @@ class WarmStart:
 
 
 def mp2_t(s, layout):
-    """t_vec with T2 = MP2 (the first sweep's result from T = 0), for comparison."""
+    """t_vec with T2 = MP2, -<ij||ab> / (f_aa + f_bb - f_ii - f_jj) (the first sweep's result from T = 0),
+    for comparison."""
+    d = s['dims']
+    fr = d.froz
+    fa = np.diag(s['f_a'])[fr:]
+    fb = np.diag(s['f_b'])[fr:]
+    oa, ob = d.oa, d.ob
     t = np.zeros(layout.t_size)
-    for name, X, mp2, shape in system_blocks(s, 1.0):
-        layout.view(t, name)[...] = mp2.reshape(shape)
+    for name, (eo1, eo2, ev1, ev2, v) in (
+            ('T2A', (fa[:oa], fa[:oa], fa[oa:], fa[oa:], s['v_aa'][:oa, :oa, oa:, oa:])),
+            ('T2B', (fa[:oa], fb[:ob], fa[oa:], fb[ob:], s['v_ab'][:oa, :ob, oa:, ob:])),
+            ('T2C', (fb[:ob], fb[:ob], fb[ob:], fb[ob:], s['v_bb'][:ob, :ob, ob:, ob:]))):
+        gap = (ev1[None, None, :, None] + ev2[None, None, None, :] - eo1[:, None, None, None] -
+               eo2[None, :, None, None])
+        layout.view(t, name)[...] = -np.asarray(v) / gap
     return t
 
 
 def tlayout(s):
     return I.TLayout(s['dims'])
-
-
-T1_T3 = ('T1A', 'T1B', 'T3A', 'T3B', 'T3C', 'T3D')
 
 
 def bracket(train_lams, lam, exclude=None):
@@ -280,19 +203,11 @@ def bracket(train_lams, lam, exclude=None):
     return [(a, 1.0 - wb), (b, wb)]
 
 
-def start_transfer(s, lam, layout, anchor, t_anchor):
-    """No network: T2 = mp2 (1 + the anchor's converged ratio), T1 and T3 copied from the anchor."""
-    t = np.array(t_anchor, dtype=np.float64)
-    for name, X, mp2, shape in system_blocks(s, lam):
-        layout.view(t, name)[...] = (mp2 * (1.0 + anchor[1][name].reshape(-1))).reshape(shape)
-    return t
-
-
-def start_interp(s, lam, layout, members):
-    """No network: members = [(weight, anchor, t_vec)] of ``bracket``; every amplitude (T1, T2, T3)
-    interpolated linearly in lambda between the two members."""
+def interp_start(s, lam, layout, members):
+    """The base of the start, no network: members = [(weight, _, t_vec, lambda)] of ``bracket``;
+    every amplitude (T1, T2, T3) interpolated linearly in lambda between the two members."""
     t = np.zeros(layout.t_size)
-    for w, anc, tv in members:
+    for w, _, tv, la in members:
         t += w * np.asarray(tv)
     return t
 
@@ -384,11 +299,6 @@ def interp_features(s, lam, members, layout, blocks, rng=None, per_block=None, c
     return out
 
 
-def interp_start(s, lam, layout, members):
-    """The base of the two-anchor start (T1, T2, T3 interpolated), no network."""
-    return start_interp(s, lam, layout, [(w, anc, tv) for w, anc, tv, la in members])
-
-
 class TwoAnchorWarmStart:
     """net2 (T2) and net3 (T3) over the interpolated start; trained and evaluated by the library's
     kernels (``ccq_b200_mlp_*``)."""
@@ -439,9 +349,15 @@ class TwoAnchorWarmStart:
 
 
 def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1e-8, epochs=600, seed=C4_SEED,
-          log=None, ablation=True, chunk=50):
-    """Plain solves of the whole family, training on ``train`` of them, warm-started
-    solves of the rest; iterations to tol and |dE| between the two starts."""
+          log=None, chunk=50):
+    """The family solved plainly (T = 0, the reference's start), the networks trained on ``train`` of
+    its members, and the other members solved from each start: iterations to tol and |dE| against the
+    plain solves.
+
+    Starts of the evaluation members: ``warm`` (interpolation in lambda between the two bracketing
+    solved members, corrected by net2 on T2 and net3 on T3), and without a network: the T2 of MP2,
+    the nearest solved member's amplitudes as they are (``anchor``), the interpolation alone
+    (``interp``), and the networks on T2 only (``warm_t2_only``)."""
     import time
     from . import batch
     specs = [synth.SynthSpec(norb, nel, 2 * norb, 0.03, seed, float(l)) for l in np.linspace(0.5, 2.0, count)]
@@ -449,82 +365,46 @@ def study(method='CCSDT', norb=24, nel=10, count=C4_COUNT, train=C4_TRAIN, tol=1
     t0 = time.perf_counter()
     plain, _ = batch.solve_batch(specs, tol=tol, calc_type=method, keep_t=True, chunk=chunk)
     t1 = time.perf_counter()
-    anchors = {i: anchor_of(specs[i], plain[i]['t']) for i in tr}
+    tl = [specs[j].lam for j in tr]
 
-    def nearest(i, exclude_self):
-        # the solved training member closest in lambda (another one for a training member)
-        cand = [j for j in tr if not (exclude_self and j == i)]
-        return min(cand, key=lambda j: (abs(specs[j].lam - specs[i].lam), j))
-    data = []
-    for i in tr:
-        s = synth.system(specs[i])
-        lay = tlayout(s)
-        data.append((specs[i], {b: lay.view(plain[i]['t'], b) for b in ('T2A', 'T2B', 'T2C')},
-                     anchors[nearest(i, True)]))
-    X, y = WarmStart.samples(data)
-    ws = WarmStart(seed=seed)
-    ws.fit_scaling(X, y)
-    hist = ws.train(X, y, epochs=epochs, log=log)
+    def members(i, exclude=None):
+        return [(w, None, plain[tr[k]]['t'], specs[tr[k]].lam) for k, w in bracket(tl, specs[i].lam, exclude)]
+    # training: every training member from its two bracketing neighbours (itself left out)
+    items = [(specs[i], plain[i]['t'], members(i, k)) for k, i in enumerate(tr)]
+    two = TwoAnchorWarmStart(seed=seed)
+    X2, Y2, X3, Y3 = two.samples(items, tlayout, seed=seed)
+    h2, h3 = two.train(X2, Y2, X3, Y3, epochs=epochs, log=log)
     t2 = time.perf_counter()
-    inits, mp2s = [], []
+    starts = {'warm': [], 'mp2': [], 'anchor': [], 'interp': [], 'warm_t2_only': []}
     for i in ev:
         s = synth.system(specs[i])
         lay = tlayout(s)
-        a = nearest(i, False)
-        inits.append(ws.initial_t(s, specs[i].lam, lay, anchors[a], plain[a]['t']))
-        mp2s.append(mp2_t(s, lay))
-    warm, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=inits, chunk=chunk)
+        mem = members(i)
+        starts['warm'].append(two.initial_t(s, specs[i].lam, lay, mem))
+        starts['mp2'].append(mp2_t(s, lay))
+        near = min(tr, key=lambda j: (abs(specs[j].lam - specs[i].lam), j))
+        starts['anchor'].append(np.array(plain[near]['t']))
+        starts['interp'].append(interp_start(s, specs[i].lam, lay, mem))
+        starts['warm_t2_only'].append(two.initial_t(s, specs[i].lam, lay, mem, use_t3=False))
     t3 = time.perf_counter()
-    mp2r, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=mp2s, chunk=chunk)
     legs = {}
-    if ablation:
-        # the same anchors without the network: the nearest member's converged amplitudes as they are,
-        # its T2/MP2 ratio transferred, and a linear interpolation in lambda between two members
-        tl = [specs[j].lam for j in tr]
-        starts = {'anchor': [], 'transfer': [], 'interp': []}
-        for i in ev:
-            s = synth.system(specs[i])
-            lay = tlayout(s)
-            a = nearest(i, False)
-            starts['anchor'].append(np.array(plain[a]['t']))
-            starts['transfer'].append(start_transfer(s, specs[i].lam, lay, anchors[a], plain[a]['t']))
-            mem = [(w, anchors[tr[k]], plain[tr[k]]['t']) for k, w in bracket(tl, specs[i].lam)]
-            starts['interp'].append(start_interp(s, specs[i].lam, lay, mem))
-        # the two-anchor start with its networks (T2 and T3 corrections over the interpolation)
-        tw = time.perf_counter()
-        items = []
-        for k, i in enumerate(tr):
-            mem = [(w, anchors[tr[j]], plain[tr[j]]['t'], specs[tr[j]].lam) for j, w in bracket(tl, specs[i].lam, k)]
-            items.append((specs[i], plain[i]['t'], mem))
-        two = TwoAnchorWarmStart(seed=seed)
-        X2, Y2, X3, Y3 = two.samples(items, tlayout, seed=seed)
-        h2, h3 = two.train(X2, Y2, X3, Y3, epochs=epochs)
-        starts['two_anchor_net_t2'] = []
-        starts['two_anchor_net'] = []
-        for i in ev:
-            s = synth.system(specs[i])
-            lay = tlayout(s)
-            mem = [(w, anchors[tr[k]], plain[tr[k]]['t'], specs[tr[k]].lam) for k, w in bracket(tl, specs[i].lam)]
-            starts['two_anchor_net_t2'].append(two.initial_t(s, specs[i].lam, lay, mem, use_t3=False))
-            starts['two_anchor_net'].append(two.initial_t(s, specs[i].lam, lay, mem))
-        legs['two_anchor_training'] = {'t2_samples': int(X2.shape[0]), 't3_samples': int(X3.shape[0]),
-                                       'loss_t2': [h2[0][1], h2[-1][1]] if h2 else None,
-                                       'loss_t3': [h3[0][1], h3[-1][1]] if h3 else None,
-                                       'seconds': time.perf_counter() - tw}
-        for name, st in starts.items():
-            rr, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=st, chunk=chunk)
-            it_ = np.array([r['iterations'] for r in rr], dtype=float)
-            legs[name] = {'iterations_mean': float(it_.mean()),
-                          'max_dE': float(max(abs(plain[i]['e_cor'] - r['e_cor']) for i, r in zip(ev, rr))),
-                          'failed': int(sum(r['failed'] for r in rr))}
+    for name, st in starts.items():
+        rr, _ = batch.solve_batch([specs[i] for i in ev], tol=tol, calc_type=method, t_init=st, chunk=chunk)
+        it_ = np.array([r['iterations'] for r in rr], dtype=float)
+        legs[name] = {'iterations_mean': float(it_.mean()),
+                      'max_dE': float(max(abs(plain[i]['e_cor'] - r['e_cor']) for i, r in zip(ev, rr))),
+                      'failed': int(sum(r['failed'] for r in rr))}
+        if name == 'warm':
+            t4 = time.perf_counter()
     pi = np.array([plain[i]['iterations'] for i in ev], dtype=float)
-    wi = np.array([r['iterations'] for r in warm], dtype=float)
-    mi = np.array([r['iterations'] for r in mp2r], dtype=float)
-    de = max(abs(plain[i]['e_cor'] - r['e_cor']) for i, r in zip(ev, warm))
+    w = legs['warm']
     return {'method': method, 'norb': norb, 'nel': nel, 'family': count, 'train': len(tr), 'eval': len(ev),
-            'tol': tol, 'plain_iterations_mean': float(pi.mean()), 'warm_iterations_mean': float(wi.mean()),
-            'mp2_start_iterations_mean': float(mi.mean()), 'no_network': legs,
-            'iteration_reduction': float(1.0 - wi.sum() / pi.sum()), 'max_dE': float(de),
-            'failed': int(sum(r['failed'] for r in warm) + sum(plain[i]['failed'] for i in ev)),
-            'train_samples': int(X.shape[0]), 'loss_history': hist,
-            'seconds': {'plain_family': t1 - t0, 'train': t2 - t1, 'warm_eval': t3 - t2}}
+            'tol': tol, 'plain_iterations_mean': float(pi.mean()), 'warm_iterations_mean': w['iterations_mean'],
+            'iteration_reduction': float(1.0 - w['iterations_mean'] / pi.mean()), 'max_dE': w['max_dE'],
+            'failed': int(w['failed'] + sum(plain[i]['failed'] for i in ev)),
+            'starts': {k: v for k, v in legs.items()},
+            'network_gain_over_interp': float(1.0 - w['iterations_mean'] / legs['interp']['iterations_mean']),
+            'train_samples': {'t2': int(X2.shape[0]), 't3': int(X3.shape[0])},
+            'loss': {'t2': [h2[0][1], h2[-1][1]] if h2 else None, 't3': [h3[0][1], h3[-1][1]] if h3 else None},
+            'loss_history': {'t2': h2, 't3': h3},
+            'seconds': {'plain_family': t1 - t0, 'train': t2 - t1, 'starts': t3 - t2, 'warm_eval': t4 - t3}}

@@ -130,6 +130,42 @@ int ccq_b200_init_rowmajor(const ccq_b200_dims *dims, const char *calc_type,
                            int64_t rhf, double shift, int64_t diis_space,
                            ccq_b200_ctx **out);
 
+/* Options of ccq_b200_init_ex. */
+typedef struct {
+    int64_t rowmajor;     /* 0: f and v Fortran-ordered (as ccq_b200_init), 1: row-major (as ccq_b200_init_rowmajor) */
+    int64_t act_occ_b;    /* calc_type "CCSDt": ccq's sys%act_occ_b; -1 otherwise */
+    int64_t act_unocc_a;  /* calc_type "CCSDt": ccq's sys%act_unocc_a; -1 otherwise */
+} ccq_b200_init_opts;
+
+/* ccq_b200_init with options; the one way to build calc_type "CCSDt"
+ * (parser.f90:380-388, update_clusters_t3_opt update_cc.F90:325-2191):
+ * triples with at least one active occupied orbital (above act_occ_b) and one
+ * active virtual (up to act_unocc_a) are iterated, the others stay zero, and
+ * every T3 residual contraction runs only over the active triples' index
+ * ranges.  The T vector keeps the full-block layout of get_t_sizes here;
+ * ccq_b200_t3_compress / _expand convert to and from ccq's compressed
+ * CCSDt layout (get_t_sizes_act). */
+int ccq_b200_init_ex(const ccq_b200_dims *dims, const char *calc_type, const ccq_b200_init_opts *opts,
+                     const double *f_a, const double *f_b,
+                     const double *v_aa, const double *v_ab, const double *v_bb,
+                     int64_t rhf, double shift, int64_t diis_space,
+                     ccq_b200_ctx **out);
+
+/* ccq's compressed CCSDt T vector (get_t_sizes_act, cc_utils.f90:560-630;
+ * the sub-blocks t3A, t3B1..t3B4, t3C1..t3C4, t3D of
+ * cc_opt_ccsdt/t2B0000_update_opt.f:48-57) and the full-block T vector of a
+ * CCSDt context (get_t_sizes).  Host functions, no context or device needed.
+ * ccq_b200_t_size_act returns the compressed length (pos(16) - 1) or a
+ * negative error code.  compress copies the active slices out of a full
+ * vector; expand writes them back with every antisymmetric copy and zeros
+ * elsewhere.  n_full / n_act must equal the two lengths (else
+ * CCQ_B200_EINVAL). */
+int64_t ccq_b200_t_size_act(const ccq_b200_dims *dims, int64_t act_occ_b, int64_t act_unocc_a);
+int ccq_b200_t_compress(const ccq_b200_dims *dims, int64_t act_occ_b, int64_t act_unocc_a,
+                        const double *t_full, int64_t n_full, double *t_act, int64_t n_act);
+int ccq_b200_t_expand(const ccq_b200_dims *dims, int64_t act_occ_b, int64_t act_unocc_a,
+                      const double *t_act, int64_t n_act, double *t_full, int64_t n_full);
+
 /* Length of t_vec (get_t_sizes, cc_utils.f90:479-559) and of the DIIS
  * vector (solve_cc.f90:66-77). */
 int ccq_b200_sizes(const ccq_b200_ctx *ctx, int64_t *t_size, int64_t *vec_size);

@@ -19,39 +19,14 @@ def test_oracle_gradient_matches_finite_differences():
         assert abs(fd - g[k]) < 1e-7 + 1e-5 * abs(fd)
 
 
-def test_features_keep_the_amplitude_symmetry():
+def test_mp2_start_is_the_first_sweeps_doubles():
+    """T2 = -<ij||ab> / D, antisymmetric, T1 and T3 zero."""
     s = synth.system(synth.SynthSpec(8, 4, 16, 0.03, 4000, 1.3))
-    for name, X, mp2, shape in warmstart.system_blocks(s, 1.3):
-        Xr = X.reshape(shape + (warmstart.NFEAT,))
-        m = mp2.reshape(shape)
-        if name in ('T2A', 'T2C'):
-            # antisymmetric mp2, symmetric features: mp2 * (1 + r(x)) stays antisymmetric
-            assert np.allclose(m, -m.transpose(1, 0, 2, 3))
-            assert np.allclose(Xr, Xr.transpose(1, 0, 2, 3, 4))
-            assert np.allclose(Xr, Xr.transpose(0, 1, 3, 2, 4))
-
-
-def test_anchor_features_keep_the_symmetry():
-    """The anchor's converged ratio t/mp2 - 1 is symmetric where mp2 is antisymmetric."""
-    spec = synth.SynthSpec(8, 4, 16, 0.03, 4000, 1.1)
-    s = synth.system(spec)
     lay = warmstart.tlayout(s)
-    rng = np.random.default_rng(3)
-    t = np.zeros(lay.t_size)
-    for name, X, mp2, shape in warmstart.system_blocks(s, 1.1):
-        # an antisymmetric stand-in for a converged T2: mp2 times a symmetric factor
-        f = 1.0 + 0.1 * rng.normal(size=shape)
-        if name in ('T2A', 'T2C'):
-            f = 0.25 * (f + f.transpose(1, 0, 2, 3) + f.transpose(0, 1, 3, 2) + f.transpose(1, 0, 3, 2))
-        lay.view(t, name)[...] = mp2.reshape(shape) * f
-    anchor = warmstart.anchor_of(spec, t)
-    s2 = synth.system(synth.SynthSpec(8, 4, 16, 0.03, 4000, 1.3))
-    for name, X, mp2, shape in warmstart.system_blocks(s2, 1.3, anchor):
-        Xr = X.reshape(shape + (warmstart.NFEAT,))
-        assert np.allclose(Xr[..., 7], 1.3 - 1.1)
-        if name in ('T2A', 'T2C'):
-            assert np.allclose(Xr, Xr.transpose(1, 0, 2, 3, 4))
-            assert np.allclose(Xr, Xr.transpose(0, 1, 3, 2, 4))
+    t = warmstart.mp2_t(s, lay)
+    m = lay.view(t, 'T2A')
+    assert np.allclose(m, -m.transpose(1, 0, 2, 3)) and np.abs(m).max() > 0
+    assert not np.any(lay.view(t, 'T1A')) and not np.any(lay.view(t, 'T3B'))
 
 
 def test_family_and_split():
@@ -93,8 +68,7 @@ def test_two_anchor_start_keeps_the_antisymmetry():
         s = synth.system(sp)
         lay = warmstart.tlayout(s)
         sols.append((sp, s, lay, _antisym_t(lay, rng)))
-    members = [(w, warmstart.anchor_of(sols[k][0], sols[k][3]), sols[k][3], sols[k][0].lam)
-               for k, w in warmstart.bracket([1.0, 1.2], 1.1)]
+    members = [(w, None, sols[k][3], sols[k][0].lam) for k, w in warmstart.bracket([1.0, 1.2], 1.1)]
     s = synth.system(synth.SynthSpec(8, 6, 16, 0.03, 4000, 1.1))
     lay = warmstart.tlayout(s)
     t = warmstart.interp_start(s, 1.1, lay, members)
@@ -117,8 +91,7 @@ def test_two_anchor_start_keeps_the_antisymmetry():
             P = Xr.transpose(perm + (6,))
             assert np.allclose(Xr[nz], P[nz])
     # at the anchor's own lambda the interpolation gives that anchor's amplitudes
-    own = [(w, warmstart.anchor_of(sols[k][0], sols[k][3]), sols[k][3], sols[k][0].lam)
-           for k, w in warmstart.bracket([1.0, 1.2], 1.0)]
+    own = [(w, None, sols[k][3], sols[k][0].lam) for k, w in warmstart.bracket([1.0, 1.2], 1.0)]
     t0 = warmstart.interp_start(sols[0][1], 1.0, sols[0][2], own)
     for b in ('T1A', 'T3B'):
         np.testing.assert_allclose(sols[0][2].view(t0, b), sols[0][2].view(sols[0][3], b), atol=1e-15)
