@@ -435,4 +435,4 @@ def header_symbols(header=None):
     header = header or os.path.join(HERE, '..', 'include', 'ccq_b200.h')
     text = open(header).read()
     text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
-    return sorted(set(re.findall(r'^\s*(?:int|void)\s+(\w+)\s*\(', text, flags=re.M)))
+    return sorted(set(re.findall(r'^\s*(?:int|int64_t|void)\s+(\w+)\s*\(', text, flags=re.M)))
