@@ -108,7 +108,9 @@ def create_instances(specs, calc_type='CCSD', diis_space=5, graph=True, threads=
     def make(sp):
         torch.cuda.set_device(dev)
         return Instance(sp, calc_type, diis_space, graph)
-    n = threads or min(16, os.cpu_count() or 1, max(1, len(specs)))
+    # four threads: more contend for the CUDA runtime's locks (64 contexts of 16-48 orbitals: 1.2 s with
+    # four threads, 1.4 s with eight, 2.4 s with sixteen, 5.9 s with one)
+    n = threads or min(4, os.cpu_count() or 1, max(1, len(specs)))
     if n <= 1 or len(specs) <= 1:
         return [make(sp) for sp in specs]
     with ThreadPoolExecutor(max_workers=n) as ex:

@@ -145,6 +145,127 @@ void for_each_sub_element(const Layout &L, F f) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Device side: the compressed T3 part of a DIIS vector gathered from, and
+// scattered back into, the full T3 blocks of a resident T vector.  One thread
+// per compressed element; a thread decodes its sub-block and coordinates from
+// the ten sub-block geometries (no tables).  The scatter writes every
+// antisymmetric copy; elements reached from several compressed positions get
+// the same value from each.
+// ---------------------------------------------------------------------------
+namespace ccqb {
+
+void t3act_geometry(long long froz, long long occ_a, long long occ_b, long long orbs, long long act_occ_b,
+                    long long act_unocc_a, T3ActGeom &g) {
+    const ccq_b200_dims dims{froz, occ_a, occ_b, orbs};
+    const Layout L(dims, act_occ_b, act_unocc_a);
+    g.t12 = L.t12;
+    long long off = 0;
+    for (int s = 0; s < 10; ++s) {
+        const Sub &u = L.subs[s];
+        g.sub_off[s] = off;
+        g.block[s] = u.block;
+        long long n = 1;
+        for (int k = 0; k < 6; ++k) {
+            g.lo[s][k] = (int)(u.r[k].lo - L.full[u.block][k].lo);
+            g.n[s][k] = (int)u.r[k].n();
+            n *= u.r[k].n();
+        }
+        off += n;
+    }
+    g.sub_off[10] = off;
+    g.n_act = off;
+    for (int b = 0; b < 4; ++b) {
+        g.full_off[b] = L.full_off[b];
+        for (int k = 0; k < 6; ++k) g.fn[b][k] = (int)L.full[b][k].n();
+    }
+    g.t3_begin = L.full_off[0];
+    g.t3_end = L.full_size;
+}
+
+}  // namespace ccqb
+
+namespace {
+
+// the sub-block of compressed element p (sub_off is increasing; empty sub-blocks are passed over) and
+// its coordinates in the full block
+__device__ __forceinline__ int t3act_decode(const ccqb::T3ActGeom &g, long long p, int x[6]) {
+    int s = 0;
+    while (s < 9 && p >= g.sub_off[s + 1]) ++s;
+    long long e = p - g.sub_off[s];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        x[k] = g.lo[s][k] + (int)(e % g.n[s][k]);
+        e /= g.n[s][k];
+    }
+    return g.block[s];
+}
+
+__device__ __forceinline__ long long t3act_full(const ccqb::T3ActGeom &g, int b, const int x[6]) {
+    long long o = 0, st = 1;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        o += (long long)x[k] * st;
+        st *= g.fn[b][k];
+    }
+    return g.full_off[b] + o;
+}
+
+__global__ void t3act_gather_kernel(ccqb::T3ActGeom g, const double *tvec, double *cvec) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.n_act;
+         p += (long long)gridDim.x * blockDim.x) {
+        int x[6];
+        const int b = t3act_decode(g, p, x);
+        cvec[p] = tvec[t3act_full(g, b, x)];
+    }
+}
+
+__global__ void t3act_scatter_kernel(ccqb::T3ActGeom g, const double *cvec, double *tvec) {
+    // permutations of a group of three (with parity); a group of two uses the first two
+    const int p3[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 1, 0}, {1, 2, 0}, {2, 0, 1}};
+    const int s3[6] = {1, -1, -1, -1, 1, 1};
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.n_act;
+         p += (long long)gridDim.x * blockDim.x) {
+        int x[6];
+        const int b = t3act_decode(g, p, x);
+        const double v = cvec[p];
+        // same-spin axis groups: t3a, t3d (0,1,2),(3,4,5); t3b (1,2),(4,5); t3c (0,1),(3,4)
+        const bool three = b == 0 || b == 3;
+        const int g0 = b == 1 ? 1 : 0, g1 = b == 1 ? 4 : 3;
+        const int np = three ? 6 : 2, len = three ? 3 : 2;
+        for (int u = 0; u < np; ++u)
+            for (int w = 0; w < np; ++w) {
+                int y[6] = {x[0], x[1], x[2], x[3], x[4], x[5]};
+                for (int k = 0; k < len; ++k) {
+                    y[g0 + k] = x[g0 + p3[u][k]];
+                    y[g1 + k] = x[g1 + p3[w][k]];
+                }
+                tvec[t3act_full(g, b, y)] = s3[u] * s3[w] * v;
+            }
+    }
+}
+
+int layout_grid(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+namespace ccqb {
+
+void launch_t3act_gather(const T3ActGeom &g, const double *tvec, double *cvec, cudaStream_t s) {
+    if (g.n_act) t3act_gather_kernel<<<layout_grid(g.n_act), 256, 0, s>>>(g, tvec, cvec);
+}
+
+void launch_t3act_scatter(const T3ActGeom &g, const double *cvec, double *tvec, cudaStream_t s) {
+    cudaMemsetAsync(tvec + g.t3_begin, 0, sizeof(double) * (size_t)(g.t3_end - g.t3_begin), s);
+    if (g.n_act) t3act_scatter_kernel<<<layout_grid(g.n_act), 256, 0, s>>>(g, cvec, tvec);
+}
+
+}  // namespace ccqb
+
 extern "C" {
 
 int64_t ccq_b200_t_size_act(const ccq_b200_dims *dims, int64_t act_occ_b, int64_t act_unocc_a) {

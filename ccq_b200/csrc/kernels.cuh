@@ -123,6 +123,23 @@ void launch_assemble(const AsmArgs &a, cudaStream_t s);
 void launch_fill(double *p, double v, long long n, cudaStream_t s);
 void launch_f2c4(const double *f, double *out, long long n, cudaStream_t s);
 void launch_sqdiff(const double *a, const double *b, long long n, double *out, cudaStream_t s);
+
+// ccq's compressed CCSDt T3 (get_t_sizes_act): geometry of its ten sub-blocks inside the full T3
+// blocks of a T vector, and the gather / scatter between the two (csrc/ccsdt_layout.cu)
+struct T3ActGeom {
+    long long t12 = 0;              // T1 + T2 elements (the same in both layouts)
+    long long sub_off[11] = {};     // sub-block offsets within the compressed T3 part
+    int block[10] = {};             // 0..3: T3A..T3D
+    int lo[10][6] = {}, n[10][6] = {};   // sub-range start (0-based in the full block's axis) and extent
+    long long full_off[4] = {};     // T3A..T3D offsets in the full T vector
+    int fn[4][6] = {};              // full block extents (Fortran axis order)
+    long long n_act = 0;            // compressed T3 elements
+    long long t3_begin = 0, t3_end = 0;   // T3 range of the full T vector
+};
+void t3act_geometry(long long froz, long long occ_a, long long occ_b, long long orbs, long long act_occ_b,
+                    long long act_unocc_a, T3ActGeom &g);
+void launch_t3act_gather(const T3ActGeom &g, const double *tvec, double *cvec, cudaStream_t s);
+void launch_t3act_scatter(const T3ActGeom &g, const double *cvec, double *tvec, cudaStream_t s);
 void launch_diis_gram(const double *ring, long long stride, int ds, long long n, double *gram, cudaStream_t s);
 void launch_diis_solve(double *gram, int ds, double *coef, int *info, cudaStream_t s);
 void launch_diis_extrap(const double *ring, long long stride, int ds, long long n, const double *coef, double *t,

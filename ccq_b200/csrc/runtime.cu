@@ -99,9 +99,15 @@ struct Op {
     ViewSpec c, a, b;
     std::string tag;
     std::vector<std::vector<std::string>> restrict_groups;   // R= annotation
-    // labels whose range starts above their view's own start (sub-ranges of an active-space
-    // restriction): the offset, so that restriction groups compare the labels' full-range values
-    std::map<std::string, long long> lshift;
+    // active-space filters of the output index modes (CCSDt): a table keeps a tuple only if it passes
+    // every filter of its mode
+    struct ModeFilter {
+        int mode = 0;                      // 0: the M mode (labels of A and C), 1: the N mode (B and C)
+        bool any = true;                   // true: some label active; false: no label active
+        std::vector<std::string> labels;
+        std::vector<long long> lo, hi;     // label active iff lo <= value < hi
+    };
+    std::vector<ModeFilter> filters;
     // ASSEMBLE
     std::string block, mode;
     std::vector<std::pair<double, ViewSpec>> terms;
@@ -302,6 +308,12 @@ struct ccq_b200_ctx {
     cudaGraphExec_t gexec = nullptr;
     int device = 0;
     long long act_occ_b = -1, act_unocc_a = -1;   // CCSDt: the active space the plan was restricted to
+    // CCSDt: DIIS runs over ccq's compressed T vector (T1, T2 and the active T3 sub-blocks of
+    // get_t_sizes_act), gathered from the full blocks after each sweep and scattered back after an
+    // extrapolation
+    bool cdiis = false;
+    T3ActGeom geom{};
+    double *cvec = nullptr;
     SplitWorkspace split{};
     // host round trip of ccq_b200_iterate_host: each t_vec block is copied to host_out as soon as its
     // last write of the sweep is done (copy stream cstream, joined into the sweep's stream at its end)
@@ -386,7 +398,7 @@ bool has(const Resolved &r, const std::string &l) { return r.stride.count(l) > 0
 // Restricted groups (label lists) are enumerated for increasing values only.
 void build_table(const std::vector<std::string> &labels, const std::map<std::string, long long> &extent,
                  const Resolved &x, const Resolved *y, const std::vector<std::vector<std::string>> &groups,
-                 const std::map<std::string, long long> &shift, std::vector<int> &tx, std::vector<int> &ty) {
+                 const std::vector<const Op::ModeFilter *> &filters, std::vector<int> &tx, std::vector<int> &ty) {
     tx.clear();
     ty.clear();
     std::vector<std::vector<int>> gidx;   // positions in `labels` of each group's members, in group order
@@ -398,12 +410,26 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
         }
         if (pos.size() == g.size()) gidx.push_back(pos);
     }
+    // each filter's labels as positions in `labels`
+    struct F {
+        bool any;
+        std::vector<int> pos;
+        std::vector<long long> lo, hi;
+    };
+    std::vector<F> fl;
+    for (auto *f : filters) {
+        F q{f->any, {}, f->lo, f->hi};
+        for (auto &l : f->labels) {
+            auto it = std::find(labels.begin(), labels.end(), l);
+            if (it == labels.end()) throw Error(CCQ_B200_EPLAN, "filter label " + l + " not in its index mode");
+            q.pos.push_back((int)(it - labels.begin()));
+        }
+        fl.push_back(q);
+    }
     const size_t nd = labels.size();
-    std::vector<long long> idx(nd, 0), ev(nd), sx(nd), sy(nd, 0), sh(nd, 0);
+    std::vector<long long> idx(nd, 0), ev(nd), sx(nd), sy(nd, 0);
     long long total = 1;
     for (size_t d = 0; d < nd; ++d) {
-        auto it = shift.find(labels[d]);
-        if (it != shift.end()) sh[d] = it->second;
         ev[d] = extent.at(labels[d]);
         sx[d] = x.stride.at(labels[d]);
         if (y) sy[d] = y->stride.at(labels[d]);
@@ -412,12 +438,42 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
     if (total == 0) return;
     tx.reserve((size_t)total);
     if (y) ty.reserve((size_t)total);
+    if (gidx.empty() && fl.empty()) {
+        // a plain product of the labels' ranges: expanded label by label (the last one fastest),
+        // the same order as the enumeration below, without per-tuple checks
+        long long mx = 0, my = 0;
+        for (size_t d = 0; d < nd; ++d) {
+            mx += (ev[d] - 1) * sx[d];
+            my += (ev[d] - 1) * sy[d];
+        }
+        if (mx > INT32_MAX || my > INT32_MAX) throw Error(CCQ_B200_ERANGE, "view offset beyond int32");
+        tx.assign(1, 0);
+        if (y) ty.assign(1, 0);
+        for (size_t d = 0; d < nd; ++d) {
+            const size_t cur = tx.size();
+            std::vector<int> nx(cur * (size_t)ev[d]), ny(y ? cur * (size_t)ev[d] : 0);
+            for (size_t j = 0; j < cur; ++j)
+                for (long long i = 0; i < ev[d]; ++i) {
+                    nx[j * ev[d] + i] = tx[j] + (int)(i * sx[d]);
+                    if (y) ny[j * ev[d] + i] = ty[j] + (int)(i * sy[d]);
+                }
+            tx.swap(nx);
+            if (y) ty.swap(ny);
+        }
+        return;
+    }
     bool more = true;
     while (more) {
         bool ok = true;
         for (auto &g : gidx)
             for (size_t q = 1; q < g.size(); ++q)
-                if (idx[g[q]] + sh[g[q]] <= idx[g[q - 1]] + sh[g[q - 1]]) ok = false;
+                if (idx[g[q]] <= idx[g[q - 1]]) ok = false;
+        for (auto &f : fl) {
+            bool hit = false;
+            for (size_t q = 0; q < f.pos.size(); ++q)
+                hit = hit || (idx[f.pos[q]] >= f.lo[q] && idx[f.pos[q]] < f.hi[q]);
+            if (hit != f.any) ok = false;
+        }
         if (ok) {
             long long ox = 0, oy = 0;
             for (size_t d = 0; d < nd; ++d) {
@@ -448,24 +504,19 @@ void build_table(const std::vector<std::string> &labels, const std::map<std::str
 // occupied labels hold an active index and whose virtual labels hold one: a set
 // that every permutation of the labels keeps, so the assemble's permuted and
 // sorted reads of an active triple stay inside it.  Each GETT that writes such a
-// Z is replaced by GETTs over a disjoint cover of that set by rectangles (on
-// each side: the first k-1 labels inactive, the k-th active, the rest free),
-// whose views take the labels' sub-ranges.  Labels of a restriction group keep
-// their order by comparing full-range values (Op::lshift).
+// Z keeps only those elements through filters on its output offset tables.  The
+// labels of one kind (occupied or virtual) may sit in both output modes; then
+// "some label active" is the disjoint union of "some M label active" and "no M
+// label active, some N label active", so a contraction becomes at most four
+// GETTs (usually one or two), each with filtered M and N tables.
 // ---------------------------------------------------------------------------
 struct ActiveSpace {
     long long occ_lo = 0;          // occupied index (from froz) >= occ_lo is active, both spins
     long long vir_hi[2] = {0, 0};  // virtual index (from occ of the spin) < vir_hi[spin] is active
 };
 
-std::string num_token(ccq_b200_ctx *c, long long v) {
-    std::string t = "#" + std::to_string(v);
-    c->size[t] = v;
-    return t;
-}
-
 void restrict_to_active(ccq_b200_ctx *c, const ActiveSpace &as) {
-    std::map<std::string, int> t3z;   // Z buffer -> 1 if read only by T3 Jacobi assembles
+    std::map<std::string, int> t3z;   // Z buffers read only by T3 Jacobi assembles
     for (auto &o : c->plan.ops)
         if (o.kind == OP_ASM && o.block.size() == 3 && o.block[1] == '3' && o.mode == "jacobi")
             for (auto &t : o.terms)
@@ -479,42 +530,10 @@ void restrict_to_active(ccq_b200_ctx *c, const ActiveSpace &as) {
             for (auto &t : o.terms) t3z.erase(t.second.buf);
     }
     const long long full_o[2] = {c->oa, c->ob}, full_v[2] = {c->va, c->vb};
-    struct Lab {
-        std::string name;
-        int spin;
-        bool occ;
-    };
-    // (label, start, extent) assignments of one side's rectangles
-    using Rect = std::vector<std::pair<std::string, std::pair<long long, long long>>>;
-    auto side_rects = [&](std::vector<Lab> labs, const std::vector<std::vector<std::string>> &groups, bool occ) {
-        // a restriction group (increasing values) contributes its largest occupied / smallest virtual
-        // label first: once that one is inactive, so are the others
-        auto rank = [&](const std::string &l) {
-            for (auto &g : groups)
-                for (size_t q = 0; q < g.size(); ++q)
-                    if (g[q] == l) return occ ? -(long long)q : (long long)q;
-            return 0LL;
-        };
-        std::stable_sort(labs.begin(), labs.end(), [&](const Lab &a, const Lab &b) { return rank(a.name) < rank(b.name); });
-        std::vector<Rect> out;
-        for (size_t k = 0; k < labs.size(); ++k) {
-            Rect r;
-            bool empty = false;
-            for (size_t j = 0; j <= k; ++j) {
-                const Lab &l = labs[j];
-                long long n = occ ? full_o[l.spin] : full_v[l.spin];
-                long long cut = occ ? std::min(std::max(as.occ_lo, 0LL), n)
-                                    : std::min(std::max(as.vir_hi[l.spin], 0LL), n);
-                // occupied: inactive [0, cut), active [cut, n); virtual: active [0, cut), inactive [cut, n)
-                bool active = j == k;
-                long long lo = occ ? (active ? cut : 0) : (active ? 0 : cut);
-                long long hi = occ ? (active ? n : cut) : (active ? cut : n);
-                if (hi <= lo) empty = true;
-                r.push_back({l.name, {lo, hi - lo}});
-            }
-            if (!empty) out.push_back(r);
-        }
-        return out;
+    auto has_label = [](const ViewSpec &v, const std::string &l) {
+        for (auto &ax : v.axes)
+            if (ax.label == l) return true;
+        return false;
     };
     std::vector<Op> ops;
     for (auto &o : c->plan.ops) {
@@ -522,34 +541,56 @@ void restrict_to_active(ccq_b200_ctx *c, const ActiveSpace &as) {
             ops.push_back(o);
             continue;
         }
-        std::vector<Lab> occ, vir;
+        // output labels by kind and index mode, with their active ranges
+        struct L {
+            std::string name;
+            long long lo, hi;
+        };
+        std::vector<L> side[2][2];   // [occ/vir][M/N]
         bool ok = true;
         for (auto &ax : o.c.axes) {
             const std::string &z = ax.size;
-            if (z == "oa" || z == "ob") occ.push_back({ax.label, z == "ob", true});
-            else if (z == "va" || z == "vb") vir.push_back({ax.label, z == "vb", false});
-            else ok = false;
+            const int mode = has_label(o.a, ax.label) ? 0 : 1;
+            if (z == "oa" || z == "ob") {
+                const long long n = full_o[z == "ob"];
+                side[0][mode].push_back({ax.label, std::min(as.occ_lo, n), n});
+            } else if (z == "va" || z == "vb") {
+                side[1][mode].push_back({ax.label, 0, std::min(as.vir_hi[z == "vb"], full_v[z == "vb"])});
+            } else {
+                ok = false;
+            }
         }
-        if (!ok || occ.empty() || vir.empty()) {
+        if (!ok || (side[0][0].empty() && side[0][1].empty()) || (side[1][0].empty() && side[1][1].empty())) {
             ops.push_back(o);
             continue;
         }
-        auto ro = side_rects(occ, o.restrict_groups, true), rv = side_rects(vir, o.restrict_groups, false);
-        for (auto &a : ro)
-            for (auto &b : rv) {
+        auto filt = [](int mode, bool any, const std::vector<L> &ls) {
+            Op::ModeFilter f;
+            f.mode = mode;
+            f.any = any;
+            for (auto &l : ls) {
+                f.labels.push_back(l.name);
+                f.lo.push_back(l.lo);
+                f.hi.push_back(l.hi);
+            }
+            return f;
+        };
+        // the pieces of one kind: lists of filters whose conjunction is a disjoint part of "some active"
+        auto pieces = [&](const std::vector<L> *sd) {
+            std::vector<std::vector<Op::ModeFilter>> out;
+            if (sd[1].empty()) out.push_back({filt(0, true, sd[0])});
+            else if (sd[0].empty()) out.push_back({filt(1, true, sd[1])});
+            else {
+                out.push_back({filt(0, true, sd[0])});
+                out.push_back({filt(0, false, sd[0]), filt(1, true, sd[1])});
+            }
+            return out;
+        };
+        for (auto &po : pieces(side[0]))
+            for (auto &pv : pieces(side[1])) {
                 Op q = o;
-                Rect r = a;
-                r.insert(r.end(), b.begin(), b.end());
-                for (auto &lr : r) {
-                    const long long lo = lr.second.first, ext = lr.second.second;
-                    for (ViewSpec *v : {&q.c, &q.a, &q.b})
-                        for (auto &ax : v->axes)
-                            if (ax.label == lr.first) {
-                                ax.start = num_token(c, tok(c, ax.start) + lo);
-                                ax.size = num_token(c, ext);
-                            }
-                    if (lo) q.lshift[lr.first] = lo;
-                }
+                q.filters = po;
+                q.filters.insert(q.filters.end(), pv.begin(), pv.end());
                 ops.push_back(q);
             }
     }
@@ -603,6 +644,12 @@ void instantiate(ccq_b200_ctx *c) {
     c->t_size = off;
     // CR-CC(2,3) solves CCSD; its DIIS vector is T1 + T2 (the T3 slots stay zero)
     c->vec_size = (c->calc_type == "CCSD" || c->calc_type == "CR-CC(2,3)") ? tv_off["T3A"] : c->t_size;
+    if (c->cdiis) {
+        if (c->geom.t12 != tv_off["T3A"] || c->geom.t3_end != c->t_size)
+            throw Error(CCQ_B200_EPLAN, "CCSDt layout does not match the plan's T vector");
+        c->vec_size = c->geom.t12 + c->geom.n_act;
+        c->cvec = (double *)c->dalloc(sizeof(double) * std::max(c->vec_size, 1LL));
+    }
     c->vec_full = c->vec_size;
     c->vec_t12 = tv_off["T3A"];
     // left amplitudes (L1A..L2C) share the T1/T2 layout in their own vector
@@ -855,13 +902,14 @@ void instantiate(ccq_b200_ctx *c) {
                     throw Error(CCQ_B200_EPLAN, "restriction group spans index modes");
                 }
                 for (auto &l : g)
-                    if (ext[l] != ext[g[0]] && o.lshift.empty())
-                        throw Error(CCQ_B200_EPLAN, "restriction group with unequal extents");
+                    if (ext[l] != ext[g[0]]) throw Error(CCQ_B200_EPLAN, "restriction group with unequal extents");
             }
             std::vector<int> am, ak, bn, bk, cm, cn;
-            build_table(ml, ext, A, &C, o.restrict_groups, o.lshift, am, cm);
-            build_table(kl, ext, A, &B, o.restrict_groups, o.lshift, ak, bk);
-            build_table(nl, ext, B, &C, o.restrict_groups, o.lshift, bn, cn);
+            std::vector<const Op::ModeFilter *> fm, fn;
+            for (auto &f : o.filters) (f.mode == 0 ? fm : fn).push_back(&f);
+            build_table(ml, ext, A, &C, o.restrict_groups, fm, am, cm);
+            build_table(kl, ext, A, &B, o.restrict_groups, {}, ak, bk);
+            build_table(nl, ext, B, &C, o.restrict_groups, fn, bn, cn);
             o.hcm = cm;
             o.hcn = cn;
             if (ml.empty()) { am.assign(1, 0); cm.assign(1, 0); }
@@ -1098,6 +1146,9 @@ void instantiate(ccq_b200_ctx *c) {
         o.g.offC_m = dtab + p.cm;
         o.g.offC_n = dtab + p.cn;
     }
+    if (c->trace_init)
+        fprintf(stderr, "ccq_b200_init table entries %zu, ops %zu, assemble terms %zu\n", itab.size(),
+                c->plan.ops.size(), hterms.size());
     trace_stamp(c, "op tables");
     // Group small-K contractions that add into the same Z view (consecutive writers
     // of that Z within one block phase, identical output tables): one launch per
@@ -1652,6 +1703,8 @@ static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const dou
             restrict_to_active(c, as);
             c->act_occ_b = act_occ_b;
             c->act_unocc_a = act_unocc_a;
+            t3act_geometry(fr, dims->occ_a, dims->occ_b, dims->orbs, act_occ_b, act_unocc_a, c->geom);
+            c->cdiis = true;
         }
         stamp("parse");
         // host-side integral preparation
@@ -2060,7 +2113,14 @@ static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
         return q == 0 ? ds + 1 : q;
     };
     double *cur = c->ring + (slot(iter) - 1) * vs;
-    CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
+    const bool packed = c->cdiis && vs > c->vec_t12;   // CCSDt's compressed DIIS vector (not while T3 is held)
+    if (packed) {
+        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * c->vec_t12, cudaMemcpyDeviceToDevice, c->stream));
+        launch_t3act_gather(c->geom, c->tvec, cur + c->vec_t12, c->stream);
+        c->launches += 1;
+    } else {
+        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
+    }
     const double *prev = iter == 1 ? nullptr : c->ring + (slot(iter - 1) - 1) * vs;
     launch_sqdiff(prev, cur, vs, c->scratch, c->stream);
     c->launches += 1;
@@ -2068,7 +2128,14 @@ static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
     if (diis) {
         launch_diis_gram(c->ring, vs, ds, vs, c->scratch + 8, c->stream);
         launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
-        launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
+        if (packed) {
+            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->cvec, c->stream);
+            CK(cudaMemcpyAsync(c->tvec, c->cvec, sizeof(double) * c->vec_t12, cudaMemcpyDeviceToDevice, c->stream));
+            launch_t3act_scatter(c->geom, c->cvec + c->vec_t12, c->tvec, c->stream);
+            c->launches += 2;
+        } else {
+            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
+        }
         c->launches += 3;
         // the extrapolation rewrote T1 .. T3: the host copy is taken again
         if (c->host_out)

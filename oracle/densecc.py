@@ -94,8 +94,20 @@ class DenseCC:
         ts = self.so.from_blocks({k: v for k, v in blocks.items() if int(k[1]) <= 2}, 2)
         return self.so.energy(ts)
 
-    def solve(self, diis_space=5, max_iter=60, tol=1e-8, log=None, t0=None):
+    def solve(self, diis_space=5, max_iter=60, tol=1e-8, log=None, t0=None, compressed_diis=False):
+        """compressed_diis (with an active space): DIIS over ccq's compressed CCSDt T vector, as ccq runs
+        CCSDt (its t_vec is get_t_sizes_act's)."""
         tvec = np.zeros(self.layout.t_size) if t0 is None else np.array(t0, dtype=np.float64)
         vs = self.layout.vec_size('CCSD' if self.external else self.method)
-        e, it, failed, hist = S.jacobi_iter(self.update, self.energy, tvec, vs, diis_space, max_iter, tol, log)
+        pack = unpack = None
+        if compressed_diis:
+            from oracle import ccsdt_layout as CL
+            d = self.dims
+            dims = (d.froz, d.occ_a, d.occ_b, d.orbs)
+            m1, m2 = self.active
+            pack = lambda t: CL.compress(t, dims, m1, m2)  # noqa: E731
+            unpack = lambda v: CL.expand(v, dims, m1, m2)  # noqa: E731
+            vs = CL.pos_offsets(*dims, m1, m2)[-1] - 1
+        e, it, failed, hist = S.jacobi_iter(self.update, self.energy, tvec, vs, diis_space, max_iter, tol, log,
+                                            pack, unpack)
         return e, it, failed, hist, tvec

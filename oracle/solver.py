@@ -179,9 +179,13 @@ class Ring:
         return out
 
 
-def jacobi_iter(update, energy, tvec, vec_size, diis_space=5, max_iter=60, tol=1e-4, log=None):
+def jacobi_iter(update, energy, tvec, vec_size, diis_space=5, max_iter=60, tol=1e-4, log=None, pack=None,
+                unpack=None):
     """Fixed-point loop of ccq.  ``update(tvec)`` updates in place.
 
+    ``pack(tvec)`` / ``unpack(vec)`` (optional) map the T vector to the DIIS vector and back: for
+    active-space CCSDt, ccq's t_vec is the compressed one of get_t_sizes_act
+    (src/utils/cc_utils.f90:560-630), over which its ring, residuum and extrapolation run.
     Returns (e_cor, iterations, failed, history[(e, de, res)]).
     """
     conv = [1.0, 1.0, 1.0]
@@ -196,10 +200,13 @@ def jacobi_iter(update, energy, tvec, vec_size, diis_space=5, max_iter=60, tol=1
         diff = en_cor - e_new
         conv = [conv[1], conv[2], diff]
         en_cor = e_new
-        ring.write(it, tvec)
+        ring.write(it, tvec if pack is None else pack(tvec))
         res = ring.residuum(it)
         if it % (diis_space + 1) == 0:
-            tvec[:vec_size] = ring.diis()
+            if unpack is None:
+                tvec[:vec_size] = ring.diis()
+            else:
+                tvec[:] = unpack(ring.diis())
         hist.append((e_new, diff, res))
         if log:
             log(f"  {it:4d}{e_new:15.10f}{diff:15.10f}{res:15.10f}")

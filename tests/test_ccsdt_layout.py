@@ -72,3 +72,21 @@ def test_bad_arguments():
         lib.t_size_act(*dims, 5, 6)      # act_occ_b above occ_b
     with pytest.raises(lib.CCQB200Error):
         lib.t_compress(dims, 2, 6, np.zeros(7))
+
+
+def test_compressed_diis_of_the_oracle():
+    """DIIS over ccq's compressed vector: with every orbital active the compressed vector is the full one
+    (the same solve); with a partial active space the solve reaches the masked full-DIIS energy."""
+    from oracle.densecc import DenseCC
+    from tests.helpers import random_system
+    s = random_system(5, 3, 2, seed=29, sigma=0.08)
+    d = s['dims']
+    cc = lambda act: DenseCC(s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d, 'CCSDT', active=act)  # noqa
+    full = (d.froz, d.orbs)
+    e1, it1, f1, _, _ = cc(full).solve(tol=1e-10, max_iter=100)
+    e2, it2, f2, _, _ = cc(full).solve(tol=1e-10, max_iter=100, compressed_diis=True)
+    assert not f1 and not f2 and it1 == it2 and abs(e1 - e2) < 1e-12
+    act = (d.occ_b - 1, d.occ_a + 1)
+    e3, _, f3, _, _ = cc(act).solve(tol=1e-10, max_iter=100)
+    e4, _, f4, _, _ = cc(act).solve(tol=1e-10, max_iter=100, compressed_diis=True)
+    assert not f3 and not f4 and abs(e3 - e4) < 1e-9

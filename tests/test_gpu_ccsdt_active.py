@@ -52,7 +52,7 @@ def test_ccsdt_input_deck(tmp_path, h4):
                                      'max_iterations=100\nkeep_bin=.false.\n')
     r = driver.run(str(tmp_path / 'in.inp'), out=lambda x: None, base_dir=str(tmp_path))
     dc = DenseCC(h4['f_a'], h4['f_b'], h4['v_aa'], h4['v_ab'], h4['v_bb'], h4['dims'], 'CCSDT', active=(1, 3))
-    e, it, failed, _, _ = dc.solve(tol=1e-11, max_iter=100)
+    e, it, failed, _, _ = dc.solve(tol=1e-11, max_iter=100, compressed_diis=True)
     assert not r.failed and r.iterations == it and abs(r.e_cor - e) < 1e-10
 
 
@@ -62,12 +62,13 @@ def _ctx_restricted(s, act, rhf=False):
                        rhf=rhf, active=act)
 
 
-@pytest.mark.parametrize('n,oa,ob,froz,act_d', [(8, 4, 3, 0, (1, 2)), (8, 4, 4, 1, (1, 3)), (9, 4, 3, 0, (2, 1)),
-                                                 (7, 3, 2, 0, (0, 2))])
-def test_restricted_ccsdt_matches_oracle(n, oa, ob, froz, act_d):
-    """calc_type CCSDt: the T3 residual contractions run over the active triples' ranges only; sweeps,
-    converged energies and iteration counts equal the masked dense oracle's, at a fraction of the FLOPs."""
-    s = random_system(n, oa, ob, seed=31, sigma=0.08, froz=froz)
+@pytest.mark.parametrize('n,oa,ob,froz,act_d,seed', [(8, 4, 3, 0, (1, 2), 29), (8, 4, 4, 1, (1, 3), 37),
+                                                      (9, 4, 3, 0, (2, 1), 29), (7, 3, 2, 0, (0, 2), 29)])
+def test_restricted_ccsdt_matches_oracle(n, oa, ob, froz, act_d, seed):
+    """calc_type CCSDt: the T3 residual contractions run over the active triples only, and DIIS runs over
+    ccq's compressed T vector; sweeps, converged energies and iteration counts equal the dense oracle's
+    with the same mask and the same DIIS vector, at a fraction of the FLOPs."""
+    s = random_system(n, oa, ob, seed=seed, sigma=0.08, froz=froz)
     d = s['dims']
     act = (d.occ_b - act_d[0], d.occ_a + act_d[1])
     ctx = _ctx_restricted(s, act)
@@ -94,11 +95,14 @@ def test_restricted_ccsdt_matches_oracle(n, oa, ob, froz, act_d):
     ctx = _ctx_restricted(s, act)
     cfg = config.Config(calc_type='CCSDT', tol=1e-10, max_iter=200).calc_macros()
     r = driver.solve_cc(ctx, cfg, out=lambda x: None)
+    assert ctx.vec_size == lib.t_size_act(d.froz, d.occ_a, d.occ_b, d.orbs, *act)
     ctx.close()
-    e, it, failed, _, _ = DenseCC(s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d, 'CCSDT',
-                                  active=act).solve(tol=1e-10, max_iter=200)
+    e, it, failed, hist, _ = DenseCC(s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d, 'CCSDT',
+                                     active=act).solve(tol=1e-10, max_iter=200, compressed_diis=True)
     assert not r.failed and not failed
     assert r.iterations == it and abs(r.e_cor - e) < 1e-10
+    for k in range(min(8, it)):
+        assert abs(r.history[k]['e'] - hist[k][0]) < 1e-11, k
 
 
 def test_restricted_ccsdt_rhf_and_compressed_layout():
@@ -112,7 +116,7 @@ def test_restricted_ccsdt_rhf_and_compressed_layout():
     t = ctx.get_t()
     ctx.close()
     e, it, failed, _, _ = DenseCC(s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d, 'CCSDT', rhf=True,
-                                  active=act).solve(tol=1e-10, max_iter=200)
+                                  active=act).solve(tol=1e-10, max_iter=200, compressed_diis=True)
     assert not r.failed and r.iterations == it and abs(r.e_cor - e) < 1e-10
     dims = (d.froz, d.occ_a, d.occ_b, d.orbs)
     c = lib.t_compress(dims, *act, t)

@@ -108,7 +108,7 @@ def test_partial_active_space_matches_dense(tmp_path):
     act = (2, 5)
     d = s['dims']
     cc = DenseCC(s['f_a'], s['f_b'], s['v_aa'], s['v_ab'], s['v_bb'], d, 'CCSDT', active=act)
-    e, it, failed, _, tvec = cc.solve(tol=1e-11, max_iter=200)
+    e, it, failed, _, tvec = cc.solve(tol=1e-11, max_iter=200, compressed_diis=True)
     dc = DenseCRCC(cc, tvec, e)
     dc.solve_left(tol=1e-11, max_iter=200)
     ref = dc.energies(active=act)
