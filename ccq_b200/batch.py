@@ -82,6 +82,10 @@ class Instance:
     def step_finish(self, tol, max_iter):
         e_new, res, did = self.ctx.iterate_wait()
         self.device_ms += self.ctx.timing()[1]
+        self.record(e_new, tol, max_iter)
+
+    def record(self, e_new, tol, max_iter):
+        """jacobi_iter's bookkeeping after iteration self.it: convergence, NaN and max_iter exits."""
         diff = self.e - e_new
         self.conv = [self.conv[1], self.conv[2], diff]
         self.e = e_new
@@ -118,20 +122,22 @@ def create_instances(specs, calc_type='CCSD', diis_space=5, graph=True, threads=
 
 
 def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, graph=True, t_init=None,
-                keep_t=False, chunk=None):
+                keep_t=False, chunk=None, grouped=False):
     """Solve every instance; returns (results, timings).
 
     ``results[i]`` = dict(e_cor, iterations, failed, device_ms) (plus ``t``, the
     converged t_vec, with ``keep_t``); ``t_init[i]`` (a t_vec) replaces the
     T = 0 start of instance i.  Timings: wall seconds of context creation and
     of the iterations.  ``chunk`` bounds the number of contexts alive at once
-    (the instances are solved in consecutive groups of that size).
+    (the instances are solved in consecutive groups of that size).  ``grouped``:
+    the instances iterate as one batch (``lib.Batch``): each plan operation of
+    every active instance runs in one launch, then each instance's DIIS step.
     """
     if chunk and len(specs) > chunk:
         res, tim = [], {'setup_s': 0.0, 'solve_s': 0.0}
         for k in range(0, len(specs), chunk):
             r, t = solve_batch(specs[k:k + chunk], tol, max_iter, calc_type, diis_space, graph,
-                               None if t_init is None else t_init[k:k + chunk], keep_t)
+                               None if t_init is None else t_init[k:k + chunk], keep_t, grouped=grouped)
             res += r
             tim['setup_s'] += t['setup_s']
             tim['solve_s'] += t['solve_s']
@@ -143,8 +149,22 @@ def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, g
             if t is not None:
                 x.ctx.set_t(t)
     t1 = time.perf_counter()
+    bt = None
     try:
         active = list(insts)
+        if grouped:
+            bt = lib.Batch([x.ctx for x in insts])
+            it = 0
+            while active:
+                it += 1
+                e, _, _ = bt.iterate(it, [0 if x.done else 1 for x in insts])
+                ms = bt.stats()['sweep_ms'] / len(active)
+                for j, x in enumerate(insts):
+                    if not x.done:
+                        x.it = it
+                        x.device_ms += ms
+                        x.record(float(e[j]), tol, max_iter)
+                active = [x for x in active if not x.done]
         while active:
             for x in active:
                 x.step_launch()
@@ -158,6 +178,8 @@ def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, g
             for r, x in zip(res, insts):
                 r['t'] = x.ctx.get_t()
     finally:
+        if bt is not None:
+            bt.close()
         for x in insts:
             x.close()
     return res, {'setup_s': t1 - t0, 'solve_s': t2 - t1}

@@ -172,8 +172,9 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As
     }
 }
 
+// One 64 x 64 output tile (bx, by) of a GETT, K slice bz; split: several K slices add into C.
 template <bool AK, bool BKM, bool GROUPED, int NST>
-__global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
+__device__ __forceinline__ void gett_f64_tile(const GettArgs &g, int bx, int by, int bz, bool split) {
     extern __shared__ __align__(16) double smem[];
     double *As = smem;
     double *Bs = smem + NST * TILE;
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     const int gid = lane >> 2, tig = lane & 3;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int m0 = bx * BM, n0 = by * BN;
 
     double acc[2][4][4];
 #pragma unroll
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
             alpha = sg.alpha;
         }
     } else {
-        const int kbeg = blockIdx.z * g.kchunk;
+        const int kbeg = bz * g.kchunk;
         const int kend = min(g.K, kbeg + g.kchunk);
         gett_mainloop<AK, BKM, NST>(acc, As, Bs, g.A, g.B, g.offA_m, g.offA_k, g.offB_n, g.offB_k, g.M, g.N, m0, n0, kbeg,
                                kend, tid, wm, wn, gid, tig, g.vec_a != 0, g.vec_b != 0);
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
     // split-K slices and beta = 1 updates add into C with fire-and-forget reductions
     // (one add per element and slice: the same rounding as a read-add-write, with no
     // dependent read in the epilogue)
-    const bool atomic = gridDim.z > 1 || g.beta;
+    const bool atomic = split || g.beta;
     if (g.vec_c && !atomic) {
         // output pairs along the fast mode are contiguous and 16-byte aligned
         const int fast = 2 * (tid & 31), slow0 = tid >> 5;
@@ -293,6 +294,74 @@ __global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
                 if (cp[u]) *cp[u] = old[u] + cv[u];
         }
     }
+}
+
+template <bool AK, bool BKM, bool GROUPED, int NST>
+__global__ void __launch_bounds__(128) gett_f64_kernel(GettArgs g) {
+    gett_f64_tile<AK, BKM, GROUPED, NST>(g, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z > 1);
+}
+
+// Many GETTs of the same operand orientation in one launch (one per context of a batch of
+// independent solves): block b runs tile b - tstart[i] of GETT i, where tstart[i] <= b < tstart[i + 1]
+// (64 x 64 tiles, the whole K range, no split-K).  GETT i is skipped when active[owner[i]] is zero.
+template <bool AK, bool BKM, int NST>
+__global__ void __launch_bounds__(128) gett_f64_batched_kernel(const GettArgs *__restrict__ args,
+                                                               const int *__restrict__ tstart, int n,
+                                                               const int *__restrict__ owner,
+                                                               const int *__restrict__ active) {
+    const int b = blockIdx.x;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(tstart + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    if (!__ldg(active + __ldg(owner + lo))) return;
+    const GettArgs &g = args[lo];
+    const int t = b - __ldg(tstart + lo);
+    const int tm = (g.M + BM - 1) / BM, tn = (g.N + BN - 1) / BN;
+    if (g.nseg > 0) {
+        gett_f64_tile<AK, BKM, true, NST>(g, t % tm, (t / tm) % tn, 0, false);
+    } else {
+        // split-K slices (kchunk of the context's own launch) add into C, zeroed beforehand
+        const int nz = (g.K + g.kchunk - 1) / g.kchunk;
+        gett_f64_tile<AK, BKM, false, NST>(g, t % tm, (t / tm) % tn, t / (tm * tn), nz > 1);
+    }
+}
+
+// the output views of many GETTs set to zero (before their split-K slices add into them)
+__global__ void zero_views_batched_kernel(const GettArgs *__restrict__ args, int n, const int *__restrict__ owner,
+                                          const int *__restrict__ active) {
+    for (int i = blockIdx.y; i < n; i += gridDim.y) {
+        if (!__ldg(active + __ldg(owner + i))) continue;
+        const GettArgs &g = args[i];
+        const long long total = (long long)g.M * g.N;
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+             e += (long long)gridDim.x * blockDim.x) {
+            const int m = (int)(e / g.N), nn = (int)(e % g.N);
+            g.C[(long long)__ldg(g.offC_m + m) + __ldg(g.offC_n + nn)] = 0.0;
+        }
+    }
+}
+
+void launch_zero_views_batched(const GettArgs *args, int n, const int *owner, const int *active, cudaStream_t s) {
+    if (n <= 0) return;
+    dim3 grid(64, (unsigned)std::min(n, 65535));
+    zero_views_batched_kernel<<<grid, 256, 0, s>>>(args, n, owner, active);
+}
+
+void launch_gett_f64_batched(const GettArgs *args, const int *tstart, int n, int tiles, const int *owner,
+                             const int *active, int a_kmajor, int b_kmajor, cudaStream_t s) {
+    if (n <= 0 || tiles <= 0) return;
+    constexpr size_t sm = sizeof(double) * 2 * 2 * TILE;
+    if (a_kmajor && b_kmajor)
+        gett_f64_batched_kernel<true, true, 2><<<tiles, 128, sm, s>>>(args, tstart, n, owner, active);
+    else if (a_kmajor)
+        gett_f64_batched_kernel<true, false, 2><<<tiles, 128, sm, s>>>(args, tstart, n, owner, active);
+    else if (b_kmajor)
+        gett_f64_batched_kernel<false, true, 2><<<tiles, 128, sm, s>>>(args, tstart, n, owner, active);
+    else
+        gett_f64_batched_kernel<false, false, 2><<<tiles, 128, sm, s>>>(args, tstart, n, owner, active);
 }
 
 template <bool G, int NST>
@@ -925,14 +994,13 @@ __device__ __forceinline__ void canonical_element(const AsmArgs &a, Off lin, int
 }
 
 // Off: index type of every offset (int when AsmArgs::off32 says they all fit)
-template <int RK, typename Off>
-__global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
-    constexpr int CH = 128;
-    __shared__ SmTerm<RK> st[CH];
+// The canonical elements [base0, total) of one assemble, blockDim.x * ASM_EPT of them per step.
+template <int RK, typename Off, int CH>
+__device__ __forceinline__ void assemble_body(const AsmArgs &a, SmTerm<RK> (&st)[CH], long long base0,
+                                              long long step) {
     const int nch = (a.nterms + CH - 1) / CH;
     double nacc = 0.0;
-    const long long step = (long long)gridDim.x * blockDim.x * ASM_EPT;
-    for (long long base = (long long)blockIdx.x * blockDim.x * ASM_EPT; base < a.total; base += step) {
+    for (long long base = base0; base < a.total; base += step) {
         int x[ASM_EPT][RK];
         bool act[ASM_EPT];    // an element of the block
         bool need[ASM_EPT];   // ... whose residual is gathered (inside the active space when one is set)
@@ -1085,6 +1153,70 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
         for (int o = 16; o > 0; o >>= 1) nacc += __shfl_down_sync(0xffffffffu, nacc, o);
         if ((threadIdx.x & 31) == 0 && nacc != 0.0) atomicAdd(a.norm, nacc);
     }
+}
+
+template <int RK, typename Off>
+__global__ void __launch_bounds__(256, 4) assemble_kernel(AsmArgs a) {
+    constexpr int CH = 128;
+    __shared__ SmTerm<RK> st[CH];
+    assemble_body<RK, Off, CH>(a, st, (long long)blockIdx.x * blockDim.x * ASM_EPT,
+                               (long long)gridDim.x * blockDim.x * ASM_EPT);
+}
+
+// Many assembles of the same rank in one launch (one per context of a batch of independent
+// solves): block b handles the chunk b - cstart[i] (256 * ASM_EPT canonical elements) of assemble
+// i, where cstart[i] <= b < cstart[i + 1]; assemble i is skipped when active[owner[i]] is zero.
+template <int RK>
+__global__ void __launch_bounds__(256, 4) assemble_batched_kernel(const AsmArgs *__restrict__ args,
+                                                                  const long long *__restrict__ cstart, int n,
+                                                                  const int *__restrict__ owner,
+                                                                  const int *__restrict__ active) {
+    constexpr int CH = 128;
+    __shared__ SmTerm<RK> st[CH];
+    const long long b = blockIdx.x;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(cstart + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    if (!__ldg(active + __ldg(owner + lo))) return;
+    const AsmArgs &a = args[lo];
+    const long long base = (b - __ldg(cstart + lo)) * blockDim.x * ASM_EPT;
+    const long long step = a.total + 1;   // one chunk per block
+    if (a.off32) assemble_body<RK, int, CH>(a, st, base, step);
+    else assemble_body<RK, long long, CH>(a, st, base, step);
+}
+
+void launch_assemble_batched(const AsmArgs *args, const long long *cstart, int n, long long chunks, int rank,
+                             const int *owner, const int *active, cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    switch (rank) {
+        case 2: assemble_batched_kernel<2><<<(unsigned)chunks, 256, 0, s>>>(args, cstart, n, owner, active); break;
+        case 4: assemble_batched_kernel<4><<<(unsigned)chunks, 256, 0, s>>>(args, cstart, n, owner, active); break;
+        case 6: assemble_batched_kernel<6><<<(unsigned)chunks, 256, 0, s>>>(args, cstart, n, owner, active); break;
+        case 8: assemble_batched_kernel<8><<<(unsigned)chunks, 256, 0, s>>>(args, cstart, n, owner, active); break;
+        default: break;
+    }
+}
+
+// Buffer copies (n doubles, src -> dst) and zeroing (src null) of many contexts in one launch;
+// entry i belongs to context owner[i] and is skipped when active[owner[i]] is zero.
+__global__ void copy_batched_kernel(const BatchCopy *__restrict__ cp, int n, const int *__restrict__ owner,
+                                    const int *__restrict__ active) {
+    for (int i = blockIdx.y; i < n; i += gridDim.y) {
+        if (!__ldg(active + __ldg(owner + i))) continue;
+        const BatchCopy c = cp[i];
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+             e += (long long)gridDim.x * blockDim.x)
+            c.dst[e] = c.src ? __ldg(c.src + e) : 0.0;
+    }
+}
+
+void launch_copy_batched(const BatchCopy *cp, int n, const int *owner, const int *active, cudaStream_t s) {
+    if (n <= 0) return;
+    dim3 grid(64, (unsigned)std::min(n, 65535));
+    copy_batched_kernel<<<grid, 256, 0, s>>>(cp, n, owner, active);
 }
 
 void launch_assemble(const AsmArgs &a, cudaStream_t s) {

@@ -120,6 +120,24 @@ cudaError_t preload_kernels(int diis_space);
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s);
 void launch_zero_view(double *C, const int *offm, const int *offn, int M, int N, cudaStream_t s);
 void launch_assemble(const AsmArgs &a, cudaStream_t s);
+
+// Batched launches over the contexts of many independent solves (one plan operation of every
+// context at once).  owner[i] is the context of entry i; entries of contexts with active[owner[i]]
+// zero do nothing.  GETTs: 64 x 64 tiles, split into K slices of the entry's kchunk (slices add into
+// C atomically: zero it first), tstart[i] = first tile of entry i (tiles = all tiles); assembles: cstart[i] = first chunk of ASM_CHUNK canonical elements of entry i.
+struct BatchCopy {
+    double *dst;
+    const double *src;   // null: zero dst
+    long long n;
+};
+constexpr int ASM_CHUNK = 512;   // canonical elements per block of a batched assemble (256 threads x 2)
+void launch_gett_f64_batched(const GettArgs *args, const int *tstart, int n, int tiles, const int *owner,
+                             const int *active, int a_kmajor, int b_kmajor, cudaStream_t s);
+void launch_assemble_batched(const AsmArgs *args, const long long *cstart, int n, long long chunks, int rank,
+                             const int *owner, const int *active, cudaStream_t s);
+void launch_copy_batched(const BatchCopy *cp, int n, const int *owner, const int *active, cudaStream_t s);
+// zero the output views of the entries (before split-K slices add into them)
+void launch_zero_views_batched(const GettArgs *args, int n, const int *owner, const int *active, cudaStream_t s);
 void launch_fill(double *p, double v, long long n, cudaStream_t s);
 void launch_f2c4(const double *f, double *out, long long n, cudaStream_t s);
 void launch_sqdiff(const double *a, const double *b, long long n, double *out, cudaStream_t s);

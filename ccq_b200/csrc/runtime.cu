@@ -2099,13 +2099,9 @@ int ccq_b200_energy(ccq_b200_ctx *c, double *e) {
 // write, the residuum and (on schedule) DIIS, and copies the results to pinned
 // host slots; the finish waits for them.  Many contexts on their own streams
 // can be launched before any is waited for.
-static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
-    CK(cudaSetDevice(c->device));
-    c->launches = 0;
-    CK(cudaEventRecord(c->ev0, c->stream));
-    sweep(c);
-    CK(cudaEventRecord(c->ev1, c->stream));
-    c->launches = count_sweep_launches(c);
+// After the sweep of iteration iter: the DIIS ring write, residuum, the extrapolation every
+// diis_space + 1 iterations, and the energy / residuum / DIIS status copied to the pinned slots.
+static void post_sweep(ccq_b200_ctx *c, int64_t iter, cudaStream_t st) {
     const int ds = c->ds;
     const long long vs = c->vec_size;
     auto slot = [&](long long it) {
@@ -2115,37 +2111,47 @@ static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
     double *cur = c->ring + (slot(iter) - 1) * vs;
     const bool packed = c->cdiis && vs > c->vec_t12;   // CCSDt's compressed DIIS vector (not while T3 is held)
     if (packed) {
-        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * c->vec_t12, cudaMemcpyDeviceToDevice, c->stream));
-        launch_t3act_gather(c->geom, c->tvec, cur + c->vec_t12, c->stream);
+        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * c->vec_t12, cudaMemcpyDeviceToDevice, st));
+        launch_t3act_gather(c->geom, c->tvec, cur + c->vec_t12, st);
         c->launches += 1;
     } else {
-        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(cur, c->tvec, sizeof(double) * vs, cudaMemcpyDeviceToDevice, st));
     }
     const double *prev = iter == 1 ? nullptr : c->ring + (slot(iter - 1) - 1) * vs;
-    launch_sqdiff(prev, cur, vs, c->scratch, c->stream);
+    launch_sqdiff(prev, cur, vs, c->scratch, st);
     c->launches += 1;
     const int diis = (iter % (ds + 1)) == 0;
     if (diis) {
-        launch_diis_gram(c->ring, vs, ds, vs, c->scratch + 8, c->stream);
-        launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, c->stream);
+        launch_diis_gram(c->ring, vs, ds, vs, c->scratch + 8, st);
+        launch_diis_solve(c->scratch + 8, ds, c->scratch + 8 + 169, c->dinfo, st);
         if (packed) {
-            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->cvec, c->stream);
-            CK(cudaMemcpyAsync(c->tvec, c->cvec, sizeof(double) * c->vec_t12, cudaMemcpyDeviceToDevice, c->stream));
-            launch_t3act_scatter(c->geom, c->cvec + c->vec_t12, c->tvec, c->stream);
+            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->cvec, st);
+            CK(cudaMemcpyAsync(c->tvec, c->cvec, sizeof(double) * c->vec_t12, cudaMemcpyDeviceToDevice, st));
+            launch_t3act_scatter(c->geom, c->cvec + c->vec_t12, c->tvec, st);
             c->launches += 2;
         } else {
-            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, c->stream);
+            launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, st);
         }
         c->launches += 3;
         // the extrapolation rewrote T1 .. T3: the host copy is taken again
         if (c->host_out)
-            CK(cudaMemcpyAsync(c->host_out, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(c->host_out, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost, st));
     }
-    CK(cudaEventRecord(c->ev2, c->stream));
-    CK(cudaMemcpyAsync(c->hpin, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(c->hpin + 1, c->scratch, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->ev2, st));
+    CK(cudaMemcpyAsync(c->hpin, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->hpin + 1, c->scratch, sizeof(double), cudaMemcpyDeviceToHost, st));
     c->hpin[2] = 0.0;
-    if (diis) CK(cudaMemcpyAsync(c->hpin + 2, c->dinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    if (diis) CK(cudaMemcpyAsync(c->hpin + 2, c->dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+static void iterate_launch(ccq_b200_ctx *c, int64_t iter) {
+    CK(cudaSetDevice(c->device));
+    c->launches = 0;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    sweep(c);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    c->launches = count_sweep_launches(c);
+    post_sweep(c, iter, c->stream);
     c->async_iter = iter;
 }
 
@@ -2690,3 +2696,277 @@ int ccq_b200_free(ccq_b200_ctx *c) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched iterations of many independent contexts (C ABI ccq_b200_batch_*).
+// Every context of a batch runs the same plan (same calc_type, rhf and diis_space, on one device),
+// so operation k of every context is launched together: one GETT launch over the output tiles of
+// all contexts' k-th contraction (64 x 64 tiles, whole K), one assemble launch over all their
+// canonical elements, one launch for their buffer copies.  A device flag per context switches off
+// the contexts that have converged.  Each context keeps its own amplitudes, ring and DIIS; only the
+// per-context DIIS steps after the sweep are launched one context at a time.
+// ---------------------------------------------------------------------------
+struct BatchGett {
+    int akm = 1, bkm = 1, n = 0, tiles = 0;
+    GettArgs *args = nullptr;
+    int *tstart = nullptr, *owner = nullptr;
+    int nzero = 0;                      // entries whose split-K slices need a zeroed output
+    GettArgs *zargs = nullptr;
+    int *zowner = nullptr;
+};
+
+struct BatchStep {
+    std::vector<BatchGett> gett;          // one launch per operand-orientation class
+    int asm_rank = 0, asm_n = 0;
+    long long asm_chunks = 0;
+    AsmArgs *asm_args = nullptr;
+    long long *asm_cstart = nullptr;
+    int *asm_owner = nullptr;
+    int ncopy = 0;
+    BatchCopy *copies = nullptr;
+    int *copy_owner = nullptr;
+    std::vector<std::pair<int, GettArgs>> kzero;   // K = 0 contractions with beta = 0: zero the view
+};
+
+struct ccq_b200_batch {
+    std::vector<ccq_b200_ctx *> ctx;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<BatchStep> steps;
+    int *active_d = nullptr, *active_h = nullptr;
+    std::vector<void *> owned;
+    long long launches = 0;
+    double sweep_ms = 0.0;
+
+    template <typename T>
+    T *upload(const std::vector<T> &h) {
+        void *p = nullptr;
+        CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(h.size(), 1)));
+        owned.push_back(p);
+        if (!h.empty()) CK(cudaMemcpy(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        return static_cast<T *>(p);
+    }
+    ~ccq_b200_batch() {
+        for (void *p : owned) cudaFree(p);
+        if (active_h) cudaFreeHost(active_h);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" int ccq_b200_batch_create(ccq_b200_ctx *const *ctxs, int64_t n, ccq_b200_batch **out) {
+    ccq_b200_batch *b = nullptr;
+    try {
+        if (!ctxs || n < 1 || !out) throw Error(CCQ_B200_EINVAL, "batch_create: bad argument");
+        *out = nullptr;
+        b = new ccq_b200_batch();
+        for (int64_t j = 0; j < n; ++j) {
+            ccq_b200_ctx *c = ctxs[j];
+            if (!c) throw Error(CCQ_B200_EINVAL, "batch_create: null context");
+            const ccq_b200_ctx *c0 = ctxs[0];
+            if (c->device != c0->device || c->calc_type != c0->calc_type || c->rhf != c0->rhf || c->ds != c0->ds ||
+                c->plan.ops.size() != c0->plan.ops.size() || c->cc_end != c0->cc_end)
+                throw Error(CCQ_B200_EINVAL, "batch_create: contexts must share device, calc_type, rhf and diis_space");
+            if (c->cdiis || c->async_iter) throw Error(CCQ_B200_EINVAL, "batch_create: unsupported context state");
+            b->ctx.push_back(c);
+        }
+        b->device = ctxs[0]->device;
+        CK(cudaSetDevice(b->device));
+        CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&b->ev0));
+        CK(cudaEventCreate(&b->ev1));
+        CK(cudaMallocHost(&b->active_h, sizeof(int) * n));
+        std::vector<int> ones(n, 1);
+        b->active_d = b->upload(ones);
+        const ccq_b200_ctx *c0 = ctxs[0];
+        for (size_t i = 0; i < c0->cc_end; ++i) {
+            BatchStep stp;
+            const OpKind kind = c0->plan.ops[i].kind;
+            std::map<std::pair<int, int>, std::vector<std::pair<int, GettArgs>>> cls;
+            std::vector<AsmArgs> aa;
+            std::vector<long long> cs;
+            std::vector<int> aow;
+            std::vector<BatchCopy> cp;
+            std::vector<int> cow;
+            for (int64_t j = 0; j < n; ++j) {
+                ccq_b200_ctx *c = b->ctx[j];
+                const Op &o = c->plan.ops[i];
+                if (o.kind != kind) throw Error(CCQ_B200_EPLAN, "batch_create: plans differ");
+                if (o.frozen) continue;
+                switch (o.kind) {
+                    case OP_GETT: {
+                        if (o.skip || o.g.M == 0 || o.g.N == 0) break;
+                        if (o.g.K == 0) {
+                            if (!o.beta) stp.kzero.push_back({(int)j, o.g});
+                            break;
+                        }
+                        GettArgs g = o.g;
+                        if (g.nseg == 0 && (g.kchunk <= 0 || g.kchunk > g.K)) g.kchunk = g.K;
+                        cls[{o.akm, o.bkm}].push_back({(int)j, g});
+                        break;
+                    }
+                    case OP_ASM: {
+                        if (stp.asm_rank && o.asmargs.rank != stp.asm_rank)
+                            throw Error(CCQ_B200_EPLAN, "batch_create: assemble ranks differ");
+                        stp.asm_rank = o.asmargs.rank;
+                        cs.push_back(stp.asm_chunks);
+                        stp.asm_chunks += (o.asmargs.total + ASM_CHUNK - 1) / ASM_CHUNK;
+                        aa.push_back(o.asmargs);
+                        aow.push_back((int)j);
+                        break;
+                    }
+                    case OP_COPY: {
+                        const DevBuf &d = c->bufs.at(o.arg0), &sbuf = c->bufs.at(o.arg1);
+                        if (d.numel != sbuf.numel) throw Error(CCQ_B200_EPLAN, "COPY size mismatch");
+                        cp.push_back({d.ptr, sbuf.ptr, d.numel});
+                        cow.push_back((int)j);
+                        break;
+                    }
+                    case OP_ZERO: {
+                        const DevBuf &d = c->bufs.at(o.arg0);
+                        cp.push_back({d.ptr, nullptr, std::max(d.numel, 1LL)});
+                        cow.push_back((int)j);
+                        break;
+                    }
+                    case OP_PHASE:
+                        break;
+                    default:
+                        throw Error(CCQ_B200_EPLAN, "batch: plan operation without a batched kernel");
+                }
+            }
+            for (auto &kv : cls) {
+                BatchGett bg;
+                bg.akm = kv.first.first;
+                bg.bkm = kv.first.second;
+                std::vector<GettArgs> args, zargs;
+                std::vector<int> ts, ow, zow;
+                for (auto &e : kv.second) {
+                    const GettArgs &g = e.second;
+                    const long long nz = g.nseg > 0 ? 1 : (g.K + g.kchunk - 1) / g.kchunk;
+                    ts.push_back(bg.tiles);
+                    bg.tiles += (int)(((g.M + 63) / 64) * ((g.N + 63) / 64) * nz);
+                    args.push_back(g);
+                    ow.push_back(e.first);
+                    if (nz > 1 && !g.beta) {
+                        zargs.push_back(g);
+                        zow.push_back(e.first);
+                    }
+                }
+                bg.n = (int)args.size();
+                bg.args = b->upload(args);
+                bg.tstart = b->upload(ts);
+                bg.owner = b->upload(ow);
+                if (!zargs.empty()) {
+                    bg.nzero = (int)zargs.size();
+                    bg.zargs = b->upload(zargs);
+                    bg.zowner = b->upload(zow);
+                }
+                stp.gett.push_back(bg);
+            }
+            if (!aa.empty()) {
+                stp.asm_n = (int)aa.size();
+                stp.asm_args = b->upload(aa);
+                stp.asm_cstart = b->upload(cs);
+                stp.asm_owner = b->upload(aow);
+            }
+            if (!cp.empty()) {
+                stp.ncopy = (int)cp.size();
+                stp.copies = b->upload(cp);
+                stp.copy_owner = b->upload(cow);
+            }
+            b->steps.push_back(std::move(stp));
+        }
+        *out = b;
+        return 0;
+    } catch (const Error &e) {
+        delete b;
+        return fail(e);
+    } catch (const std::exception &e) {
+        delete b;
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+extern "C" int ccq_b200_batch_iterate(ccq_b200_batch *b, int64_t iter, const int64_t *active, double *e_cor, double *res,
+                           int64_t *did_diis) {
+    try {
+        if (!b || iter < 1 || !active) throw Error(CCQ_B200_EINVAL, "batch_iterate: bad argument");
+        CK(cudaSetDevice(b->device));
+        const int n = (int)b->ctx.size();
+        for (int j = 0; j < n; ++j) b->active_h[j] = active[j] ? 1 : 0;
+        CK(cudaMemcpyAsync(b->active_d, b->active_h, sizeof(int) * n, cudaMemcpyHostToDevice, b->stream));
+        CK(cudaEventRecord(b->ev0, b->stream));
+        long long launches = 0;
+        for (auto &stp : b->steps) {
+            for (auto &kz : stp.kzero)
+                if (active[kz.first]) {
+                    launch_zero_view(kz.second.C, kz.second.offC_m, kz.second.offC_n, kz.second.M, kz.second.N,
+                                     b->stream);
+                    ++launches;
+                }
+            for (auto &g : stp.gett) {
+                if (g.nzero) {
+                    launch_zero_views_batched(g.zargs, g.nzero, g.zowner, b->active_d, b->stream);
+                    ++launches;
+                }
+                launch_gett_f64_batched(g.args, g.tstart, g.n, g.tiles, g.owner, b->active_d, g.akm, g.bkm, b->stream);
+                ++launches;
+            }
+            if (stp.asm_n) {
+                launch_assemble_batched(stp.asm_args, stp.asm_cstart, stp.asm_n, stp.asm_chunks, stp.asm_rank,
+                                        stp.asm_owner, b->active_d, b->stream);
+                ++launches;
+            }
+            if (stp.ncopy) {
+                launch_copy_batched(stp.copies, stp.ncopy, stp.copy_owner, b->active_d, b->stream);
+                ++launches;
+            }
+        }
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(b->ev1, b->stream));
+        for (int j = 0; j < n; ++j) {
+            if (!active[j]) continue;
+            ccq_b200_ctx *c = b->ctx[j];
+            c->launches = 0;
+            post_sweep(c, iter, b->stream);
+            launches += c->launches;
+        }
+        CK(cudaStreamSynchronize(b->stream));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        b->sweep_ms = ms;
+        b->launches = launches;
+        const int diis = (iter % (b->ctx[0]->ds + 1)) == 0;
+        for (int j = 0; j < n; ++j) {
+            if (!active[j]) continue;
+            ccq_b200_ctx *c = b->ctx[j];
+            int info = 0;
+            memcpy(&info, c->hpin + 2, sizeof(int));
+            if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
+            if (e_cor) e_cor[j] = c->hpin[0];
+            if (res) res[j] = std::sqrt(std::sqrt(c->hpin[1]));
+            if (did_diis) did_diis[j] = diis;
+        }
+        return 0;
+    } catch (const Error &e) {
+        return fail(e);
+    } catch (const std::exception &e) {
+        return fail(Error(CCQ_B200_EINVAL, e.what()));
+    }
+}
+
+extern "C" int ccq_b200_batch_stats(const ccq_b200_batch *b, int64_t *launches, double *sweep_ms) {
+    if (!b) return fail(Error(CCQ_B200_EINVAL, "null batch"));
+    if (launches) *launches = b->launches;
+    if (sweep_ms) *sweep_ms = b->sweep_ms;
+    return 0;
+}
+
+extern "C" int ccq_b200_batch_free(ccq_b200_batch *b) {
+    delete b;
+    return 0;
+}
+
+

@@ -52,6 +52,10 @@ SIGNATURES = {
     'ccq_b200_t_size_act': (I64, [C.POINTER(Dims), I64, I64]),
     'ccq_b200_t_compress': (C.c_int, [C.POINTER(Dims), I64, I64, DP, I64, DP, I64]),
     'ccq_b200_t_expand': (C.c_int, [C.POINTER(Dims), I64, I64, DP, I64, DP, I64]),
+    'ccq_b200_batch_create': (C.c_int, [C.POINTER(C.c_void_p), I64, C.POINTER(C.c_void_p)]),
+    'ccq_b200_batch_iterate': (C.c_int, [C.c_void_p, I64, C.POINTER(I64), DP, DP, C.POINTER(I64)]),
+    'ccq_b200_batch_stats': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(C.c_double)]),
+    'ccq_b200_batch_free': (C.c_int, [C.c_void_p]),
     'ccq_b200_sizes': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(I64)]),
     'ccq_b200_set_t': (C.c_int, [C.c_void_p, DP, I64]),
     'ccq_b200_get_t': (C.c_int, [C.c_void_p, DP, I64]),
@@ -245,6 +249,38 @@ def egemm2(k2, k3, A, B):
     Cv = np.zeros(k2)
     _err(lib.ccq_b200_egemm2(k2, k3, _p(A), _p(B), _p(Cv)))
     return Cv
+
+
+class Batch:
+    """Contexts of one plan iterated together (ccq_b200_batch_*): operation k of every active context
+    runs as one launch."""
+
+    def __init__(self, contexts):
+        self._lib = load()
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.ptr.value for c in self.contexts])
+        self.ptr = C.c_void_p()
+        _err(self._lib.ccq_b200_batch_create(arr, len(self.contexts), C.byref(self.ptr)))
+
+    def iterate(self, it, active):
+        """One iteration of every context j with active[j]; returns (e_cor, residuum, did_diis) arrays."""
+        n = len(self.contexts)
+        act = np.ascontiguousarray(np.asarray(active, dtype=np.int64))
+        e, r = np.zeros(n), np.zeros(n)
+        d = np.zeros(n, dtype=np.int64)
+        _err(self._lib.ccq_b200_batch_iterate(self.ptr, it, act.ctypes.data_as(C.POINTER(I64)), _p(e), _p(r),
+                                              d.ctypes.data_as(C.POINTER(I64))))
+        return e, r, d
+
+    def stats(self):
+        n, ms = I64(), C.c_double()
+        _err(self._lib.ccq_b200_batch_stats(self.ptr, C.byref(n), C.byref(ms)))
+        return {'launches': n.value, 'sweep_ms': ms.value}
+
+    def close(self):
+        if self.ptr:
+            self._lib.ccq_b200_batch_free(self.ptr)
+            self.ptr = C.c_void_p()
 
 
 class Context:

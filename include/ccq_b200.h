@@ -166,6 +166,25 @@ int ccq_b200_t_compress(const ccq_b200_dims *dims, int64_t act_occ_b, int64_t ac
 int ccq_b200_t_expand(const ccq_b200_dims *dims, int64_t act_occ_b, int64_t act_unocc_a,
                       const double *t_act, int64_t n_act, double *t_full, int64_t n_full);
 
+/* ---- many independent solves at once --------------------------------------
+ * No counterpart in the reference (it solves one system per run).  A batch
+ * groups contexts of one calc_type, rhf and diis_space on one device (ccq's
+ * CCSD, CCSDT or CCSDTQ plans; not CCSDt or CR-CC(2,3) contexts).  Each
+ * batch iteration runs operation k of every active context as one launch (one
+ * GETT launch over all their output tiles, one assemble launch over all their
+ * canonical elements), then each context's own ring write, residuum and DIIS
+ * step (jacobi_iter, solve_cc.f90:175-269, per context).  active[j] != 0 runs
+ * context j; e_cor, res and did_diis (arrays of n, may be NULL) receive what
+ * ccq_b200_iterate returns for each active context.  The contexts must not be
+ * iterated otherwise while in a batch; freeing the batch leaves them intact. */
+typedef struct ccq_b200_batch ccq_b200_batch;
+int ccq_b200_batch_create(ccq_b200_ctx *const *ctxs, int64_t n, ccq_b200_batch **out);
+int ccq_b200_batch_iterate(ccq_b200_batch *batch, int64_t iter, const int64_t *active,
+                           double *e_cor, double *res, int64_t *did_diis);
+/* launches and device ms of the last batch iteration's sweep */
+int ccq_b200_batch_stats(const ccq_b200_batch *batch, int64_t *launches, double *sweep_ms);
+int ccq_b200_batch_free(ccq_b200_batch *batch);
+
 /* Length of t_vec (get_t_sizes, cc_utils.f90:479-559) and of the DIIS
  * vector (solve_cc.f90:66-77). */
 int ccq_b200_sizes(const ccq_b200_ctx *ctx, int64_t *t_size, int64_t *vec_size);
