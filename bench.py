@@ -233,7 +233,7 @@ def golden_c2():
 # spin): a static count over its egemm calls (2 k1 k2 k3 with the i1, i2, i3 set before each call)
 # and its explicit OpenMP loop bodies over the unique triples (2 per product term per inner
 # iteration) in src/cc/t1A..t3D_update.f90: GEMMs 4.8e10 + T3 loops 1.62e11.  This engine's plan
-# does more FLOPs for the same residuals (every term is a GETT of an antisymmetry-restricted view).
+# counts its own FLOPs from its GETT tables (flops_per_iter: 1.91e11 at this size).
 REFERENCE_FLOPS_C2 = 2.10e11
 
 # DRAM bytes (read + write) per gett_f64 launch in one tuned split-precision sweep of this workload,

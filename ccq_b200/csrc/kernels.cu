@@ -35,11 +35,14 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+// m16n8k8 (sm_90 and later): a = {(g, t), (g + 8, t), (g, t + 4), (g + 8, t + 4)}, b = {(t, g), (t + 4, g)}
+// for lane group g and thread-in-group t, as (row, k) and (k, column)
+__device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
     asm volatile(
-        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
         : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-        : "d"(a0), "d"(a1), "d"(b0));
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // Loads one BKT x BM tile of a GETT operand into shared memory (layout tix).
@@ -154,19 +157,21 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As
         cp_async_wait<NST - 1>();   // tile t has landed
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < BKT; kk += 4) {
-            double a[2][2], b[4];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi) {
-                a[mi][0] = As[st * TILE + tix<AK>(kk + tig, wm + mi * 16 + gid)];
-                a[mi][1] = As[st * TILE + tix<AK>(kk + tig, wm + mi * 16 + gid + 8)];
-            }
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[st * TILE + tix<BKM>(kk + tig, wn + ni * 8 + gid)];
+        for (int kk = 0; kk < BKT; kk += 8) {
+            double a[2][4], b[4][2];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], a[mi][0], a[mi][1], b[ni]);
+                for (int q = 0; q < 4; ++q)
+                    a[mi][q] = As[st * TILE + tix<AK>(kk + tig + 4 * (q >> 1), wm + mi * 16 + gid + 8 * (q & 1))];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) b[ni][q] = Bs[st * TILE + tix<BKM>(kk + tig + 4 * q, wn + ni * 8 + gid)];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x8(acc[mi][ni], a[mi], b[ni]);
         }
         __syncthreads();
     }
@@ -553,19 +558,21 @@ __device__ __forceinline__ void skinny_mainloop(double (&acc)[BMS / 16][4][4], d
         cp_async_commit();
         const double *As = sm + (it % ST) * T::STAGE, *Bs = As + T::ATILE;
 #pragma unroll
-        for (int kk = 0; kk < SBK; kk += 4) {
-            double a[BMS / 16][2], b[4];
-#pragma unroll
-            for (int mi = 0; mi < BMS / 16; ++mi) {
-                a[mi][0] = As[T::template ai<AK>(kk + tig, mi * 16 + gid)];
-                a[mi][1] = As[T::template ai<AK>(kk + tig, mi * 16 + gid + 8)];
-            }
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[T::template bi<BKM>(kk + tig, wn + ni * 8 + gid)];
+        for (int kk = 0; kk < SBK; kk += 8) {
+            double a[BMS / 16][4], b[4][2];
 #pragma unroll
             for (int mi = 0; mi < BMS / 16; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], a[mi][0], a[mi][1], b[ni]);
+                for (int q = 0; q < 4; ++q)
+                    a[mi][q] = As[T::template ai<AK>(kk + tig + 4 * (q >> 1), mi * 16 + gid + 8 * (q & 1))];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) b[ni][q] = Bs[T::template bi<BKM>(kk + tig + 4 * q, wn + ni * 8 + gid)];
+#pragma unroll
+            for (int mi = 0; mi < BMS / 16; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x8(acc[mi][ni], a[mi], b[ni]);
         }
     }
     cp_async_wait<0>();

@@ -1,7 +1,7 @@
 // Device kernels of libccq_b200 (sm_100a).
 //
 //  gett_f64     : GEMM over strided/permuted tensor views (GETT) in FP64 on the
-//                 DMMA tensor pipe (mma.sync m16n8k4 f64).  Operand addresses
+//                 DMMA tensor pipe (mma.sync m16n8k8 f64).  Operand addresses
 //                 come from per-mode offset tables, so a permuted slice of a
 //                 resident tensor is read in place: this fuses the reference's
 //                 reorder_shift / reorder_stripe + egemm + sum_stripe triple

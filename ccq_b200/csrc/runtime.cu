@@ -326,13 +326,23 @@ struct ccq_b200_ctx {
     std::vector<std::pair<size_t, std::string>> out_after;   // (op index, block) of every block's last write
     bool out_ready = false;
 
+    // Device memory comes from the device's stream-ordered pool (on this context's stream): the memory of
+    // a closed context goes back to the pool and a new context takes it from there, instead of a driver
+    // unmap and map per buffer (a CR-CC(2,3) context created after another was freed spent 1.3 s in
+    // cudaMalloc; this pool keeps up to kPoolKeep bytes of freed memory for the process).
     void *dalloc(size_t bytes) {
         void *p = nullptr;
-        CK(cudaMalloc(&p, bytes ? bytes : 8));
+        CK(cudaMallocAsync(&p, bytes ? bytes : 8, stream));
         owned.push_back(p);
+        // the buffer is filled by copies and kernels on other streams: complete the allocation now
+        CK(cudaStreamSynchronize(stream));
         return p;
     }
     ~ccq_b200_ctx() {
+        // every stream of this context is idle before its memory goes back to the pool
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto st : side) cudaStreamSynchronize(st);
+        if (cstream) cudaStreamSynchronize(cstream);
         if (gexec) cudaGraphExecDestroy(gexec);
         if (lgexec) cudaGraphExecDestroy(lgexec);
         if (gexec_host) cudaGraphExecDestroy(gexec_host);
@@ -344,7 +354,10 @@ struct ccq_b200_ctx {
         for (auto st : side) cudaStreamDestroy(st);
         split_free(split);
         if (hpin) cudaFreeHost(hpin);
-        for (void *p : owned) cudaFree(p);
+        if (stream) {
+            for (void *p : owned) cudaFreeAsync(p, stream);
+            cudaStreamSynchronize(stream);
+        }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev2) cudaEventDestroy(ev2);
@@ -619,6 +632,22 @@ void apply_active_masks(ccq_b200_ctx *c, long long act_occ_b, long long act_unoc
     }
 }
 
+// The device's default memory pool keeps up to kPoolKeep bytes of freed memory for this process (its
+// release threshold; a property of this process's pool, not of the GPU), set once per device.
+constexpr uint64_t kPoolKeep = 16ull << 30;
+
+void keep_pool_memory(int dev) {
+    static std::once_flag once[64];
+    if (dev < 0 || dev >= 64) return;
+    std::call_once(once[dev], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = kPoolKeep;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    });
+}
+
 void trace_stamp(const ccq_b200_ctx *c, const char *what) {
     if (!c->trace_init) return;
     double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - c->t_init0).count();
@@ -754,7 +783,8 @@ void instantiate(ccq_b200_ctx *c) {
         }
         c->bufs[b.name] = d;
     }
-    launch_fill(c->bufs.at("ONES").ptr, 1.0, c->bufs.at("ONES").numel, c->stream);
+    for (auto &b : c->plan.bufs)
+        if (b.kind == "ones") launch_fill(c->bufs.at(b.name).ptr, 1.0, std::max(c->bufs.at(b.name).numel, 1LL), c->stream);
     trace_stamp(c, "buffers");
 
     // ---- operations ----------------------------------------------------------
@@ -1674,6 +1704,7 @@ static int init_impl(const ccq_b200_dims *dims, const char *calc_type, const dou
         c->trace_init = getenv("CCQ_B200_TRACE_INIT") != nullptr;
         c->t_init0 = std::chrono::steady_clock::now();
         CK(cudaGetDevice(&c->device));
+        keep_pool_memory(c->device);
         CK(gett_f64_prepare());
         CK(preload_kernels((int)diis_space));
         c->calc_type = ct;

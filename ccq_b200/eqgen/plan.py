@@ -20,6 +20,7 @@ serialised as text; ``libccq_b200`` instantiates it for concrete sizes.
 from __future__ import annotations
 
 import itertools
+import re
 from dataclasses import dataclass, field
 from fractions import Fraction
 
@@ -663,7 +664,8 @@ class PlanBuilder:
             else:
                 self.emit_block(b)
         self.emit_energy()
-        return self
+        merge_equal_views(self)
+        return merge_shared_operand(self)
 
     def build_crcc(self):
         """CCSD sweep followed by the CR-CC(2,3) phases (``src/calc_driver.f90:55-73``).
@@ -812,3 +814,176 @@ def plan_flops(builder, sizes=SIZES_C2):
             m, n, k, _ = gett_count(op, sizes)
             tot += 2 * m * n * k
     return tot
+
+
+# ---------------------------------------------------------------------------
+# Shared-operand merge.  Within one block phase, several GETTs often add into
+# the same output view with the same amplitude operand, contracted over the
+# same axes, and differ only in the small operand (an integral slice and a
+# T2-built intermediate of the same shape: the linear ring term v T3 and the
+# quadratic T2 v T3 term of the same topology, or f_oo T3 and X_oo T3).
+# Z += a1 S1 T + a2 S2 T is then computed as W = a1 S1 + a2 S2 (a small
+# buffer, built by GETTs against the scalar ONE) followed by one Z += W T, so
+# the amplitude block is read once and the large product is done once.  The
+# merged GETT takes the place of the group's last member (every small operand
+# exists there; nothing reads Z before the block's assemble), and the first
+# remaining writer of Z becomes the overwriting one.
+# ---------------------------------------------------------------------------
+_BIG = re.compile(r'^T[234][A-E]$')
+_PHASE = re.compile(r'^T[1-4][A-E]$')
+
+
+def merge_shared_operand(builder):
+    ops = builder.ops
+    phases = []
+    start = None
+    for i, op in enumerate(ops):
+        if isinstance(op, Simple) and op.kind == 'PHASE':
+            if start is not None:
+                phases.append((start, i))
+            start = i if _PHASE.match(str(op.args[0])) else None
+    if start is not None:
+        phases.append((start, len(ops)))
+    if 'ONE' not in builder.buffers:
+        builder.buf('ONE', 'ones', ())
+    new_ops = list(ops)
+    replace = {}    # op index -> list of ops in its place ([] deletes it)
+    for p0, p1 in phases:
+        groups = {}
+        for i in range(p0 + 1, p1):
+            op = ops[i]
+            if not isinstance(op, Gett):
+                continue
+            for big_is_b in (True, False):
+                big, small = (op.b, op.a) if big_is_b else (op.a, op.b)
+                if not _BIG.match(big.buf) or _BIG.match(small.buf):
+                    continue
+                sl, bl, cl = small.labels(), big.labels(), op.c.labels()
+                if len(set(sl)) != len(sl) or len(set(bl)) != len(bl):
+                    continue
+                kl = [l for l in bl if l not in cl]
+                ren = {l: ('o' if _sp(l) == 'o' else 'v') + f'w{j}' for j, l in enumerate(kl)}
+                outg = tuple(sorted(tuple(g) for g in op.restrict if all(l in cl for l in g)))
+                kg = tuple(sorted(tuple(ren[l] for l in g) for g in op.restrict if all(l in ren for l in g)))
+                if len(outg) + len(kg) != len(op.restrict):
+                    continue
+                bigc = View(big.buf, [Axis(ren.get(a.label, a.label), a.size, a.start) for a in big.axes])
+                smallc = View(small.buf, [Axis(ren.get(a.label, a.label), a.size, a.start) for a in small.axes])
+                key = (op.c.text(), bigc.text(), big_is_b, outg, kg)
+                groups.setdefault(key, []).append((i, op, smallc, bigc))
+                break
+        used = set()
+        for key, mem in groups.items():
+            mem = [m for m in mem if m[0] not in used]
+            if len(mem) < 2:
+                continue
+            c_text, big_text, big_is_b, outg, kg = key
+            # one shape for W: the first member's small axes; every member's small view has the same labels
+            wax = [Axis(a.label, a.size) for a in mem[0][2].axes]
+            sig = sorted((a.label, a.size) for a in wax)
+            if any(sorted((a.label, a.size) for a in m[2].axes) != sig for m in mem):
+                continue
+            w = builder.new_x([a.size for a in wax])
+            wv = View(w, wax)
+            seq = []
+            for k, (i, op, smallc, bigc) in enumerate(mem):
+                seq.append(Gett(wv, smallc, View('ONE', []), op.alpha, 0 if k == 0 else 1, op.tag))
+            first = mem[0][1]
+            a, b = (wv, mem[0][3]) if big_is_b else (mem[0][3], wv)
+            seq.append(Gett(first.c, a, b, 1.0, 1, first.tag, [list(g) for g in outg] + [list(g) for g in kg]))
+            for i, *_ in mem[:-1]:
+                replace[i] = []
+            replace[mem[-1][0]] = seq
+            used.update(i for i, *_ in mem)
+    if not replace:
+        return builder
+    out = []
+    for i, op in enumerate(new_ops):
+        out.extend(replace.get(i, [op]))
+    builder.ops = out
+    _first_writer_overwrites(builder)
+    return builder
+
+
+def _first_writer_overwrites(builder):
+    """The first writer of every work buffer of a phase overwrites it, the others add."""
+    seen = set()
+    for op in builder.ops:
+        if isinstance(op, Simple) and op.kind == 'PHASE':
+            seen = set()
+            continue
+        if isinstance(op, Gett) and op.c.buf[0] in 'ZX':
+            if op.c.buf not in seen:
+                op.beta = 0
+                seen.add(op.c.buf)
+            else:
+                op.beta = 1
+
+
+# ---------------------------------------------------------------------------
+# Equal-view merge.  The assemble of a block reads every Z buffer through a
+# set of permuted views with coefficients.  Term groups of different topology
+# often end with the same view set (up to one common factor) on Z buffers of
+# the same shape and the same antisymmetric storage: the T3B residual has 25
+# Z buffers but only 7 distinct (shape, storage, view set) classes.  The
+# writers of every Z of a class then add into the class's first Z, scaled by
+# the ratio of the view coefficients, and the assemble reads one buffer per
+# class: fewer gathered terms per element, fewer buffers, and small-K writers
+# of one Z view become one grouped launch in the runtime.
+# ---------------------------------------------------------------------------
+def merge_equal_views(builder):
+    ops = builder.ops
+    refs = {}
+    for i, op in enumerate(ops):
+        if isinstance(op, Gett):
+            for role, v in (('c', op.c), ('a', op.a), ('b', op.b)):
+                refs.setdefault(v.buf, []).append((i, role))
+        elif isinstance(op, Assemble):
+            for _, v in op.terms:
+                refs.setdefault(v.buf, []).append((i, 'asm'))
+            refs.setdefault(op.block, []).append((i, 'asm_out'))
+        elif isinstance(op, Simple):
+            for a in op.args:
+                refs.setdefault(str(a), []).append((i, 'simple'))
+    changed = False
+    start = None
+    for i, op in enumerate(ops):
+        if isinstance(op, Simple) and op.kind == 'PHASE':
+            start = i
+            continue
+        if not isinstance(op, Assemble) or start is None or not _PHASE.match(op.block):
+            continue
+        views = {}
+        for c, v in op.terms:
+            if v.buf.startswith('Z'):
+                views.setdefault(v.buf, []).append((Fraction(c), tuple((a.label, a.size, a.start) for a in v.axes)))
+        classes = {}
+        for z, mem in views.items():
+            # Z is written only by GETTs of this phase and read only by this assemble
+            if not all((r == 'c' and start < j < i) or (j == i and r == 'asm') for j, r in refs.get(z, [])):
+                continue
+            mem = sorted(mem, key=lambda m: m[1])
+            c0 = mem[0][0]
+            key = (builder.buffers[z], tuple(builder.zgroups.get(z, ())), tuple((vk, c / c0) for c, vk in mem))
+            classes.setdefault(key, []).append((z, c0))
+        drop = {}
+        for members in classes.values():
+            (zt, ct), rest = members[0], members[1:]
+            for z, c0 in rest:
+                r = float(c0 / ct)
+                for j, role in refs[z]:
+                    if role == 'c':
+                        w = ops[j]
+                        w.c = View(zt, w.c.axes)
+                        w.alpha = w.alpha * r
+                drop[z] = zt
+        if not drop:
+            continue
+        op.terms[:] = [(c, v) for c, v in op.terms if v.buf not in drop]
+        for z in drop:
+            del builder.buffers[z]
+            builder.zgroups.pop(z, None)
+        changed = True
+    if changed:
+        _first_writer_overwrites(builder)
+    return builder

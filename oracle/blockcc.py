@@ -115,7 +115,9 @@ class BlockCC:
         self.buf['VBB0'][...] = v_bb
         self.buf['HA0'][...] = fa - np.einsum('piqi->pq', v_aa[:, :oa, :, :oa]) - np.einsum('piqi->pq', v_ab[:, :ob, :, :ob])
         self.buf['HB0'][...] = fb - np.einsum('piqi->pq', v_bb[:, :ob, :, :ob]) - np.einsum('ipiq->pq', v_ab[:oa, :, :oa, :])
-        self.buf['ONES'][...] = 1.0
+        for name, (kind, dd) in self.plan['buffers'].items():
+            if kind == 'ones':
+                self.buf[name][...] = 1.0
         self.fdiag_a = np.diag(fa).copy()
         self.fdiag_b = np.diag(fb).copy()
         self.flops = 0
