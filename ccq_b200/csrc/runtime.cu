@@ -334,7 +334,10 @@ struct ccq_b200_ctx {
         void *p = nullptr;
         CK(cudaMallocAsync(&p, bytes ? bytes : 8, stream));
         owned.push_back(p);
-        // the buffer is filled by copies and kernels on other streams: complete the allocation now
+        // touched once here: the first write to fresh device memory is slow (a 538 MB DIIS ring slot first
+        // written at the first DIIS step cost 30-60 ms inside an iteration); the buffer is also filled by
+        // copies and kernels on other streams, so the allocation completes now
+        CK(cudaMemsetAsync(p, 0, bytes ? bytes : 8, stream));
         CK(cudaStreamSynchronize(stream));
         return p;
     }
@@ -1559,8 +1562,10 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
             if (o.kind == OP_GETT) c->prof_flops[k] += fl;
             if (df) {
                 if (o.kind == OP_GETT)
-                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f %d %.6e\n", i, k, o.tag.c_str(),
-                            o.mnk[0], o.mnk[1], o.mnk[2], o.akm, o.bkm, o.beta, ms, o.group_size, fl);
+                    // ... tile choice (0: by shape), shape family (0: 64 x 64, 1/2: skinny rows/columns)
+                    fprintf(df, "%zu GETT %d %s %lld %lld %lld %d %d %d %.6f %d %.6e %d %d\n", i, k, o.tag.c_str(),
+                            o.mnk[0], o.mnk[1], o.mnk[2], o.akm, o.bkm, o.beta, ms, o.group_size, fl, o.g.tile,
+                            gett_f64_family(o.g.M, o.g.N));
                 else if (o.kind == OP_ASM)
                     fprintf(df, "%zu ASM %d %s %d %.6f\n", i, k, o.block.c_str(), o.asmargs.nterms, ms);
                 else
