@@ -1183,17 +1183,29 @@ void instantiate(ccq_b200_ctx *c) {
         fprintf(stderr, "ccq_b200_init table entries %zu, ops %zu, assemble terms %zu\n", itab.size(),
                 c->plan.ops.size(), hterms.size());
     trace_stamp(c, "op tables");
-    // Group small-K contractions that add into the same Z view (consecutive writers
-    // of that Z within one block phase, identical output tables): one launch per
-    // group at the position of its last member.  Their operands are not modified
-    // later in the phase and Z is only read by the closing assemble, so moving the
-    // earlier members later is safe.
+    // Group small-K contractions that add into the same Z buffer with the same output tables (the
+    // same split of Z's axes between the two operands; a writer whose tables match with the operands
+    // exchanged is exchanged): one launch per group at the position of its last member.  Their
+    // operands are not modified later in the phase (work buffers of one phase never share memory,
+    // amplitudes change only in the closing assemble) and Z is only read by that assemble, so moving
+    // the earlier members later is safe.  Every write into Z adds, except the first one executed,
+    // which overwrites: the overwrite flag follows the new order.  With active-space filters (an op
+    // split into pieces that must share one flag) only consecutive writers group, keeping the flags.
     {
         std::vector<GettSeg> hsegs;
         std::vector<std::pair<size_t, size_t>> leaders;
         auto groupable = [&](const Op &o) {
             return o.kind == OP_GETT && o.g.M > 0 && o.g.N > 0 && o.g.K > 0 && o.g.K < 256 && !o.zero_first &&
-                   (o.g.K + o.g.kchunk - 1) / o.g.kchunk == 1 && o.c.buf[0] == 'Z';
+                   (o.g.K + o.g.kchunk - 1) / o.g.kchunk == 1 && o.c.buf[0] == 'Z' && !o.frozen;
+        };
+        bool any_filter = false;
+        for (auto &o : c->plan.ops) any_filter = any_filter || !o.filters.empty();
+        // 0: no match, 1: same tables, 2: tables of the exchanged operands
+        auto match = [&](const Op &q, const Op &f) {
+            if (q.g.C != f.g.C) return 0;
+            if (q.hcm == f.hcm && q.hcn == f.hcn && q.g.c_nfast == f.g.c_nfast) return 1;
+            if (!any_filter && q.hcm == f.hcn && q.hcn == f.hcm) return 2;
+            return 0;
         };
         size_t b = 0;
         while (b < c->plan.ops.size()) {
@@ -1206,43 +1218,84 @@ void instantiate(ccq_b200_ctx *c) {
             }
             for (auto &wz : writers) {
                 auto &lst = wz.second;
-                size_t k = 0;
-                while (k < lst.size()) {
-                    size_t j = k + 1;
-                    Op &f = c->plan.ops[lst[k]];
-                    if (groupable(f)) {
-                        while (j < lst.size()) {
-                            Op &q = c->plan.ops[lst[j]];
-                            if (!groupable(q) || q.g.C != f.g.C || q.hcm != f.hcm || q.hcn != f.hcn ||
-                                q.g.c_nfast != f.g.c_nfast)
-                                break;
-                            ++j;
+                // classes of mutually matching groupable writers (consecutive runs only with filters)
+                std::vector<std::vector<std::pair<size_t, int>>> cls;   // (op, 1 same / 2 exchanged vs first)
+                std::vector<std::pair<size_t, int>> run;
+                for (size_t q = 0; q < lst.size(); ++q) {
+                    Op &o = c->plan.ops[lst[q]];
+                    if (!groupable(o)) {
+                        if (any_filter && !run.empty()) {
+                            cls.push_back(run);
+                            run.clear();
+                        }
+                        continue;
+                    }
+                    if (any_filter) {
+                        if (!run.empty() && match(o, c->plan.ops[run[0].first]) != 1) {
+                            cls.push_back(run);
+                            run.clear();
+                        }
+                        run.push_back({lst[q], 1});
+                        continue;
+                    }
+                    bool placed = false;
+                    for (auto &cl : cls) {
+                        const int m = match(o, c->plan.ops[cl[0].first]);
+                        if (m) {
+                            cl.push_back({lst[q], m});
+                            placed = true;
+                            break;
                         }
                     }
-                    if (j - k >= 2) {
-                        size_t off = hsegs.size();
-                        double fl = 0.0;
-                        for (size_t q = k; q < j; ++q) {
-                            Op &m = c->plan.ops[lst[q]];
+                    if (!placed) cls.push_back({{lst[q], 1}});
+                }
+                if (!run.empty()) cls.push_back(run);
+                bool regrouped = false;
+                for (auto &cl : cls) {
+                    if (cl.size() < 2) continue;
+                    regrouped = true;
+                    Op &lead = c->plan.ops[cl.back().first];
+                    const int lead_m = cl.back().second;
+                    size_t off = hsegs.size();
+                    double fl = 0.0;
+                    for (auto &mm : cl) {
+                        Op &m = c->plan.ops[mm.first];
+                        // orientation relative to the leader: exchange A and B where it differs
+                        if (mm.second == lead_m)
                             hsegs.push_back(GettSeg{m.g.A, m.g.B, m.g.offA_m, m.g.offA_k, m.g.offB_n, m.g.offB_k,
                                                     m.g.K, m.g.alpha});
-                            fl += 2.0 * m.mnk[0] * m.mnk[1] * m.mnk[2];
-                            if (q + 1 < j) m.skip = true;
-                        }
-                        Op &lead = c->plan.ops[lst[j - 1]];
-                        for (size_t q = k; q < j; ++q) {
-                            const Op &m = c->plan.ops[lst[q]];
-                            lead.g.vec_a = lead.g.vec_a && m.g.vec_a && m.akm == lead.akm;
-                            lead.g.vec_b = lead.g.vec_b && m.g.vec_b && m.bkm == lead.bkm;
-                        }
-                        lead.g.beta = f.beta;
-                        lead.g.nseg = (int)(j - k);
-                        for (size_t q = k; q < j; ++q) lead.group_ops.push_back(lst[q]);
-                        lead.group_flops = fl;
-                        lead.group_size = (int)(j - k);
-                        leaders.push_back({lst[j - 1], off});
+                        else
+                            hsegs.push_back(GettSeg{m.g.B, m.g.A, m.g.offB_n, m.g.offB_k, m.g.offA_m, m.g.offA_k,
+                                                    m.g.K, m.g.alpha});
+                        fl += 2.0 * m.mnk[0] * m.mnk[1] * m.mnk[2];
+                        if (&m != &lead) m.skip = true;
                     }
-                    k = j;
+                    for (auto &mm : cl) {
+                        const Op &m = c->plan.ops[mm.first];
+                        const bool same = mm.second == lead_m;
+                        lead.g.vec_a = lead.g.vec_a && (same ? m.g.vec_a && m.akm == lead.akm
+                                                             : m.g.vec_b && m.bkm == lead.akm);
+                        lead.g.vec_b = lead.g.vec_b && (same ? m.g.vec_b && m.bkm == lead.bkm
+                                                             : m.g.vec_a && m.akm == lead.bkm);
+                    }
+                    lead.g.beta = c->plan.ops[cl[0].first].beta;
+                    lead.g.nseg = (int)cl.size();
+                    for (auto &mm : cl) lead.group_ops.push_back(mm.first);
+                    lead.group_flops = fl;
+                    lead.group_size = (int)cl.size();
+                    leaders.push_back({cl.back().first, off});
+                }
+                if (!regrouped || any_filter) continue;
+                // the first write executed into Z overwrites it, the others add
+                bool first = true;
+                for (size_t i : lst) {
+                    Op &o = c->plan.ops[i];
+                    if (o.skip || o.frozen || o.g.M == 0 || o.g.N == 0) continue;
+                    o.beta = first ? 0 : 1;
+                    o.g.beta = o.beta;
+                    o.zero_first = !o.g.segs && o.group_ops.empty() && o.beta == 0 &&
+                                   (o.g.K + o.g.kchunk - 1) / o.g.kchunk > 1;
+                    first = false;
                 }
             }
             b = e;
