@@ -106,6 +106,29 @@ __device__ __forceinline__ void load_tile(double *S, const double *base, const i
     }
 }
 
+// The MMAs of one staged BKT-deep K tile into a warp's 32 x 32 accumulator block.
+template <bool AK, bool BKM>
+__device__ __forceinline__ void mma_stage(double (&acc)[2][4][4], const double *As, const double *Bs, int wm, int wn,
+                                          int gid, int tig) {
+#pragma unroll
+    for (int kk = 0; kk < BKT; kk += 8) {
+        double a[2][4], b[4][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                a[mi][q] = As[tix<AK>(kk + tig + 4 * (q >> 1), wm + mi * 16 + gid + 8 * (q & 1))];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) b[ni][q] = Bs[tix<BKM>(kk + tig + 4 * q, wn + ni * 8 + gid)];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma_16x8x8(acc[mi][ni], a[mi], b[ni]);
+    }
+}
+
 // K loop of one contraction term over [kbeg, kend): NST-stage cp.async pipeline
 // (As and Bs hold NST tiles each; one commit group per K tile, empty past the end).
 template <bool AK, bool BKM, int NST>
@@ -156,23 +179,7 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As
         cp_async_commit();
         cp_async_wait<NST - 1>();   // tile t has landed
         __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BKT; kk += 8) {
-            double a[2][4], b[4][2];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    a[mi][q] = As[st * TILE + tix<AK>(kk + tig + 4 * (q >> 1), wm + mi * 16 + gid + 8 * (q & 1))];
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                for (int q = 0; q < 2; ++q) b[ni][q] = Bs[st * TILE + tix<BKM>(kk + tig + 4 * q, wn + ni * 8 + gid)];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma_16x8x8(acc[mi][ni], a[mi], b[ni]);
-        }
+        mma_stage<AK, BKM>(acc, As + st * TILE, Bs + st * TILE, wm, wn, gid, tig);
         __syncthreads();
     }
 }
@@ -224,22 +231,42 @@ __device__ __forceinline__ void gett_f64_tile(const GettArgs &g, int bx, int by,
 
     // epilogue: stage the tile in shared memory, then write along the output's
     // contiguous mode (g.c_nfast) so that stores and the beta read coalesce
-    static_assert(BM * (BN + 1) * 2 + BM + BN <= 8 * TILE, "C tile and output tables must fit in two stages");
-    double (*Cs)[BN + 1] = reinterpret_cast<double (*)[BN + 1]>(smem);
+    // C tile layout: rows along the output's contiguous mode, so that the write-out reads rows.  [m][n]
+    // with row stride CSN = BN + 8 when n is the fast mode (the fragments' (j = 0, 1) pairs are stored as
+    // one 16-byte access, conflict-free per 8 lanes), else [n][m] with stride CSM = BM + 2 (scalar stores,
+    // conflict-free per half-warp)
+    constexpr int CSN = BN + 8, CSM = BM + 2;
+    constexpr int CS_ELEMS = BM * CSN > BN * CSM ? BM * CSN : BN * CSM;
+    static_assert(CS_ELEMS * 2 + BM + BN <= 8 * TILE, "C tile and output tables must fit in two stages");
+    static_assert(CSN % 2 == 0 && CSM % 2 == 0, "16-byte aligned rows");
+    double *Cs = smem;
+    const bool nf = g.c_nfast != 0;
+    auto cs = [&](int ml, int nl) -> double & { return nf ? Cs[ml * CSN + nl] : Cs[nl * CSM + ml]; };
     // the tile's output offsets, staged once (-1: outside C)
-    int *ocm = reinterpret_cast<int *>(smem + BM * (BN + 1));
+    int *ocm = reinterpret_cast<int *>(smem + CS_ELEMS);
     int *ocn = ocm + BM;
     if (tid < BM) ocm[tid] = m0 + tid < g.M ? __ldg(g.offC_m + m0 + tid) : -1;
     else if (tid < BM + BN) ocn[tid - BM] = n0 + tid - BM < g.N ? __ldg(g.offC_n + n0 + tid - BM) : -1;
+    if (nf) {
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+        for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+            for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
+                for (int ni = 0; ni < 4; ++ni)
+                    *reinterpret_cast<double2 *>(&Cs[(wm + mi * 16 + gid + 8 * h) * CSN + wn + ni * 8 + 2 * tig]) =
+                        make_double2(alpha * acc[mi][ni][2 * h], alpha * acc[mi][ni][2 * h + 1]);
+    } else {
 #pragma unroll
-                for (int j = 0; j < 2; ++j)
-                    Cs[wm + mi * 16 + gid + 8 * h][wn + ni * 8 + 2 * tig + j] = alpha * acc[mi][ni][2 * h + j];
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j)
+                        Cs[(wn + ni * 8 + 2 * tig + j) * CSM + wm + mi * 16 + gid + 8 * h] = alpha * acc[mi][ni][2 * h + j];
+    }
     __syncthreads();
     // split-K slices and beta = 1 updates add into C with fire-and-forget reductions
     // (one add per element and slice: the same rounding as a read-add-write, with no
@@ -259,7 +286,8 @@ __device__ __forceinline__ void gett_f64_tile(const GettArgs &g, int bx, int by,
                 int nl = g.c_nfast ? fast : slow;
                 const int om = ocm[ml], on = ocn[nl];
                 cp[u] = (om >= 0 && on >= 0) ? reinterpret_cast<double2 *>(g.C + (long long)om + on) : nullptr;
-                cv[u] = g.c_nfast ? make_double2(Cs[ml][nl], Cs[ml][nl + 1]) : make_double2(Cs[ml][nl], Cs[ml + 1][nl]);
+                // the pair is contiguous in the tile's row as well
+                cv[u] = *reinterpret_cast<const double2 *>(&cs(ml, nl));
             }
             double2 old[4];
 #pragma unroll
@@ -284,7 +312,7 @@ __device__ __forceinline__ void gett_f64_tile(const GettArgs &g, int bx, int by,
             int nl = g.c_nfast ? fast : slow;
             const int om = ocm[ml], on = ocn[nl];
             cp[u] = (om >= 0 && on >= 0) ? g.C + (long long)om + on : nullptr;
-            cv[u] = Cs[ml][nl];
+            cv[u] = cs(ml, nl);
         }
         if (atomic) {
 #pragma unroll
@@ -369,9 +397,13 @@ void launch_gett_f64_batched(const GettArgs *args, const int *tstart, int n, int
         gett_f64_batched_kernel<false, false, 2><<<tiles, 128, sm, s>>>(args, tstart, n, owner, active);
 }
 
+// dynamic shared memory of gett_f64_kernel: the operand stages
+template <bool G, int NST>
+constexpr size_t gett_smem() { return sizeof(double) * 2 * NST * TILE; }
+
 template <bool G, int NST>
 void launch_gett_v(const GettArgs &a, int a_kmajor, int b_kmajor, dim3 grid, cudaStream_t s) {
-    constexpr size_t sm = sizeof(double) * 2 * NST * TILE;
+    constexpr size_t sm = gett_smem<G, NST>();
     if (a_kmajor && b_kmajor)
         gett_f64_kernel<true, true, G, NST><<<grid, 128, sm, s>>>(a);
     else if (a_kmajor)
@@ -384,7 +416,7 @@ void launch_gett_v(const GettArgs &a, int a_kmajor, int b_kmajor, dim3 grid, cud
 
 template <bool G, int NST>
 cudaError_t gett_attr() {
-    constexpr int sm = (int)(sizeof(double) * 2 * NST * TILE);
+    constexpr int sm = (int)gett_smem<G, NST>();
     constexpr auto at = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaError_t e = cudaFuncSetAttribute(gett_f64_kernel<true, true, G, NST>, at, sm);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(gett_f64_kernel<true, false, G, NST>, at, sm);
@@ -865,6 +897,139 @@ bool launch_smallk(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Small-K GETT with register-direct operands: each warp owns a 32 x 32 block of a 64 x 64 tile and loads
+// its m16n8k8 fragments straight from global memory through the offset tables (the operands of small-K
+// contractions are small and stay in L2), so there is no shared-memory staging and no barrier; the
+// accumulators are written from registers (8 consecutive outputs per lane group, 16-byte pairs where the
+// output pairs up along n).  Whole K per launch, every warp independent; grouped launches loop over their
+// segments, rescaling the running sum by alpha_{s-1} / alpha_s.
+// ---------------------------------------------------------------------------
+template <bool GROUPED>
+__global__ void __launch_bounds__(128) gett_f64_direct_kernel(GettArgs g) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int m0 = blockIdx.x * BM + (warp >> 1) * 32, n0 = blockIdx.y * BN + (warp & 1) * 32;
+    if (m0 >= g.M || n0 >= g.N) return;   // the warp's block lies outside C (warp-uniform)
+    double acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+    double alpha = g.alpha;
+    const int nseg = GROUPED ? g.nseg : 1;
+    for (int sgi = 0; sgi < nseg; ++sgi) {
+        const double *A = g.A, *B = g.B;
+        const int *oam = g.offA_m, *oak = g.offA_k, *obn = g.offB_n, *obk = g.offB_k;
+        int K = g.K;
+        double sa = g.alpha;
+        if (GROUPED) {
+            const GettSeg sg = g.segs[sgi];
+            A = sg.A;
+            B = sg.B;
+            oam = sg.offA_m;
+            oak = sg.offA_k;
+            obn = sg.offB_n;
+            obk = sg.offB_k;
+            K = sg.K;
+            sa = sg.alpha;
+            if (sgi > 0 && sa != alpha) {
+                const double r = alpha / sa;
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[i][j][q] *= r;
+            }
+            alpha = sa;
+        }
+        // A rows m0 + mi*16 + gid + 8h and B columns n0 + ni*8 + gid of this thread's fragments
+        int ra[2][2], rb[4];
+        bool ia[2][2], ib[4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int m = m0 + mi * 16 + gid + 8 * h;
+                ia[mi][h] = m < g.M;
+                ra[mi][h] = ia[mi][h] ? __ldg(oam + m) : 0;
+            }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int n = n0 + ni * 8 + gid;
+            ib[ni] = n < g.N;
+            rb[ni] = ib[ni] ? __ldg(obn + n) : 0;
+        }
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            int ka[2], kb[2];
+            bool ik[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int kk = k0 + tig + 4 * q;
+                ik[q] = kk < K;
+                ka[q] = ik[q] ? __ldg(oak + kk) : 0;
+                kb[q] = ik[q] ? __ldg(obk + kk) : 0;
+            }
+            double a[2][4], b[4][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int h = q & 1, kq = q >> 1;
+                    a[mi][q] = (ia[mi][h] && ik[kq]) ? __ldg(A + (long long)ra[mi][h] + ka[kq]) : 0.0;
+                }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) b[ni][q] = (ib[ni] && ik[q]) ? __ldg(B + (long long)rb[ni] + kb[q]) : 0.0;
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x8(acc[mi][ni], a[mi], b[ni]);
+        }
+    }
+    // outputs (m0 + mi*16 + gid + 8h, n0 + ni*8 + 2 tig + j) = acc[mi][ni][2h + j]
+    int om[2][2], on[4][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int m = m0 + mi * 16 + gid + 8 * h;
+            om[mi][h] = m < g.M ? __ldg(g.offC_m + m) : -1;
+        }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int n = n0 + ni * 8 + 2 * tig + j;
+            on[ni][j] = n < g.N ? __ldg(g.offC_n + n) : -1;
+        }
+    const bool pairs = !g.beta && g.vec_c && g.c_nfast;
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (om[mi][h] < 0) continue;
+            double *crow = g.C + om[mi][h];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+                const double v0 = alpha * acc[mi][ni][2 * h], v1 = alpha * acc[mi][ni][2 * h + 1];
+                if (pairs && on[ni][1] >= 0) {
+                    *reinterpret_cast<double2 *>(crow + on[ni][0]) = make_double2(v0, v1);
+                } else if (g.beta) {
+                    if (on[ni][0] >= 0) atomicAdd(crow + on[ni][0], v0);
+                    if (on[ni][1] >= 0) atomicAdd(crow + on[ni][1], v1);
+                } else {
+                    if (on[ni][0] >= 0) crow[on[ni][0]] = v0;
+                    if (on[ni][1] >= 0) crow[on[ni][1]] = v1;
+                }
+            }
+        }
+}
+
 int gett_f64_family(long long M, long long N) {
     if (M <= 32 && M <= N) return 1;
     if (N <= 32 && N < M) return 2;
@@ -891,6 +1056,15 @@ int gett_f64_kchunk(long long M, long long N, long long K) {
 
 void launch_gett_f64(const GettArgs &a, int a_kmajor, int b_kmajor, cudaStream_t s) {
     if (a.tile == 3 && launch_smallk(a, a_kmajor, b_kmajor, s)) return;
+    if (a.tile == 6) {
+        // register-direct small-K kernel: the whole K range in one pass (no split-K slices)
+        dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, 1);
+        if (a.segs)
+            gett_f64_direct_kernel<true><<<grid, 128, 0, s>>>(a);
+        else
+            gett_f64_direct_kernel<false><<<grid, 128, 0, s>>>(a);
+        return;
+    }
     const int zsplit = a.segs ? 1 : std::max(1, (a.K + a.kchunk - 1) / a.kchunk);
     int fam = gett_f64_family(a.M, a.N);
     if (a.tile == 1 || a.tile == 4) fam = 0;

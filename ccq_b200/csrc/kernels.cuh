@@ -51,7 +51,8 @@ struct GettArgs {
     int tile;       // 0: tile family by shape (gett_f64_family); 1: 64 x 64 tiles; 2: skinny tiles;
                     // 3: small-K FMA kernel (whole K per launch, kchunk ignored);
                     // 4: 64 x 64 tiles with a 3-stage operand pipeline;
-                    // 5: skinny tiles with a 2-stage ring (more CTAs per SM)
+                    // 5: skinny tiles with a 2-stage ring (more CTAs per SM);
+                    // 6: register-direct small-K kernel (whole K per launch, kchunk ignored)
 };
 
 constexpr int MAXG = 4;  // antisymmetric axis groups per source view

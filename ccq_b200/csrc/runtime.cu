@@ -2595,8 +2595,9 @@ int ccq_b200_autotune(ccq_b200_ctx *c, int64_t reps, double *ms_default, double 
                         if (!dup) cand.push_back(t);
                     }
                 }
-                // small-K FMA kernel: whole K per launch
+                // small-K FMA kernel and register-direct DMMA kernel: whole K per launch
                 if (K <= 128) cand.push_back(TuneCfg{3, o.g.segs ? o.g.kchunk : (int)((K + 15) / 16 * 16), 0});
+                if (K <= 64) cand.push_back(TuneCfg{6, o.g.segs ? o.g.kchunk : (int)((K + 15) / 16 * 16), 0});
                 // split precision: DMMA, the per-tile and the persistent int8 kernel
                 if (c->precision == CCQ_B200_PREC_SPLIT && o.split && (split_capable(o.g) || cur.split))
                     for (int v : {0, 1, 2})
@@ -2695,13 +2696,13 @@ int ccq_b200_set_active(ccq_b200_ctx *c, int64_t act_occ_b, int64_t act_unocc_a)
 
 int ccq_b200_force_tile(ccq_b200_ctx *c, int64_t tile) {
     if (!c) return fail(Error(CCQ_B200_EINVAL, "null context"));
-    if (tile < 0 || tile > 5) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..5"));
+    if (tile < 0 || tile > 6) return fail(Error(CCQ_B200_EINVAL, "force_tile: 0..6"));
     for (auto &o : c->plan.ops) {
         if (o.kind != OP_GETT || o.g.K == 0) continue;
         o.g.tile = (int)tile;
         if (o.g.segs) continue;
         // the small-K kernel takes the whole K range in one launch; the others the shape's split-K
-        o.g.kchunk = tile == 3 ? (o.g.K + 15) / 16 * 16 : gett_f64_kchunk(o.g.M, o.g.N, o.g.K);
+        o.g.kchunk = (tile == 3 || tile == 6) ? (o.g.K + 15) / 16 * 16 : gett_f64_kchunk(o.g.M, o.g.N, o.g.K);
         o.zero_first = (o.g.K + o.g.kchunk - 1) / o.g.kchunk > 1 && o.beta == 0;
     }
     drop_graphs(c);

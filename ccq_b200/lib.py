@@ -401,7 +401,7 @@ class Context:
 
     def force_tile(self, tile):
         """Every contraction on one kernel family (0 shape default, 1 64x64, 2 skinny, 3 small-K, 4 64x64 3-stage,
-        5 skinny 2-stage)."""
+        5 skinny 2-stage, 6 register-direct small-K)."""
         _err(self._lib.ccq_b200_force_tile(self.ptr, tile))
 
     def save_checkpoint(self, path, iteration=0, state=None, with_ring=True):

@@ -262,7 +262,8 @@ int ccq_b200_set_active(ccq_b200_ctx *ctx, int64_t act_occ_b, int64_t act_unocc_
 /* Pins every contraction to one GETT kernel family: 0 = by shape, 1 = 64 x 64
  * DMMA tiles, 2 = skinny DMMA tiles (where one side is <= 32), 3 = small-K
  * FMA kernel, 4 = 64 x 64 DMMA tiles with a 3-stage operand pipeline, 5 = skinny
- * DMMA tiles with a 2-stage ring.  A family that does not fit a shape falls back to the shape's
+ * DMMA tiles with a 2-stage ring, 6 = register-direct small-K DMMA kernel (the
+ * whole K range in one pass).  A family that does not fit a shape falls back to the shape's
  * default.  For tests and experiments; ccq_b200_autotune picks per contraction. */
 int ccq_b200_force_tile(ccq_b200_ctx *ctx, int64_t tile);
 

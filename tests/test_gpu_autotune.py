@@ -72,10 +72,10 @@ def test_tuned_solve_matches_untuned(prec):
     assert abs(res[True].iterations - res[False].iterations) <= 1
 
 
-@pytest.mark.parametrize('tile', [1, 2, 3, 4, 5])
+@pytest.mark.parametrize('tile', [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize('method,n,oa,ob', [('CCSD', 7, 3, 2), ('CCSDT', 7, 3, 2)])
 def test_forced_kernel_family_matches_oracle(tile, method, n, oa, ob, plan_text):
-    """Every contraction on one GETT family (64 x 64 DMMA, skinny DMMA, small-K FMA)."""
+    """Every contraction on one GETT family (64 x 64 DMMA, skinny DMMA, small-K FMA, register-direct DMMA)."""
     s = random_system(n, oa, ob, seed=21)
     ctx = make_ctx(s, method, shift=0.05)
     ctx.force_tile(tile)
@@ -92,12 +92,13 @@ def test_forced_kernel_family_matches_oracle(tile, method, n, oa, ob, plan_text)
 
 
 def test_small_k_kernel_on_large_views():
-    """20 orbitals: several 256-wide F tiles and 32-wide S tiles per contraction, grouped launches."""
+    """20 orbitals: several 256-wide F tiles and 32-wide S tiles per contraction, grouped launches; the
+    small-K FMA kernel and the register-direct DMMA kernel against the default families."""
     s = synth.system(synth.SynthSpec(20, 8, 40, 0.05, 3))
     d = s['dims']
     t, _ = random_t(d, seed=6, scale=0.02, nmax=3)
     out = {}
-    for tile in (0, 3):
+    for tile in (0, 3, 6):
         ctx = make_ctx(s, 'CCSDT')
         ctx.force_tile(tile)
         ctx.set_t(t)
@@ -106,3 +107,4 @@ def test_small_k_kernel_on_large_views():
         out[tile] = ctx.get_t()
         ctx.close()
     np.testing.assert_allclose(out[3], out[0], atol=1e-12, rtol=0)
+    np.testing.assert_allclose(out[6], out[0], atol=1e-12, rtol=0)
