@@ -238,12 +238,12 @@ REFERENCE_FLOPS_C2 = 2.10e11
 
 # DRAM bytes (read + write) per gett_f64 launch in one tuned split-precision sweep of this workload,
 # from one ncu capture of every GETT launch of that sweep (dram__bytes_read.sum + dram__bytes_write.sum,
-# a single-pass metric set, full size): 22.0 GB over 490 launches of the 64x64, skinny and small-K
-# families.  Command: `ncu --nvtx --nvtx-include "sweep/" --metrics
+# a single-pass metric set, full size): 17.0 GB over 527 launches of the 64x64, skinny, register-direct and
+# small-K families.  Command: `ncu --nvtx --nvtx-include "sweep/" --metrics
 # dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none --csv
 # python bench.py --case sweep split /tmp/ops_split.txt 3 tune`.
-GETT_F64_TRAFFIC = 44.93e6
-GETT_F64_TRAFFIC_NOTE = ('traffic = DRAM bytes per gett_f64 launch (mean over the 490 launches of one tuned split '
+GETT_F64_TRAFFIC = 32.18e6
+GETT_F64_TRAFFIC_NOTE = ('traffic = DRAM bytes per gett_f64 launch (mean over the 527 launches of one tuned split '
                          'sweep, ncu dram__bytes_read.sum + dram__bytes_write.sum, captured at full size)')
 
 BASELINE_KIND = ('numpy executor of this repository\'s CCSDT contraction plan (oracle/blockcc.py, threaded '

@@ -123,6 +123,7 @@ struct Op {
     double group_flops = 0.0;  // FLOPs of a grouped launch (leader only)
     int group_size = 0;
     int split_choice = -1;     // -1 by shape (split_eligible); autotuned: 0 DMMA, 1 per-tile split kernel, 2 persistent
+    int split_ws = 0;          // slicing workspace of a split GETT (0: the context's first; see split_pool)
     bool frozen = false;       // in a T3 / T4 phase of an externally corrected solve: not run
     std::vector<size_t> group_ops;   // every op of a grouped launch (leader only; members are skipped)
     std::vector<int> hcm, hcn; // output offset tables (grouping key)
@@ -315,6 +316,9 @@ struct ccq_b200_ctx {
     T3ActGeom geom{};
     double *cvec = nullptr;
     SplitWorkspace split{};
+    // further slicing workspaces: split GETTs take them in turn, so that a split GETT is a node of the sweep's
+    // dependency graph (waiting only for the previous user of its workspace) instead of a barrier
+    std::vector<SplitWorkspace> split_pool;
     // host round trip of ccq_b200_iterate_host: each t_vec block is copied to host_out as soon as its
     // last write of the sweep is done (copy stream cstream, joined into the sweep's stream at its end)
     double *host_out = nullptr;
@@ -356,6 +360,7 @@ struct ccq_b200_ctx {
         if (cap_ev) cudaEventDestroy(cap_ev);
         for (auto st : side) cudaStreamDestroy(st);
         split_free(split);
+        for (auto &w : split_pool) split_free(w);
         if (hpin) cudaFreeHost(hpin);
         if (stream) {
             for (void *p : owned) cudaFreeAsync(p, stream);
@@ -1343,6 +1348,14 @@ bool use_split(const ccq_b200_ctx *c, const Op &o) {
 // persistent split kernel (one CTA per SM, overlapped epilogue) unless tuned to the per-tile one
 int split_persistent(const Op &o) { return o.split_choice == 1 ? 0 : 1; }
 
+// split GETTs of a sweep rotate over this many slicing workspaces when one takes at most kSplitPoolBytes
+constexpr int kSplitPool = 3;
+constexpr long long kSplitPoolBytes = 1LL << 30;
+
+SplitWorkspace &split_ws(ccq_b200_ctx *c, const Op &o) {
+    return o.split_ws > 0 && o.split_ws <= (int)c->split_pool.size() ? c->split_pool[o.split_ws - 1] : c->split;
+}
+
 int op_class(const ccq_b200_ctx *c, const Op &o) {
     if (o.kind == OP_GETT) return use_split(c, o) ? 1 : 0;
     if (o.kind == OP_ASM) return 2;
@@ -1366,7 +1379,7 @@ void run_op(ccq_b200_ctx *c, Op &o, cudaStream_t st) {
                 break;
             }
             if (use_split(c, o)) {
-                c->launches += split_gett(c->split, o.g, o.akm, o.bkm, c->nslices, st, split_persistent(o));
+                c->launches += split_gett(split_ws(c, o), o.g, o.akm, o.bkm, c->nslices, st, split_persistent(o));
             } else {
                 launch_gett_f64(o.g, o.akm, o.bkm, st);
                 ++c->launches;
@@ -1503,7 +1516,9 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         // buffers (and its own block) and overwrites one buffer
         const bool plain_node = !serial_nodes && ((o.kind == OP_ASM && o.asmargs.mode != 2) ||
                                                   o.kind == OP_COPY || o.kind == OP_ZERO);
-        const bool barrier = (o.kind != OP_GETT && !plain_node) || (o.kind == OP_GETT && use_split(c, o));
+        // a split GETT is a barrier only while every split GETT shares one slicing workspace
+        const bool splitop = o.kind == OP_GETT && use_split(c, o);
+        const bool barrier = (o.kind != OP_GETT && !plain_node) || (splitop && c->split_pool.empty());
         if (barrier) {
             join();
             run_op(c, o, c->stream);
@@ -1559,6 +1574,12 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
             alias_deps(b);
         }
         alias_deps(out);
+        // the slicing workspace of a split GETT: wait for its previous user
+        const std::string wsname = splitop ? "@split" + std::to_string(o.split_ws) : std::string();
+        if (splitop) {
+            add(st[wsname].writers);
+            add(st[wsname].readers);
+        }
         BufState &cs = st[out];
         add(cs.readers);
         add(overwrite ? cs.writers : cs.full);
@@ -1571,6 +1592,10 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         CK(cudaEventRecord(c->opev[i], sd));
         copy_out_after(c, i, sd);
         pending.push_back(i);
+        if (splitop) {
+            st[wsname].writers.assign(1, i);
+            st[wsname].readers.clear();
+        }
         for (auto &b : ins) st[b].readers.push_back(i);
         if (overwrite) {
             cs.writers.assign(1, i);
@@ -2259,8 +2284,11 @@ static void iterate_finish(ccq_b200_ctx *c, double *e_cor, double *res, int64_t 
     int info = 0;
     memcpy(&info, c->hpin + 2, sizeof(int));
     if (diis && info != 0) throw Error(CCQ_B200_ESINGULAR, "calc_diis: DIIS error in DGESV");
-    if (c->precision == CCQ_B200_PREC_SPLIT && split_error(c->split))
-        throw Error(CCQ_B200_ECUDA, "split GETT pipeline wait expired");
+    if (c->precision == CCQ_B200_PREC_SPLIT) {
+        bool expired = split_error(c->split) != 0;
+        for (auto &w : c->split_pool) expired = expired || split_error(w) != 0;
+        if (expired) throw Error(CCQ_B200_ECUDA, "split GETT pipeline wait expired");
+    }
     if (e_cor) *e_cor = c->hpin[0];
     if (res) *res = std::sqrt(std::sqrt(c->hpin[1]));
     if (did_diis) *did_diis = diis;
@@ -2715,7 +2743,10 @@ int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {
         if (mode != CCQ_B200_PREC_FP64 && mode != CCQ_B200_PREC_SPLIT) throw Error(CCQ_B200_EINVAL, "precision mode");
         if (mode == CCQ_B200_PREC_SPLIT && (nslices < 2 || nslices > MAX_SLICES))
             throw Error(CCQ_B200_EINVAL, "nslices out of range");
-        if (mode == CCQ_B200_PREC_SPLIT) split_reserve(c->split, c->plan.ops.size() ? [&] {
+        if (c->async_iter) throw Error(CCQ_B200_EINVAL, "set_precision: an iteration is pending");
+        if (mode == CCQ_B200_PREC_SPLIT) {
+            CK(cudaSetDevice(c->device));
+            CK(cudaStreamSynchronize(c->stream));
             long long ma = 0, mb = 0, mc = 0;
             for (auto &o : c->plan.ops)
                 if (o.kind == OP_GETT && o.split) {
@@ -2723,8 +2754,18 @@ int ccq_b200_set_precision(ccq_b200_ctx *c, int64_t mode, int64_t nslices) {
                     mb = std::max(mb, o.mnk[1] * ((o.mnk[2] + 63) / 64 * 64));
                     mc = std::max(mc, std::max(o.mnk[0], o.mnk[1]));
                 }
-            return SplitSizes{ma, mb, mc};
-        }() : SplitSizes{0, 0, 0}, (int)nslices);
+            const SplitSizes sz{ma, mb, mc};
+            split_reserve(c->split, sz, (int)nslices);
+            // kSplitPool workspaces in turn when they are small (else one, and split GETTs stay barriers)
+            const long long bytes = (ma + mb) * nslices + 8 * mc;
+            const int pool = bytes <= kSplitPoolBytes ? kSplitPool : 1;
+            for (auto &w : c->split_pool) split_free(w);
+            c->split_pool.assign(pool - 1, SplitWorkspace{});
+            for (auto &w : c->split_pool) split_reserve(w, sz, (int)nslices);
+            int k = 0;
+            for (auto &o : c->plan.ops)
+                if (o.kind == OP_GETT && o.split) o.split_ws = (k++) % pool;
+        }
         drop_graphs(c);
         c->precision = (int)mode;
         c->nslices = (int)nslices;
