@@ -13,8 +13,10 @@ plus the DIIS ring) exceeds the 126 MB L2, so no flush is needed between steps.
 stream), whole job: max over ranks of the time / (ranks x K).  Multi-GPU runs
 are independent replicas (one solve per GPU, no collective on the data path).
 ``e2e`` is the same metric through the C ABI with the T vector in pinned host
-memory: every step copies it to the device and back (ccq_b200_iterate_host,
-whose block copies overlap the sweep).  ``--impl reference`` times the CPU
+memory: every step reads it from the host and writes it back
+(ccq_b200_iterate_host: the T3 blocks are read at their canonical elements
+inside the sweep, each operation waiting only for the blocks it reads, and
+every block is copied out as soon as the sweep has written it).  ``--impl reference`` times the CPU
 executor of this repository's CCSDT plan (numpy + threaded BLAS) on this host
 (ccq itself cannot be built: no Fortran compiler).
 
@@ -718,21 +720,25 @@ def main():
                      'note': 'achieved = algorithmic FLOPs of all launches of that kernel in 2 eager sweeps (CUDA '
                              'events around every launch) / their summed durations'})
 
-    # end-to-end through the C ABI with host buffers: every step copies the t_vec in from pinned host
-    # memory and back out (ccq_b200_iterate_host: the block copies overlap the sweep)
+    # end-to-end through the C ABI with host buffers: every step reads the t_vec from pinned host memory
+    # and writes it back (ccq_b200_iterate_host: the T3 blocks are read at their canonical elements inside
+    # the sweep, every block is copied out as soon as the sweep has written it)
     pinned = torch.empty(ctx.t_size, dtype=torch.float64, pin_memory=True)
     pinned.copy_(torch.from_numpy(ctx.get_t()))
     ctx.iterate_host(it, pinned.data_ptr(), pinned.data_ptr())   # captures the graph with its copies
     it += 1
     barrier(world)
+    io_in = io_out = 0
     t0 = time.perf_counter()
     for k in range(args.steps):
         ctx.iterate_host(it, pinned.data_ptr(), pinned.data_ptr())
+        h2d, d2h = ctx.io_bytes()
+        io_in += h2d
+        io_out += d2h + 16   # and the energy and residuum
         it += 1
     torch.cuda.synchronize()
     barrier(world)
     e2e_s = allmax(time.perf_counter() - t0, world) / (world * args.steps)
-    bytes_t = ctx.t_size * 8
     ctx.close()
 
     # convergence to tol with the headline path, |dE| vs the FP64 oracle fixture
@@ -805,8 +811,11 @@ def main():
                                       if 'split' in results else None),
             'roofline': roofline,
             'cpu_baseline': cpu,
-            'e2e': {'value': e2e_s, 'unit': 's/iter', 'h2d_bytes_per_step': bytes_t,
-                    'd2h_bytes_per_step': bytes_t + 16},
+            'e2e': {'value': e2e_s, 'unit': 's/iter', 'h2d_bytes_per_step': io_in // args.steps,
+                    'd2h_bytes_per_step': io_out // args.steps,
+                    'note': 'T1/T2 copied whole, T3 blocks read from the host at their canonical elements (the '
+                            'rest are their antisymmetric images); every block copied back out, the whole '
+                            'vector again after a DIIS step'},
             'gpu_launches': head['launches_per_iter'] * args.steps,
             'clocks': clk, 'convergence': conv, 'crcc23': crcc, 'batched_ccsd': batched, 'warm_start': warm,
             'ccsdt_active': ccsdt_act,

@@ -324,6 +324,19 @@ struct ccq_b200_ctx {
     double *host_out = nullptr;
     cudaGraphExec_t gexec_host = nullptr;
     double *gexec_host_ptr = nullptr;
+    // ... and with host_in set (pinned input, dependency-graph sweep), the t_vec is copied in block by block on
+    // istream inside the graph: an operation waits only for the copies of the blocks it reads
+    const double *host_in = nullptr;
+    const double *gexec_host_in = nullptr;
+    cudaStream_t istream = nullptr;
+    // when host_in is mapped into the device's address space (host_in_dev), the T3 blocks are read there at
+    // their canonical elements only (sorted occupied and virtual indices within each same-spin run) by a
+    // copy-mode assemble per block, which also writes every antisymmetric image on the device
+    const double *host_in_dev = nullptr;
+    std::map<std::string, AsmArgs> cin_args;   // per block read this way
+    AsmTerm *cin_terms = nullptr;               // device: one term per such block
+    long long cin_h2d = 0;                      // bytes the captured host round trip reads from host_in
+    long long io_h2d = 0, io_d2h = 0;           // bytes of the last host round trip
     cudaStream_t cstream = nullptr;
     cudaEvent_t cjoin = nullptr;
     std::vector<cudaEvent_t> cev;
@@ -350,12 +363,14 @@ struct ccq_b200_ctx {
         if (stream) cudaStreamSynchronize(stream);
         for (auto st : side) cudaStreamSynchronize(st);
         if (cstream) cudaStreamSynchronize(cstream);
+        if (istream) cudaStreamSynchronize(istream);
         if (gexec) cudaGraphExecDestroy(gexec);
         if (lgexec) cudaGraphExecDestroy(lgexec);
         if (gexec_host) cudaGraphExecDestroy(gexec_host);
         for (auto e : cev) cudaEventDestroy(e);
         if (cjoin) cudaEventDestroy(cjoin);
         if (cstream) cudaStreamDestroy(cstream);
+        if (istream) cudaStreamDestroy(istream);
         for (auto e : opev) cudaEventDestroy(e);
         if (cap_ev) cudaEventDestroy(cap_ev);
         for (auto st : side) cudaStreamDestroy(st);
@@ -1457,6 +1472,60 @@ void prepare_copy_out(ccq_b200_ctx *c) {
     c->out_ready = true;
 }
 
+// Copy-mode assembles reading the T3 blocks of the mapped host t_vec at their canonical elements (built
+// before a sweep with host_in is captured); cin_h2d counts the bytes that then cross the host link.
+void prepare_copy_in(ccq_b200_ctx *c) {
+    c->cin_args.clear();
+    c->cin_h2d = sizeof(double) * c->t_dev;
+    if (!c->host_in || !c->host_in_dev) return;
+    auto source = [&](const std::string &name) -> const Op * {
+        for (size_t i = 0; i < c->cc_end; ++i) {
+            const Op &o = c->plan.ops[i];
+            if (o.kind == OP_ASM && o.block == name && (o.asmargs.mode == 0 || o.asmargs.mode == 1)) return &o;
+        }
+        return nullptr;
+    };
+    std::vector<AsmTerm> terms;
+    std::vector<std::string> names;
+    for (auto &b : c->plan.bufs) {
+        if (b.kind != "amp") continue;
+        const DevBuf &d = c->bufs.at(b.name);
+        if (!d.ptr || d.ptr < c->tvec || d.ptr >= c->tvec + c->t_dev || d.shape.size() != 6) continue;
+        const Op *src = source(b.name);
+        if (!src) continue;
+        AsmTerm t{};
+        t.p = c->host_in_dev + (d.ptr - c->tvec);
+        t.coef = 1.0;
+        t.rank = 6;
+        for (int j = 0; j < 6; ++j) {
+            t.src[j] = (signed char)j;
+            t.zstride[j] = src->asmargs.tstride[j];
+        }
+        terms.push_back(t);
+        names.push_back(b.name);
+    }
+    if (terms.empty()) return;
+    if (!c->cin_terms) {
+        size_t cap = 0;
+        for (auto &b : c->plan.bufs) cap += b.kind == "amp";
+        c->cin_terms = (AsmTerm *)c->dalloc(sizeof(AsmTerm) * std::max<size_t>(cap, 1));
+    }
+    CK(cudaMemcpy(c->cin_terms, terms.data(), sizeof(AsmTerm) * terms.size(), cudaMemcpyHostToDevice));
+    for (size_t k = 0; k < names.size(); ++k) {
+        AsmArgs a = source(names[k])->asmargs;
+        a.mode = 1;
+        a.nterms = 1;
+        a.nplain = 1;
+        a.terms = c->cin_terms + k;
+        a.act = 0;
+        a.ecor = nullptr;
+        a.norm = nullptr;
+        c->cin_args[names[k]] = a;
+        const DevBuf &d = c->bufs.at(names[k]);
+        c->cin_h2d -= sizeof(double) * (d.numel - a.total);   // only the canonical elements cross
+    }
+}
+
 void copy_block_out(ccq_b200_ctx *c, size_t k, cudaStream_t after) {
     const DevBuf &d = c->bufs.at(c->out_after[k].second);
     CK(cudaEventRecord(c->cev[k], after));
@@ -1508,6 +1577,56 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         pending.clear();
         st.clear();
     };
+    if (c->host_in && from == 0) {
+        // the t_vec from the host, one node per amplitude block in t_vec order (T1, T2, then the T3 blocks)
+        // that the block's readers wait for (pseudo-op index ops.size() + k)
+        std::vector<std::pair<long long, std::string>> blk;
+        for (auto &b : c->plan.bufs) {
+            if (b.kind != "amp") continue;
+            const DevBuf &d = c->bufs.at(b.name);
+            if (d.ptr && d.ptr >= c->tvec && d.ptr < c->tvec + c->t_dev) blk.push_back({d.ptr - c->tvec, b.name});
+        }
+        std::sort(blk.begin(), blk.end());
+        const size_t base = c->plan.ops.size();
+        if (c->opev.size() < base + blk.size() + 1) {
+            size_t old = c->opev.size();
+            c->opev.resize(base + blk.size() + 1, nullptr);
+            for (size_t i = old; i < c->opev.size(); ++i)
+                CK(cudaEventCreateWithFlags(&c->opev[i], cudaEventDisableTiming));
+        }
+        if (!c->istream) CK(cudaStreamCreateWithFlags(&c->istream, cudaStreamNonBlocking));
+        CK(cudaStreamWaitEvent(c->istream, gate, 0));
+        // every element of [0, t_dev) once: block k covers up to the next block's start
+        long long lo = 0;
+        for (size_t k = 0; k < blk.size(); ++k) {
+            const long long hi = k + 1 < blk.size() ? blk[k + 1].first : c->t_dev;
+            auto ca = c->cin_args.find(blk[k].second);
+            if (ca != c->cin_args.end()) {
+                // canonical elements from the mapped host block, antisymmetric images written on the device
+                launch_assemble(ca->second, c->istream);
+                const long long end = blk[k].first + c->bufs.at(blk[k].second).numel;
+                if (lo < blk[k].first)
+                    CK(cudaMemcpyAsync(c->tvec + lo, c->host_in + lo, sizeof(double) * (blk[k].first - lo),
+                                       cudaMemcpyHostToDevice, c->istream));
+                if (end < hi)
+                    CK(cudaMemcpyAsync(c->tvec + end, c->host_in + end, sizeof(double) * (hi - end),
+                                       cudaMemcpyHostToDevice, c->istream));
+            } else {
+                CK(cudaMemcpyAsync(c->tvec + lo, c->host_in + lo, sizeof(double) * (hi - lo), cudaMemcpyHostToDevice,
+                                   c->istream));
+            }
+            lo = hi;
+            CK(cudaEventRecord(c->opev[base + k], c->istream));
+            st[blk[k].second].writers.assign(1, base + k);
+            st[blk[k].second].full.assign(1, base + k);
+            pending.push_back(base + k);
+        }
+        if (blk.empty()) {
+            CK(cudaMemcpyAsync(c->tvec, c->host_in, sizeof(double) * c->t_dev, cudaMemcpyHostToDevice, c->istream));
+            CK(cudaEventRecord(c->opev[base], c->istream));
+            pending.push_back(base);
+        }
+    }
     for (size_t i = from; i < to; ++i) {
         Op &o = c->plan.ops[i];
         if (o.kind == OP_PHASE || o.frozen) continue;
@@ -1660,6 +1779,7 @@ void sweep(ccq_b200_ctx *c) {
     cudaGraphExec_t &ge = c->host_out ? c->gexec_host : c->gexec;
     if (c->use_graph && !c->profile) {
         if (!ge) {
+            if (c->host_out) prepare_copy_in(c);
             cudaGraph_t g;
             long long l0 = c->launches;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1693,6 +1813,7 @@ void drop_graphs(ccq_b200_ctx *c) {
     if (c->gexec_host) cudaGraphExecDestroy(c->gexec_host);
     c->gexec = c->lgexec = c->gexec_host = nullptr;
     c->gexec_host_ptr = nullptr;
+    c->gexec_host_in = nullptr;
     c->out_ready = false;
 }
 
@@ -2301,33 +2422,54 @@ int ccq_b200_iterate_host(ccq_b200_ctx *c, int64_t iter, const double *t_in, dou
         if (n != c->t_size) throw Error(CCQ_B200_EINVAL, "iterate_host: size must equal t_size");
         if (c->async_iter) throw Error(CCQ_B200_EINVAL, "iterate_host: an iteration is pending");
         CK(cudaSetDevice(c->device));
-        CK(cudaMemcpyAsync(c->tvec, t_in, sizeof(double) * c->t_dev, cudaMemcpyHostToDevice, c->stream));
-        cudaPointerAttributes pa{};
-        const bool pinned = cudaPointerGetAttributes(&pa, t_out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-        cudaGetLastError();
+        auto host_ptr = [](const void *p, const void **dev) {
+            cudaPointerAttributes pa{};
+            const bool r = cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+            cudaGetLastError();
+            if (dev) *dev = r ? pa.devicePointer : nullptr;
+            return r;
+        };
+        const void *in_dev = nullptr;
+        const bool pinned = host_ptr(t_out, nullptr);
+        // pinned input and a dependency-graph sweep: the input blocks are copied inside the graph, each
+        // operation waiting only for the blocks it reads; else the whole t_vec is copied first
+        const bool in_graph = pinned && host_ptr(t_in, &in_dev) && c->use_graph == 1 && !c->profile;
+        if (!in_graph)
+            CK(cudaMemcpyAsync(c->tvec, t_in, sizeof(double) * c->t_dev, cudaMemcpyHostToDevice, c->stream));
         if (!pinned) {
             // pageable memory cannot take asynchronous copies inside a captured sweep: copy after it
             iterate_launch(c, iter);
             iterate_finish(c, e_cor, res, did_diis);
             CK(cudaMemcpy(t_out, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost));
+            c->io_h2d = c->io_d2h = (long long)sizeof(double) * c->t_dev;
             if (c->t_dev < n) std::fill(t_out + c->t_dev, t_out + n, 0.0);
             return 0;
         }
-        if (c->gexec_host_ptr != t_out) {
-            // the copy targets are part of the captured graph
+        const double *in_ptr = in_graph ? t_in : nullptr;
+        if (c->gexec_host_ptr != t_out || c->gexec_host_in != in_ptr) {
+            // the copy sources and targets are part of the captured graph
             if (c->gexec_host) cudaGraphExecDestroy(c->gexec_host);
             c->gexec_host = nullptr;
             c->gexec_host_ptr = t_out;
+            c->gexec_host_in = in_ptr;
         }
         c->host_out = t_out;
+        c->host_in = in_ptr;
+        c->host_in_dev = in_graph ? (const double *)in_dev : nullptr;
         try {
             iterate_launch(c, iter);
         } catch (...) {
             c->host_out = nullptr;
+            c->host_in = nullptr;
             throw;
         }
         c->host_out = nullptr;
+        c->host_in = nullptr;
         iterate_finish(c, e_cor, res, did_diis);
+        // bytes across the host link: the input (canonical T3 elements when read in the graph), every
+        // block out, and the whole vector again after a DIIS step
+        c->io_h2d = in_graph ? c->cin_h2d : (long long)sizeof(double) * c->t_dev;
+        c->io_d2h = (long long)sizeof(double) * c->t_dev * ((did_diis && *did_diis) ? 2 : 1);
         if (c->t_dev < n) std::fill(t_out + c->t_dev, t_out + n, 0.0);
         return 0;
     } catch (const Error &e) {
@@ -2335,6 +2477,13 @@ int ccq_b200_iterate_host(ccq_b200_ctx *c, int64_t iter, const double *t_in, dou
     } catch (const std::exception &e) {
         return fail(Error(CCQ_B200_EINVAL, e.what()));
     }
+}
+
+int ccq_b200_io_bytes(ccq_b200_ctx *c, int64_t *h2d, int64_t *d2h) {
+    if (!c || !h2d || !d2h) return fail(Error(CCQ_B200_EINVAL, "null argument"));
+    *h2d = c->io_h2d;
+    *d2h = c->io_d2h;
+    return 0;
 }
 
 int ccq_b200_iterate(ccq_b200_ctx *c, int64_t iter, double *e_cor, double *res, int64_t *did_diis) {

@@ -65,6 +65,7 @@ SIGNATURES = {
     'ccq_b200_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
     'ccq_b200_iterate_async': (C.c_int, [C.c_void_p, I64]),
     'ccq_b200_iterate_host': (C.c_int, [C.c_void_p, I64, C.c_void_p, C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
+    'ccq_b200_io_bytes': (C.c_int, [C.c_void_p, C.POINTER(I64), C.POINTER(I64)]),
     'ccq_b200_iterate_wait': (C.c_int, [C.c_void_p, DP, DP, C.POINTER(I64)]),
     'ccq_b200_lambda_init': (C.c_int, [C.c_void_p, C.c_double]),
     'ccq_b200_lambda_iterate': (C.c_int, [C.c_void_p, I64, DP, DP, C.POINTER(I64)]),
@@ -349,6 +350,12 @@ class Context:
         e, r, d = C.c_double(), C.c_double(), I64()
         _err(self._lib.ccq_b200_iterate(self.ptr, it, C.byref(e), C.byref(r), C.byref(d)))
         return e.value, r.value, bool(d.value)
+
+    def io_bytes(self):
+        """(host-to-device, device-to-host) bytes of the last iterate_host."""
+        a, b = I64(), I64()
+        _err(self._lib.ccq_b200_io_bytes(self.ptr, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def iterate_host(self, it, t_in_ptr, t_out_ptr):
         """One iteration from host t_vec t_in to host t_vec t_out (pointers to t_size doubles, pinned

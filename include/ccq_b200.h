@@ -218,9 +218,20 @@ int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
  * written it for the last time, overlapping the rest of the sweep (after a
  * DIIS step the whole vector is copied again).  t_in may equal t_out.  With
  * pageable t_out the copy-out follows the sweep instead of overlapping it.
+ * With pinned t_in and t_out and the dependency-graph sweep (use_graph 1),
+ * the input is read inside the sweep, block by block, each operation waiting
+ * only for the blocks it reads; when t_in is mapped into the device's address
+ * space (pinned by cudaHostAlloc, or registered as mapped) the T3 blocks are
+ * read there at their canonical elements only (sorted indices within each
+ * same-spin run of occupied and of virtual labels), every other element being
+ * the antisymmetric image that the reference's t*_update fill writes.
  * Returns what ccq_b200_iterate does. */
 int ccq_b200_iterate_host(ccq_b200_ctx *ctx, int64_t iter, const double *t_in, double *t_out, int64_t n,
                           double *e_cor, double *residuum, int64_t *did_diis);
+
+/* Bytes the last ccq_b200_iterate_host moved from host to device and back.
+ * No counterpart in the reference. */
+int ccq_b200_io_bytes(ccq_b200_ctx *ctx, int64_t *h2d, int64_t *d2h);
 
 /* ccq_b200_iterate in two halves, for many independent solves at once (one
  * context per Hamiltonian, each on its own stream): _async enqueues the

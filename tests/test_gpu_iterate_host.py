@@ -18,14 +18,22 @@ def _ctx(s, method, graph):
 
 
 @pytest.mark.parametrize('method,graph,pinned', [('CCSDT', 1, True), ('CCSDT', 2, False), ('CCSDT', 0, True),
-                                                 ('CCSD', 1, True), ('CCSDTQ', 1, False)])
+                                                 ('CCSD', 1, True), ('CCSDTQ', 1, False), ('CCSDTQ', 1, True),
+                                                 ('CCSDT', 1, 'two')])
 def test_iterate_host_equals_iterate_and_get_t(method, graph, pinned):
+    """pinned True: one pinned buffer in and out; 'two': separate pinned input and output buffers (the
+    input read block by block inside the dependency-graph sweep); False: pageable memory."""
     import torch
     s = random_system(7, 3, 2, seed=12, sigma=0.08) if method != 'CCSDTQ' else random_system(5, 2, 2, seed=12)
     a = _ctx(s, method, graph)
     b = _ctx(s, method, graph)
     n = a.t_size
-    if pinned:
+    if pinned == 'two':
+        bin_ = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+        bout = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+        pin, pout = bin_.data_ptr(), bout.data_ptr()
+        view = bout.numpy()
+    elif pinned:
         buf = torch.zeros(n, dtype=torch.float64, pin_memory=True)
         pin, pout = buf.data_ptr(), buf.data_ptr()
         view = buf.numpy()
@@ -38,10 +46,22 @@ def test_iterate_host_equals_iterate_and_get_t(method, graph, pinned):
         ta = a.get_t()
         eb, rb, db = b.iterate_host(it, pin, pout)
         tb = view.copy() if pinned else tout.copy()
-        if not pinned:
+        if pinned == 'two':
+            bin_.numpy()[...] = view
+        elif not pinned:
             tin[...] = tout
         assert da == db
         assert abs(ea - eb) < 1e-12 and abs(ra - rb) < 1e-12
         np.testing.assert_allclose(tb, ta, atol=1e-12, rtol=0)
+        h2d, d2h = b.io_bytes()
+        # pinned output: each block as the sweep finishes it, and the whole vector again after a DIIS step;
+        # the device holds the amplitude blocks of the method (t_vec may be longer)
+        full = d2h // (2 if (db and pinned) else 1)
+        assert 0 < full <= 8 * n and d2h % full == 0
+        if pinned and graph == 1 and method != 'CCSD':
+            # the T3 blocks were read from the mapped host vector at their canonical elements only
+            assert h2d < full
+        else:
+            assert h2d == full
     a.close()
     b.close()
