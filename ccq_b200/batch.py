@@ -121,6 +121,53 @@ def create_instances(specs, calc_type='CCSD', diis_space=5, graph=True, threads=
         return list(ex.map(make, specs))
 
 
+def solve_pipelined(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, threads=None):
+    """Solve every instance, iterating the instances whose contexts exist while host threads create the others
+    (largest first); returns (results, timings) as solve_batch, timings with ``total_s`` (first context
+    requested to last instance converged) and ``setup_s`` (until the last context exists).  Each instance
+    iterates exactly as on its own."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor, FIRST_COMPLETED, wait
+    import torch
+    dev = torch.cuda.current_device()
+
+    def make(sp):
+        torch.cuda.set_device(dev)
+        return Instance(sp, calc_type, diis_space, True)
+    n = threads or min(4, os.cpu_count() or 1, max(1, len(specs)))
+    order = sorted(range(len(specs)), key=lambda i: -cost(specs[i]))
+    insts = [None] * len(specs)
+    t0 = time.perf_counter()
+    t_setup = t0
+    active = []
+    ex = ThreadPoolExecutor(max_workers=n)
+    try:
+        pending = {ex.submit(make, specs[i]): i for i in order}
+        while pending or active:
+            if not active:
+                wait(list(pending), return_when=FIRST_COMPLETED)
+            for f in [f for f in pending if f.done()]:
+                i = pending.pop(f)
+                insts[i] = f.result()
+                active.append(insts[i])
+                if not pending:
+                    t_setup = time.perf_counter()
+            for x in active:
+                x.step_launch()
+            for x in active:
+                x.step_finish(tol, max_iter)
+            active = [x for x in active if not x.done]
+        t2 = time.perf_counter()
+        res = [dict(e_cor=x.e, iterations=x.it, failed=x.failed, device_ms=x.device_ms, synth_s=x.t_synth,
+                    context_s=x.t_ctx) for x in insts]
+    finally:
+        ex.shutdown(wait=True)
+        for x in insts:
+            if x is not None:
+                x.close()
+    return res, {'setup_s': t_setup - t0, 'solve_s': t2 - t_setup, 'total_s': t2 - t0}
+
+
 def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, graph=True, t_init=None,
                 keep_t=False, chunk=None, grouped=False):
     """Solve every instance; returns (results, timings).
@@ -185,11 +232,13 @@ def solve_batch(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=5, g
     return res, {'setup_s': t1 - t0, 'solve_s': t2 - t1}
 
 
-def solve_sharded(specs, rank, world, gather, **kw):
+def solve_sharded(specs, rank, world, gather, pipelined=False, **kw):
     """This rank's share of ``specs``; ``gather(obj)`` returns the list of every rank's obj."""
     parts = shard(specs, world)
     mine = parts[rank]
-    res, tim = solve_batch([specs[i] for i in mine], **kw) if mine else ([], {'setup_s': 0.0, 'solve_s': 0.0})
+    run = solve_pipelined if pipelined else solve_batch
+    empty = {'setup_s': 0.0, 'solve_s': 0.0, 'total_s': 0.0}
+    res, tim = run([specs[i] for i in mine], **kw) if mine else ([], empty)
     allres = gather((mine, res, tim))
     out = [None] * len(specs)
     for idx, rr, _ in allres:
