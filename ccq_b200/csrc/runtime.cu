@@ -324,6 +324,10 @@ struct ccq_b200_ctx {
     double *host_out = nullptr;
     cudaGraphExec_t gexec_host = nullptr;
     double *gexec_host_ptr = nullptr;
+    // a DIIS iteration's host round trip: the sweep reads the input but copies nothing out (the
+    // extrapolation rewrites every block); the whole extrapolated vector then goes to diis_out
+    cudaGraphExec_t gexec_hin = nullptr;
+    double *diis_out = nullptr;
     // ... and with host_in set (pinned input, dependency-graph sweep), the t_vec is copied in block by block on
     // istream inside the graph: an operation waits only for the copies of the blocks it reads
     const double *host_in = nullptr;
@@ -367,6 +371,7 @@ struct ccq_b200_ctx {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (lgexec) cudaGraphExecDestroy(lgexec);
         if (gexec_host) cudaGraphExecDestroy(gexec_host);
+        if (gexec_hin) cudaGraphExecDestroy(gexec_hin);
         for (auto e : cev) cudaEventDestroy(e);
         if (cjoin) cudaEventDestroy(cjoin);
         if (cstream) cudaStreamDestroy(cstream);
@@ -1782,10 +1787,10 @@ void run_ops(ccq_b200_ctx *c, size_t from, size_t to) {
 void sweep(ccq_b200_ctx *c) {
     // with host_out set, the captured graph also holds the copy-out of every finished block
     if (c->host_out) prepare_copy_out(c);
-    cudaGraphExec_t &ge = c->host_out ? c->gexec_host : c->gexec;
+    cudaGraphExec_t &ge = c->host_out ? c->gexec_host : (c->host_in ? c->gexec_hin : c->gexec);
     if (c->use_graph && !c->profile) {
         if (!ge) {
-            if (c->host_out) prepare_copy_in(c);
+            if (c->host_out || c->host_in) prepare_copy_in(c);
             cudaGraph_t g;
             long long l0 = c->launches;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1817,7 +1822,8 @@ void drop_graphs(ccq_b200_ctx *c) {
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->lgexec) cudaGraphExecDestroy(c->lgexec);
     if (c->gexec_host) cudaGraphExecDestroy(c->gexec_host);
-    c->gexec = c->lgexec = c->gexec_host = nullptr;
+    if (c->gexec_hin) cudaGraphExecDestroy(c->gexec_hin);
+    c->gexec = c->lgexec = c->gexec_host = c->gexec_hin = nullptr;
     c->gexec_host_ptr = nullptr;
     c->gexec_host_in = nullptr;
     c->out_ready = false;
@@ -2374,9 +2380,9 @@ static void post_sweep(ccq_b200_ctx *c, int64_t iter, cudaStream_t st) {
             launch_diis_extrap(c->ring, vs, ds, vs, c->scratch + 8 + 169, c->tvec, st);
         }
         c->launches += 3;
-        // the extrapolation rewrote T1 .. T3: the host copy is taken again
-        if (c->host_out)
-            CK(cudaMemcpyAsync(c->host_out, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost, st));
+        // the extrapolation rewrote T1 .. T3: the host copy is taken (again)
+        if (double *dst = c->host_out ? c->host_out : c->diis_out)
+            CK(cudaMemcpyAsync(dst, c->tvec, sizeof(double) * c->t_dev, cudaMemcpyDeviceToHost, st));
     }
     CK(cudaEventRecord(c->ev2, st));
     CK(cudaMemcpyAsync(c->hpin, c->bufs.at("E").ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -2455,27 +2461,32 @@ int ccq_b200_iterate_host(ccq_b200_ctx *c, int64_t iter, const double *t_in, dou
         if (c->gexec_host_ptr != t_out || c->gexec_host_in != in_ptr) {
             // the copy sources and targets are part of the captured graph
             if (c->gexec_host) cudaGraphExecDestroy(c->gexec_host);
-            c->gexec_host = nullptr;
+            if (c->gexec_hin) cudaGraphExecDestroy(c->gexec_hin);
+            c->gexec_host = c->gexec_hin = nullptr;
             c->gexec_host_ptr = t_out;
             c->gexec_host_in = in_ptr;
         }
-        c->host_out = t_out;
+        // a DIIS iteration copies nothing out during the sweep: the extrapolation after it rewrites every
+        // block, and the extrapolated vector is copied out whole
+        const bool diis_it = (iter % (c->ds + 1)) == 0;
+        c->host_out = diis_it ? nullptr : t_out;
+        c->diis_out = diis_it ? t_out : nullptr;
         c->host_in = in_ptr;
         c->host_in_dev = in_graph ? (const double *)in_dev : nullptr;
         try {
             iterate_launch(c, iter);
         } catch (...) {
-            c->host_out = nullptr;
+            c->host_out = c->diis_out = nullptr;
             c->host_in = nullptr;
             throw;
         }
-        c->host_out = nullptr;
+        c->host_out = c->diis_out = nullptr;
         c->host_in = nullptr;
         iterate_finish(c, e_cor, res, did_diis);
-        // bytes across the host link: the input (canonical T3 elements when read in the graph), every
-        // block out, and the whole vector again after a DIIS step
+        // bytes across the host link: the input (canonical T3 elements when read in the graph) and the
+        // whole vector out (block by block during the sweep, or after the extrapolation of a DIIS step)
         c->io_h2d = in_graph ? c->cin_h2d : (long long)sizeof(double) * c->t_dev;
-        c->io_d2h = (long long)sizeof(double) * c->t_dev * ((did_diis && *did_diis) ? 2 : 1);
+        c->io_d2h = (long long)sizeof(double) * c->t_dev;
         if (c->t_dev < n) std::fill(t_out + c->t_dev, t_out + n, 0.0);
         return 0;
     } catch (const Error &e) {

@@ -215,8 +215,8 @@ int ccq_b200_iterate(ccq_b200_ctx *ctx, int64_t iter, double *e_cor,
 /* One iteration from a host t_vec to a host t_vec (the reference's loop when
  * it keeps cc%t_vec on the host): t_in is copied to the device, the sweep
  * runs, and every T1..T3 block is copied to t_out as soon as the sweep has
- * written it for the last time, overlapping the rest of the sweep (after a
- * DIIS step the whole vector is copied again).  t_in may equal t_out.  With
+ * written it for the last time, overlapping the rest of the sweep (in a DIIS
+ * iteration the extrapolated vector is copied out whole after the sweep instead).  t_in may equal t_out.  With
  * pageable t_out the copy-out follows the sweep instead of overlapping it.
  * With pinned t_in and t_out and the dependency-graph sweep (use_graph 1),
  * the input is read inside the sweep, block by block, each operation waiting
