@@ -593,8 +593,11 @@ def main():
             dist.destroy_process_group()
         return
     from ccq_b200 import lib, synth
-    if args.warmup < 3:
-        args.warmup = 3
+    # at least one DIIS cycle of warm-up (diis_space + 1 = 6 iterations): a context's first DIIS step pays
+    # one-time costs (34-1229 ms were seen in the FP64 leg's timed window, 16 ms in isolated runs); the
+    # line reports the warm-up actually done
+    if args.warmup < 6:
+        args.warmup = 6
     s = synth.system(synth.C2)
     d = s['dims']
     peaks_file, peaks_kind = measured_peaks_file()
