@@ -43,6 +43,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = 'CCSDT s/iter + TFLOP/s on 1 B200, split vs FP64 GPU; |dE| vs FP64 oracle'
 WORKLOAD = 'CCSDT, 40 spatial orbitals, nel=16, nvir=64, L=80, sigma=0.025, seed=2, UHF spin blocks'
+L2_NOTE = 'working set (T3 4x134 MB + DIIS ring) > 126 MB L2, no flush'
 
 
 def parse():
@@ -304,7 +305,8 @@ def run_reference(args, rank, world):
         'n_gpus': args.gpus, 'steps': r['iters_timed'], 'warmup': w, 'ms_per_step': r['s_per_iter'] * 1e3,
         'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
         'data': 'synthetic (seeded generator, no molecular integrals)',
-        'config': {'workload': WORKLOAD, 'parallelism': 'cpu threads', 'l2': 'working set > L2'},
+        'config': {'workload': WORKLOAD, 'parallelism': f'replicas x{world}', 'l2': L2_NOTE},
+        'threads': 'all host threads (threaded BLAS)',
         'cpu_baseline': {'value': r['s_per_iter'], 'unit': 's/iter', 'cores': r['cores'], 'kind': 'port',
                          'sample': f"{r['iters_timed']} full CCSDT iteration(s) after {w} warm-up; " + BASELINE_KIND},
         'e2e': {'value': r['s_per_iter'], 'unit': 's/iter', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
@@ -814,8 +816,9 @@ def main():
             'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'f64' if headline == 'fp64' else f'f64 (int8 x{args.slices} slices, int32 acc)',
             'data': 'synthetic (seeded generator, no molecular integrals)',
-            'config': {'workload': WORKLOAD, 'precision': headline, 'parallelism': f'replicas x{world}',
-                       'l2': 'working set (T3 4x134 MB + DIIS ring) > 126 MB L2, no flush'},
+            # the same workload config as the reference arm's line; how this arm ran it is in precision
+            'config': {'workload': WORKLOAD, 'parallelism': f'replicas x{world}', 'l2': L2_NOTE},
+            'precision': headline,
             'tflops': head['tflops'],
             'flops_per_iter': head['flops_per_iter'],
             'flops_reference_per_iter': REFERENCE_FLOPS_C2,
