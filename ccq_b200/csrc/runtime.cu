@@ -790,6 +790,27 @@ void instantiate(ccq_b200_ctx *c) {
         phase_fill[ph] += ne;
         arena = std::max(arena, phase_fill[ph]);
     }
+    {
+        // consecutive phases take alternate halves of a doubled arena (up to 16 GiB), so that a phase's
+        // contractions need not wait for the previous phase's assemble to finish reading its work buffers
+        // (CCQ_B200_ARENA_SINGLE set: one shared region)
+        std::vector<std::pair<long long, std::string>> order;
+        for (auto &kv : phase_fill) {
+            const size_t h = kv.first.rfind('#');
+            order.push_back({h == std::string::npos ? -1LL : std::atoll(kv.first.c_str() + h + 1), kv.first});
+        }
+        std::sort(order.begin(), order.end());
+        if (order.size() >= 2 && sizeof(double) * 2 * arena <= (16LL << 30) && !getenv("CCQ_B200_ARENA_SINGLE")) {
+            std::map<std::string, int> parity;
+            for (size_t k = 0; k < order.size(); ++k) parity[order[k].second] = (int)(k & 1);
+            for (auto &b : c->plan.bufs) {
+                if (b.kind != "work") continue;
+                const std::string ph = first_phase.count(b.name) ? first_phase[b.name] : "unused";
+                if (parity[ph]) work_off[b.name] += arena;
+            }
+            arena *= 2;
+        }
+    }
     double *arena_ptr = (double *)c->dalloc(sizeof(double) * std::max(arena, 1LL));
     for (auto &b : c->plan.bufs) {
         DevBuf d;
