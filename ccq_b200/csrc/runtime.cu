@@ -1604,10 +1604,13 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
     cudaEvent_t gate = c->cap_ev;   // the last barrier (or the capture's start)
     CK(cudaEventRecord(gate, c->stream));
     int rr = 0;
+    std::vector<long long> last_on(NSIDE, -1);   // last node issued on each side stream since the last barrier
+    static const bool round_robin = getenv("CCQ_B200_DAG_ROUND_ROBIN") != nullptr;
     auto join = [&]() {
         for (size_t j : pending) CK(cudaStreamWaitEvent(c->stream, c->opev[j], 0));
         pending.clear();
         st.clear();
+        std::fill(last_on.begin(), last_on.end(), -1LL);
     };
     if (c->host_in && from == 0) {
         // the t_vec from the host, one node per amplitude block in t_vec order (T1, T2, then the T3 blocks)
@@ -1734,10 +1737,26 @@ void run_ops_dag(ccq_b200_ctx *c, size_t from, size_t to) {
         BufState &cs = st[out];
         add(cs.readers);
         add(overwrite ? cs.writers : cs.full);
-        cudaStream_t sd = c->side[rr++ % NSIDE];
-        CK(cudaStreamWaitEvent(sd, gate, 0));
         std::sort(deps.begin(), deps.end());
         deps.erase(std::unique(deps.begin(), deps.end()), deps.end());
+        // a captured stream orders its operations, so the stream chosen adds an edge from its last node:
+        // take the stream whose last node is the latest of this node's dependencies (a true edge), else
+        // the stream whose last node is the oldest (round robin when CCQ_B200_DAG_ROUND_ROBIN is set)
+        int si = rr++ % NSIDE;
+        if (!round_robin) {
+            int best = -1;
+            for (int q = 0; q < NSIDE; ++q)
+                if (last_on[q] >= 0 && std::binary_search(deps.begin(), deps.end(), (size_t)last_on[q]) &&
+                    (best < 0 || last_on[q] > last_on[best]))
+                    best = q;
+            if (best < 0)
+                for (int q = 0; q < NSIDE; ++q)
+                    if (best < 0 || last_on[q] < last_on[best]) best = q;
+            si = best;
+        }
+        last_on[si] = (long long)i;
+        cudaStream_t sd = c->side[si];
+        CK(cudaStreamWaitEvent(sd, gate, 0));
         for (size_t d : deps) CK(cudaStreamWaitEvent(sd, c->opev[d], 0));
         run_op(c, o, sd);
         CK(cudaEventRecord(c->opev[i], sd));
