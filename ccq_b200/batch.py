@@ -141,6 +141,7 @@ def solve_pipelined(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=
     t_setup = t0
     active = []
     ex = ThreadPoolExecutor(max_workers=n)
+    pending = {}
     try:
         pending = {ex.submit(make, specs[i]): i for i in order}
         while pending or active:
@@ -162,6 +163,9 @@ def solve_pipelined(specs, tol=1e-8, max_iter=200, calc_type='CCSD', diis_space=
                     context_s=x.t_ctx) for x in insts]
     finally:
         ex.shutdown(wait=True)
+        for f in pending:   # contexts still being created when an error stopped the loop
+            if f.exception() is None:
+                f.result().close()
         for x in insts:
             if x is not None:
                 x.close()
