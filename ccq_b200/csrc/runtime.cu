@@ -1124,6 +1124,37 @@ void instantiate(ccq_b200_ctx *c) {
                     at.glen[g] = (signed char)src.groups[g].size();
                     for (size_t q = 0; q < src.groups[g].size(); ++q) at.gpos[g][q] = (signed char)src.groups[g][q];
                 }
+                {
+                    // A group read sorted with sign whose axes all hold indices of one same-spin run of the
+                    // block: a canonical element's indices increase along that run, so the sort is the same
+                    // for every element. It is applied here (axes reassigned, sign into the coefficient)
+                    // and the term becomes a plain view, read without a per-element sort.
+                    std::vector<int> run_of(a.rank);
+                    int r = -1;
+                    for (int d = 0; d < a.rank; ++d) {
+                        if (a.runstart[d]) ++r;
+                        run_of[d] = r;
+                    }
+                    bool fixed = at.ng > 0;
+                    for (int g = 0; g < at.ng && fixed; ++g)
+                        for (int q = 1; q < at.glen[g]; ++q)
+                            fixed = fixed && run_of[at.src[at.gpos[g][q]]] == run_of[at.src[at.gpos[g][0]]];
+                    if (fixed) {
+                        for (int g = 0; g < at.ng; ++g) {
+                            std::vector<int> ax(at.gpos[g], at.gpos[g] + at.glen[g]);
+                            std::sort(ax.begin(), ax.end());
+                            std::vector<int> tg;
+                            for (int x : ax) tg.push_back(at.src[x]);
+                            int inv = 0;
+                            for (size_t u = 0; u < tg.size(); ++u)
+                                for (size_t w = u + 1; w < tg.size(); ++w) inv += tg[w] < tg[u];
+                            if (inv & 1) at.coef = -at.coef;
+                            std::sort(tg.begin(), tg.end());
+                            for (size_t u = 0; u < ax.size(); ++u) at.src[ax[u]] = (signed char)tg[u];
+                        }
+                        at.ng = 0;
+                    }
+                }
                 hterms.push_back(at);
             }
             a.nterms = (int)o.terms.size();
