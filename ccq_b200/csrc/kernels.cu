@@ -1176,11 +1176,24 @@ __device__ __forceinline__ void canonical_element(const AsmArgs &a, Off lin, int
 
 // Off: index type of every offset (int when AsmArgs::off32 says they all fit)
 // The canonical elements [base0, total) of one assemble, blockDim.x * ASM_EPT of them per step.
+constexpr int ASM_PMAX = 64;   // orbit permutations whose write strides are staged in shared memory
+
 template <int RK, typename Off, int CH>
 __device__ __forceinline__ void assemble_body(const AsmArgs &a, SmTerm<RK> (&st)[CH], long long base0,
                                               long long step) {
     const int nch = (a.nterms + CH - 1) / CH;
     double nacc = 0.0;
+    // write strides of every orbit permutation P: copy P of element x sits at sum_j pst[P][j] x[j]
+    // (pst[P][P[d]] = tstride[d]), so a copy's offset takes RK multiply-adds and no index selects
+    __shared__ int pst[ASM_PMAX * RK];
+    const bool staged = a.nperm <= ASM_PMAX;
+    if (staged) {
+        for (int i = threadIdx.x; i < a.nperm * RK; i += blockDim.x) {
+            const int pidx = i / RK, d = i - pidx * RK;
+            pst[pidx * RK + a.perm[i]] = a.tstride[d];
+        }
+        __syncthreads();
+    }
     for (long long base = base0; base < a.total; base += step) {
         int x[ASM_EPT][RK];
         bool act[ASM_EPT];    // an element of the block
@@ -1321,12 +1334,21 @@ __device__ __forceinline__ void assemble_body(const AsmArgs &a, SmTerm<RK> (&st)
             } else {
                 tnew = R[e];
             }
-            for (int pidx = 0; pidx < a.nperm; ++pidx) {
-                const signed char *P = a.perm + pidx * RK;
-                Off o = 0;
+            if (staged) {
+                for (int pidx = 0; pidx < a.nperm; ++pidx) {
+                    Off o = 0;
 #pragma unroll
-                for (int d = 0; d < RK; ++d) o += (Off)a.tstride[d] * pick<RK>(x[e], P[d]);
-                a.T[o] = a.psign[pidx] * tnew;
+                    for (int j = 0; j < RK; ++j) o += (Off)pst[pidx * RK + j] * x[e][j];
+                    a.T[o] = a.psign[pidx] * tnew;
+                }
+            } else {
+                for (int pidx = 0; pidx < a.nperm; ++pidx) {
+                    const signed char *P = a.perm + pidx * RK;
+                    Off o = 0;
+#pragma unroll
+                    for (int d = 0; d < RK; ++d) o += (Off)a.tstride[d] * pick<RK>(x[e], P[d]);
+                    a.T[o] = a.psign[pidx] * tnew;
+                }
             }
         }
     }
