@@ -109,9 +109,10 @@ __device__ __forceinline__ void load_tile(double *S, const double *base, const i
 // The MMAs of one staged BKT-deep K tile into a warp's 32 x 32 accumulator block.
 template <bool AK, bool BKM>
 __device__ __forceinline__ void mma_stage(double (&acc)[2][4][4], const double *As, const double *Bs, int wm, int wn,
-                                          int gid, int tig) {
+                                          int gid, int tig, int nk) {
 #pragma unroll
     for (int kk = 0; kk < BKT; kk += 8) {
+        if (kk >= nk) break;   // the rest of the tile is the zero fill past the K range
         double a[2][4], b[4][2];
 #pragma unroll
         for (int mi = 0; mi < 2; ++mi)
@@ -179,7 +180,7 @@ __device__ __forceinline__ void gett_mainloop(double (&acc)[2][4][4], double *As
         cp_async_commit();
         cp_async_wait<NST - 1>();   // tile t has landed
         __syncthreads();
-        mma_stage<AK, BKM>(acc, As + st * TILE, Bs + st * TILE, wm, wn, gid, tig);
+        mma_stage<AK, BKM>(acc, As + st * TILE, Bs + st * TILE, wm, wn, gid, tig, kend - (kbeg + t * BKT));
         __syncthreads();
     }
 }
@@ -589,8 +590,10 @@ __device__ __forceinline__ void skinny_mainloop(double (&acc)[BMS / 16][4][4], d
             skinny_load<BMS, AK, BKM>(sm + (tn % ST) * T::STAGE, p, t, M, N, m0, n0, kbeg + tn * SBK, kend, tid, vb);
         cp_async_commit();
         const double *As = sm + (it % ST) * T::STAGE, *Bs = As + T::ATILE;
+        const int nk = kend - (kbeg + it * SBK);   // past it the slab holds the zero fill
 #pragma unroll
         for (int kk = 0; kk < SBK; kk += 8) {
+            if (kk >= nk) break;
             double a[BMS / 16][4], b[4][2];
 #pragma unroll
             for (int mi = 0; mi < BMS / 16; ++mi)
